@@ -1,0 +1,111 @@
+"""ctypes binding of libgse_b200.so (the C ABI declared in include/gse_b200.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+the CUDA library is missing or no B200 is present, calls raise GseError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Any
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libgse_b200.so")
+
+GSE_OK = 0
+STATUS_NAMES = {
+    0: "GSE_OK", 1: "GSE_ERR_INVALID_ARG", 2: "GSE_ERR_STENCIL_TOO_LARGE", 3: "GSE_ERR_CUDA",
+    4: "GSE_ERR_OOM", 5: "GSE_ERR_TIMEOUT", 6: "GSE_ERR_NOT_READY", 7: "GSE_ERR_UNSUPPORTED",
+    8: "GSE_ERR_NONFINITE",
+}
+PRECISION = {"fp64": 0, "mixed": 1}
+GRID_RHO = 0
+GRID_PHI = 1
+
+
+class GseError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.name = STATUS_NAMES.get(status, f"status {status}")
+        super().__init__(f"{self.name}: {message}")
+
+
+class gse_params_t(ctypes.Structure):
+    _fields_ = [
+        ("size_x", ctypes.c_int), ("size_y", ctypes.c_int), ("size_z", ctypes.c_int),
+        ("sigma", ctypes.c_double), ("kappa", ctypes.c_double),
+        ("lambda_sigma", ctypes.c_double), ("lambda_sigma1", ctypes.c_double),
+        ("box_x", ctypes.c_double), ("box_y", ctypes.c_double), ("box_z", ctypes.c_double),
+        ("ccelec", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+# Every exported symbol with (restype, argtypes); used both to bind and by
+# the CPU test that checks the library exports what the header declares.
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+_dp = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "gse_params_default": (None, [ctypes.POINTER(gse_params_t)]),
+    "gse_status_string": (ctypes.c_char_p, [_i]),
+    "gse_last_error": (ctypes.c_char_p, []),
+    "gse_abi_version": (_i, []),
+    "gse_create": (_i, [ctypes.POINTER(gse_params_t), ctypes.POINTER(_vp)]),
+    "gse_destroy": (_i, [_vp]),
+    "gse_set_stream": (_i, [_vp, _vp]),
+    "gse_set_box": (_i, [_vp, _d, _d, _d]),
+    "gse_synchronize": (_i, [_vp]),
+    "gse_spread_charge": (_i, [_vp, _i, _vp]),
+    "gse_solve_poisson": (_i, [_vp]),
+    "gse_calculate_energy": (_i, [_vp, _vp]),
+    "gse_interpolate_force": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "gse_forward": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "gse_get_grid": (_i, [_vp, _i, _vp]),
+    "gse_set_grid": (_i, [_vp, _i, _vp]),
+    "gse_gauss_spread": (_i, [_vp, _d, _d, _i, _vp, _d, _d, _d, _i, _vp]),
+    "gse_gauss_interpolate": (_i, [_vp, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
+    "gse_green_mul": (_i, [_vp, _d, _d, _d, _d, _vp]),
+    "gse_fft_solve": (_i, [_vp, _d, _d, _d, _d, _vp, _vp]),
+}
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise GseError(7, f"{LIB_PATH} is not built")
+        from . import build
+        build.build_lib()
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != GSE_OK:
+        msg = _lib.gse_last_error().decode() if _lib is not None else ""
+        raise GseError(status, msg)
+
+
+def ptr(obj: Any):
+    """Address of a numpy array, a torch tensor, a ctypes object or an int."""
+    if obj is None:
+        return None
+    if isinstance(obj, int):
+        return obj
+    if hasattr(obj, "data_ptr"):          # torch.Tensor
+        return obj.data_ptr()
+    if hasattr(obj, "ctypes"):            # numpy.ndarray
+        return obj.ctypes.data
+    if isinstance(obj, ctypes._SimpleCData) or isinstance(obj, ctypes.Array):
+        return ctypes.addressof(obj)
+    raise TypeError(f"cannot take the address of {type(obj)}")

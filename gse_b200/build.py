@@ -1,0 +1,84 @@
+"""In-tree build of libgse_b200.so (nvcc, sm_100a) and the C++ drop-in check
+program.  `python -m gse_b200.build` rebuilds when a source is newer than its
+output."""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(PKG, "libgse_b200.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+              "--expt-relaxed-constexpr"]
+
+
+def _sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _deps():
+    return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
+            glob.glob(os.path.join(INCLUDE, "*.h")) + [os.path.abspath(__file__)])
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def nvcc_cmd(out=LIB):
+    return ([NVCC] + ARCH + NVCC_FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC] + _sources() +
+            ["-o", out, "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft",
+             "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")])
+
+
+def build_lib(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale(LIB, _deps()):
+        return LIB
+    if not os.path.exists(NVCC):
+        raise RuntimeError(f"nvcc not found at {NVCC}")
+    tmp = LIB + ".tmp"
+    cmd = nvcc_cmd(tmp)
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+CXX_DIR = os.path.join(PKG, "cxx")
+CXX_CHECK = os.path.join(CXX_DIR, "gse_dropin_check")
+
+
+def build_cxx_check(force: bool = False) -> str:
+    """The drop-in C++ classes compiled into a small driver (gse_dropin_check)."""
+    src = os.path.join(CXX_DIR, "gse_dropin_check.cpp")
+    deps = [src] + glob.glob(os.path.join(CXX_DIR, "*.h")) + [LIB]
+    if not force and not _stale(CXX_CHECK, deps):
+        return CXX_CHECK
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", INCLUDE, "-I", CXX_DIR, src, "-o", CXX_CHECK,
+                    "-L", PKG, "-lgse_b200", "-Wl,-rpath," + PKG], check=True)
+    return CXX_CHECK
+
+
+def build_all(force: bool = False, verbose: bool = False) -> None:
+    build_lib(force=force, verbose=verbose)
+    if os.path.exists(os.path.join(CXX_DIR, "gse_dropin_check.cpp")):
+        build_cxx_check(force=force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose=True)
+    print(LIB)

@@ -1,0 +1,732 @@
+// gse_api.cu -- C ABI of the GSE-k library (include/gse_b200.h).
+//
+// One gse_context owns, on one device and one stream: the rhoS and phiM grids
+// (CpuGSE.h:38-42), the k-space buffer rhoK (CpuFFTSolver.h:24), the int64
+// fixed-point accumulation grid of the mixed form, cuFFT plans (replacing
+// the FFTW plans of CpuFFTSolver.cpp:28-69), and staging buffers for atoms
+// and forces.
+#include <cufft.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <cmath>
+#include <string>
+
+#include "gse_b200.h"
+#include "gse_internal.cuh"
+#include "gse_kernels.cuh"
+
+using namespace gse;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gse_status_t fail(gse_status_t s, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+gse_status_t fail(gse_status_t s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define CU(call)                                                                            \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return fail(_e == cudaErrorMemoryAllocation ? GSE_ERR_OOM : GSE_ERR_CUDA,             \
+                  "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));       \
+  } while (0)
+
+#define CUFFT(call)                                                                         \
+  do {                                                                                      \
+    cufftResult _r = (call);                                                                \
+    if (_r != CUFFT_SUCCESS)                                                                \
+      return fail(_r == CUFFT_ALLOC_FAILED ? GSE_ERR_OOM : GSE_ERR_CUDA,                    \
+                  "%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, (int)_r);          \
+  } while (0)
+
+#define TRY(call)                                                                           \
+  do {                                                                                      \
+    gse_status_t _s = (call);                                                               \
+    if (_s != GSE_OK) return _s;                                                            \
+  } while (0)
+
+constexpr int kEnergyPartials = 148 * 4;
+constexpr int kBrick = 4;
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct gse_context {
+  gse_params_t p;
+  cudaStream_t stream = nullptr;
+  bool fp64 = true;
+  size_t ct = 8;  // sizeof(CT)
+  double sigma1 = 0, sigma2 = 0, rcut1 = 0;
+  long long size = 0;   // real grid points
+  long long ksize = 0;  // complex half-spectrum bins
+  void* d_rho = nullptr;
+  void* d_phi = nullptr;
+  void* d_rhok = nullptr;
+  long long* d_fixed = nullptr;
+  void* d_xyzq = nullptr;
+  void* d_sorted = nullptr;
+  int* d_perm = nullptr;
+  int* d_keys = nullptr;
+  int* d_slots = nullptr;
+  size_t atom_cap = 0;
+  int* d_counts = nullptr;
+  int* d_offsets = nullptr;
+  BinGeom bg{};
+  int nbins = 0;
+  double* d_force = nullptr;  // 3 x atom_cap
+  double* d_partials = nullptr;
+  double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch
+  int* d_bad = nullptr;
+  double* h_pinned = nullptr;  // [0] energy, [1] bad flag
+  cufftHandle plan_f = 0, plan_b = 0;
+  bool plans = false;
+  bool rho_valid = false, phi_valid = false, energy_valid = false;
+};
+
+namespace {
+
+gse_status_t check_ctx(gse_context_t* c) {
+  if (!c) return fail(GSE_ERR_INVALID_ARG, "NULL context");
+  cudaError_t e = cudaSetDevice(c->p.device);
+  if (e != cudaSuccess) return fail(GSE_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return GSE_OK;
+}
+
+double fixed_scale_for(double spread_pref) {
+  // 2^40 fixed-point units per unit density for the default widths; coarser
+  // when a narrow Gaussian makes single contributions large, so that any sum
+  // of up to 2^22 maximal contributions stays inside int64.
+  int k = 40;
+  double m = std::fabs(spread_pref) / 0.05;
+  while (m > 1.0 && k > 8) {
+    m *= 0.5;
+    k--;
+  }
+  return std::ldexp(1.0, k);
+}
+
+template <typename CT>
+Stencil<CT> stencil_of(const gse_context_t* c, const double box[3], double sigma, double rcut,
+                       bool gather, bool normalize) {
+  const int M[3] = {c->p.size_x, c->p.size_y, c->p.size_z};
+  Stencil<CT> s = make_stencil<CT>(M, box, sigma, rcut, gather, normalize, 1.0);
+  s.fixed_scale = fixed_scale_for((double)make_stencil<CT>(M, box, sigma, rcut, false, false, 1.0).pref);
+  return s;
+}
+
+struct Box3 {
+  double v[3];
+};
+Box3 ctx_box(const gse_context_t* c) { return Box3{{c->p.box_x, c->p.box_y, c->p.box_z}}; }
+
+gse_status_t check_stencil(const gse_context_t* c, const double box[3], double sigma,
+                           double rcut) {
+  if (!(sigma > 0.0) || !(rcut > 0.0) || !std::isfinite(sigma) || !std::isfinite(rcut))
+    return fail(GSE_ERR_INVALID_ARG, "sigma and rcut must be positive and finite");
+  for (int d = 0; d < 3; d++)
+    if (!(box[d] > 0.0) || !std::isfinite(box[d]))
+      return fail(GSE_ERR_INVALID_ARG, "box lengths must be positive and finite");
+  const int M[3] = {c->p.size_x, c->p.size_y, c->p.size_z};
+  for (int d = 0; d < 3; d++) {
+    const int n = (int)std::ceil(rcut / (box[d] / (double)M[d]));
+    if (2 * n + 1 > kMaxStencil)
+      return fail(GSE_ERR_STENCIL_TOO_LARGE, "stencil 2n+1=%d exceeds %d on axis %d", 2 * n + 1,
+                  kMaxStencil, d);
+  }
+  return GSE_OK;
+}
+
+gse_status_t ensure_atoms(gse_context_t* c, int n) {
+  if ((size_t)n <= c->atom_cap) return GSE_OK;
+  size_t cap = c->atom_cap ? c->atom_cap : 1024;
+  while (cap < (size_t)n) cap *= 2;
+  cudaFree(c->d_xyzq);
+  cudaFree(c->d_sorted);
+  cudaFree(c->d_perm);
+  cudaFree(c->d_keys);
+  cudaFree(c->d_slots);
+  cudaFree(c->d_force);
+  c->d_xyzq = c->d_sorted = nullptr;
+  c->d_perm = c->d_keys = c->d_slots = nullptr;
+  c->d_force = nullptr;
+  c->atom_cap = 0;
+  const size_t rec = 4 * c->ct;
+  CU(cudaMalloc(&c->d_xyzq, cap * rec));
+  CU(cudaMalloc(&c->d_sorted, cap * rec));
+  CU(cudaMalloc(&c->d_perm, cap * sizeof(int)));
+  CU(cudaMalloc(&c->d_keys, cap * sizeof(int)));
+  CU(cudaMalloc(&c->d_slots, cap * sizeof(int)));
+  CU(cudaMalloc(&c->d_force, 3 * cap * sizeof(double)));
+  c->atom_cap = cap;
+  return GSE_OK;
+}
+
+// Returns a device pointer to the n records (copied in if host memory).
+gse_status_t stage_atoms(gse_context_t* c, int n, const void* xyzq, const void** dptr) {
+  if (n < 0) return fail(GSE_ERR_INVALID_ARG, "negative atom count");
+  if (n > 0 && !xyzq) return fail(GSE_ERR_INVALID_ARG, "NULL xyzq");
+  TRY(ensure_atoms(c, n > 0 ? n : 1));
+  if (n == 0) {
+    *dptr = c->d_xyzq;
+    return GSE_OK;
+  }
+  if (is_device_ptr(xyzq)) {
+    *dptr = xyzq;
+  } else {
+    CU(cudaMemcpyAsync(c->d_xyzq, xyzq, (size_t)n * 4 * c->ct, cudaMemcpyHostToDevice,
+                       c->stream));
+    *dptr = c->d_xyzq;
+  }
+  return GSE_OK;
+}
+
+template <typename CT>
+gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s) {
+  typedef typename Vec4<CT>::type V;
+  CU(launch_bin<CT>((const V*)dx, n, c->bg, s.inv_h[0], s.inv_h[1], s.inv_h[2], c->d_keys,
+                    c->d_slots, c->d_counts, c->d_offsets, (V*)c->d_sorted, c->d_perm, c->d_bad,
+                    c->stream));
+  return GSE_OK;
+}
+
+template <typename CT>
+gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
+                       double rcut, bool normalize) {
+  typedef typename Vec4<CT>::type V;
+  const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
+  CU(launch_spread<CT>((const V*)dx, n, s, (CT*)c->d_rho, c->fp64 ? nullptr : c->d_fixed,
+                       c->stream));
+  c->rho_valid = true;
+  c->phi_valid = false;
+  c->energy_valid = false;
+  return GSE_OK;
+}
+
+template <typename CT>
+gse_status_t do_gather(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
+                       double rcut, const CT* phi, double outscale, double* fx, double* fy,
+                       double* fz) {
+  typedef typename Vec4<CT>::type V;
+  const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, true, false);
+  if (n == 0) return GSE_OK;
+  TRY(bin_atoms<CT>(c, n, dx, s));
+  CU(launch_gather<CT>((const V*)c->d_sorted, c->d_perm, n, s, phi, outscale, fx, fy, fz,
+                       c->stream));
+  return GSE_OK;
+}
+
+GreenGeom green_geom(const gse_context_t* c, double sigma, double bx, double by, double bz,
+                     bool energy) {
+  GreenGeom g;
+  g.nfft[0] = c->p.size_x;
+  g.nfft[1] = c->p.size_y;
+  g.nfft[2] = c->p.size_z;
+  for (int d = 0; d < 3; d++) g.half[d] = g.nfft[d] / 2 + (g.nfft[d] % 2);
+  g.sizeX = g.nfft[0] / 2 + 1;
+  g.nx_even = (g.nfft[0] % 2) == 0;
+  g.want_energy = energy ? 1 : 0;
+  g.twopi_box[0] = 2.0 * kPi / bx;
+  g.twopi_box[1] = 2.0 * kPi / by;
+  g.twopi_box[2] = 2.0 * kPi / bz;
+  g.fourpi_vol = 4.0 * kPi / (double)(g.nfft[0] * g.nfft[1] * g.nfft[2]);
+  g.sigmafac = sigma * sigma / 2.0;
+  return g;
+}
+
+double energy_factor(const gse_context_t* c) {
+  // CpuGSE.cpp:99-102: energy *= ccelec*hx*hy*hz*0.5
+  const double hx = c->p.box_x / (double)c->p.size_x;
+  const double hy = c->p.box_y / (double)c->p.size_y;
+  const double hz = c->p.box_z / (double)c->p.size_z;
+  return c->p.ccelec * hx * hy * hz * 0.5;
+}
+
+gse_status_t fft_forward(gse_context_t* c, const void* rho, void* rhok) {
+  if (c->fp64)
+    CUFFT(cufftExecD2Z(c->plan_f, (cufftDoubleReal*)rho, (cufftDoubleComplex*)rhok));
+  else
+    CUFFT(cufftExecR2C(c->plan_f, (cufftReal*)rho, (cufftComplex*)rhok));
+  return GSE_OK;
+}
+
+gse_status_t fft_backward(gse_context_t* c, void* rhok, void* phi) {
+  if (c->fp64)
+    CUFFT(cufftExecZ2D(c->plan_b, (cufftDoubleComplex*)rhok, (cufftDoubleReal*)phi));
+  else
+    CUFFT(cufftExecC2R(c->plan_b, (cufftComplex*)rhok, (cufftReal*)phi));
+  return GSE_OK;
+}
+
+// phi = c2r(G(sigma) r2c(rho)); optionally the k-space energy into d_scalars[0].
+gse_status_t do_solve(gse_context_t* c, const void* rho, void* phi, double sigma, double bx,
+                      double by, double bz, bool energy) {
+  TRY(fft_forward(c, rho, c->d_rhok));
+  const GreenGeom g = green_geom(c, sigma, bx, by, bz, energy);
+  if (c->fp64)
+    CU(launch_green_energy<double>((double2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
+                                   energy_factor(c), c->d_scalars, c->stream));
+  else
+    CU(launch_green_energy<float>((float2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
+                                  energy_factor(c), c->d_scalars, c->stream));
+  TRY(fft_backward(c, c->d_rhok, phi));
+  return GSE_OK;
+}
+
+// Copy `bytes` from device src to dst (host or device) on the stream.
+gse_status_t copy_out(gse_context_t* c, void* dst, const void* src, size_t bytes, bool* host) {
+  const bool dev = is_device_ptr(dst);
+  CU(cudaMemcpyAsync(dst, src, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     c->stream));
+  if (!dev) *host = true;
+  return GSE_OK;
+}
+
+gse_status_t finish(gse_context_t* c, bool host_outputs) {
+  if (host_outputs) CU(cudaStreamSynchronize(c->stream));
+  CU(cudaGetLastError());
+  return GSE_OK;
+}
+
+// Gather into fx/fy/fz (host or device, any may be NULL).
+template <typename CT>
+gse_status_t gather_to(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
+                       double rcut, const CT* phi, double outscale, double* fx, double* fy,
+                       double* fz, bool* host) {
+  const bool direct = fx && fy && fz && is_device_ptr(fx) && is_device_ptr(fy) && is_device_ptr(fz);
+  if (direct) return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz);
+  double* f = c->d_force;
+  const size_t cap = c->atom_cap;
+  TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + cap, f + 2 * cap));
+  if (n == 0) return GSE_OK;
+  if (fx) TRY(copy_out(c, fx, f, n * sizeof(double), host));
+  if (fy) TRY(copy_out(c, fy, f + cap, n * sizeof(double), host));
+  if (fz) TRY(copy_out(c, fz, f + 2 * cap, n * sizeof(double), host));
+  return GSE_OK;
+}
+
+gse_status_t energy_out(gse_context_t* c, double* energy, bool* host) {
+  if (!energy) return GSE_OK;
+  if (is_device_ptr(energy)) {
+    CU(cudaMemcpyAsync(energy, c->d_scalars, sizeof(double), cudaMemcpyDeviceToDevice,
+                       c->stream));
+  } else {
+    CU(cudaMemcpyAsync(c->h_pinned, c->d_scalars, sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    *energy = c->h_pinned[0];
+    *host = true;
+  }
+  return GSE_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+void gse_params_default(gse_params_t* p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->kappa = 0.4;
+  p->lambda_sigma = 3.0;
+  p->lambda_sigma1 = 3.0;
+  p->ccelec = 332.0716;
+  p->precision = GSE_PRECISION_FP64;
+  p->device = 0;
+}
+
+const char* gse_status_string(gse_status_t s) {
+  switch (s) {
+    case GSE_OK: return "GSE_OK";
+    case GSE_ERR_INVALID_ARG: return "GSE_ERR_INVALID_ARG";
+    case GSE_ERR_STENCIL_TOO_LARGE: return "GSE_ERR_STENCIL_TOO_LARGE";
+    case GSE_ERR_CUDA: return "GSE_ERR_CUDA";
+    case GSE_ERR_OOM: return "GSE_ERR_OOM";
+    case GSE_ERR_TIMEOUT: return "GSE_ERR_TIMEOUT";
+    case GSE_ERR_NOT_READY: return "GSE_ERR_NOT_READY";
+    case GSE_ERR_UNSUPPORTED: return "GSE_ERR_UNSUPPORTED";
+    case GSE_ERR_NONFINITE: return "GSE_ERR_NONFINITE";
+  }
+  return "GSE_ERR_UNKNOWN";
+}
+
+const char* gse_last_error(void) { return g_last_error.c_str(); }
+
+int gse_abi_version(void) { return GSE_B200_ABI_VERSION; }
+
+gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
+  g_last_error.clear();
+  if (!params || !out) return fail(GSE_ERR_INVALID_ARG, "NULL params or out");
+  *out = nullptr;
+  const gse_params_t& p = *params;
+  if (p.size_x < 1 || p.size_y < 1 || p.size_z < 1)
+    return fail(GSE_ERR_INVALID_ARG, "grid sizes must be >= 1");
+  if ((long long)p.size_x * p.size_y * p.size_z > (1LL << 31) - 1)
+    return fail(GSE_ERR_INVALID_ARG, "grid too large for 32-bit FFT plans");
+  if (!(p.kappa >= 0.0 && p.kappa <= 0.5))
+    return fail(GSE_ERR_INVALID_ARG, "kappa must lie in [0, 0.5] (CpuGSE::setParam)");
+  if (!(p.sigma > 0.0) || !(p.box_x > 0.0) || !(p.box_y > 0.0) || !(p.box_z > 0.0) ||
+      !(p.lambda_sigma1 > 0.0))
+    return fail(GSE_ERR_INVALID_ARG, "sigma, lambda_sigma1 and box lengths must be positive");
+  if (p.precision != GSE_PRECISION_FP64 && p.precision != GSE_PRECISION_MIXED)
+    return fail(GSE_ERR_INVALID_ARG, "unknown precision %d", p.precision);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(GSE_ERR_UNSUPPORTED, "no CUDA device");
+  }
+  if (p.device < 0 || p.device >= ndev) return fail(GSE_ERR_INVALID_ARG, "bad device ordinal");
+  CU(cudaSetDevice(p.device));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, p.device));
+  if (prop.major != 10)
+    return fail(GSE_ERR_UNSUPPORTED, "built for sm_100a; device is sm_%d%d", prop.major,
+                prop.minor);
+
+  gse_context_t* c = new gse_context_t();
+  c->p = p;
+  c->fp64 = (p.precision == GSE_PRECISION_FP64);
+  c->ct = c->fp64 ? sizeof(double) : sizeof(float);
+  c->sigma1 = p.sigma * std::sqrt(p.kappa);
+  c->sigma2 = p.sigma * std::sqrt(1.0 - 2.0 * p.kappa);
+  c->rcut1 = p.lambda_sigma1 * std::sqrt(2.0) * c->sigma1;
+  c->size = (long long)p.size_x * p.size_y * p.size_z;
+  c->ksize = (long long)(p.size_x / 2 + 1) * p.size_y * p.size_z;
+  gse_status_t st = check_stencil(c, ctx_box(c).v, c->sigma1, c->rcut1);
+  if (st != GSE_OK) {
+    delete c;
+    return st;
+  }
+  const int M[3] = {p.size_x, p.size_y, p.size_z};
+  for (int d = 0; d < 3; d++) {
+    c->bg.M[d] = M[d];
+    c->bg.B[d] = kBrick;
+    c->bg.nb[d] = (M[d] + kBrick - 1) / kBrick;
+  }
+  c->nbins = c->bg.nb[0] * c->bg.nb[1] * c->bg.nb[2];
+
+  auto bail = [&](gse_status_t s) {
+    gse_destroy(c);
+    return s;
+  };
+#define CUC(call)                                                                           \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return bail(fail(_e == cudaErrorMemoryAllocation ? GSE_ERR_OOM : GSE_ERR_CUDA,        \
+                       "gse_create: %s: %s", #call, cudaGetErrorString(_e)));               \
+  } while (0)
+  CUC(cudaMalloc(&c->d_rho, c->size * c->ct));
+  CUC(cudaMalloc(&c->d_phi, c->size * c->ct));
+  CUC(cudaMalloc(&c->d_rhok, c->ksize * 2 * c->ct));
+  if (!c->fp64) CUC(cudaMalloc(&c->d_fixed, c->size * sizeof(long long)));
+  CUC(cudaMalloc(&c->d_counts, sizeof(int) * c->nbins));
+  CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
+  CUC(cudaMalloc(&c->d_partials, sizeof(double) * kEnergyPartials));
+  CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 4));
+  CUC(cudaMalloc(&c->d_bad, sizeof(int)));
+  CUC(cudaMemset(c->d_bad, 0, sizeof(int)));
+  CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 4));
+  CUC(cudaMallocHost(&c->h_pinned, sizeof(double) * 4));
+#undef CUC
+  if (cufftPlan3d(&c->plan_f, p.size_z, p.size_y, p.size_x, c->fp64 ? CUFFT_D2Z : CUFFT_R2C) !=
+          CUFFT_SUCCESS ||
+      cufftPlan3d(&c->plan_b, p.size_z, p.size_y, p.size_x, c->fp64 ? CUFFT_Z2D : CUFFT_C2R) !=
+          CUFFT_SUCCESS)
+    return bail(fail(GSE_ERR_CUDA, "cufftPlan3d failed"));
+  c->plans = true;
+  if (ensure_atoms(c, 1024) != GSE_OK) return bail(GSE_ERR_OOM);
+  *out = c;
+  return GSE_OK;
+}
+
+gse_status_t gse_destroy(gse_context_t* c) {
+  if (!c) return GSE_OK;
+  cudaSetDevice(c->p.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->plans) {
+    cufftDestroy(c->plan_f);
+    cufftDestroy(c->plan_b);
+  }
+  cudaFree(c->d_rho);
+  cudaFree(c->d_phi);
+  cudaFree(c->d_rhok);
+  cudaFree(c->d_fixed);
+  cudaFree(c->d_xyzq);
+  cudaFree(c->d_sorted);
+  cudaFree(c->d_perm);
+  cudaFree(c->d_keys);
+  cudaFree(c->d_slots);
+  cudaFree(c->d_force);
+  cudaFree(c->d_counts);
+  cudaFree(c->d_offsets);
+  cudaFree(c->d_partials);
+  cudaFree(c->d_scalars);
+  cudaFree(c->d_bad);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  delete c;
+  return GSE_OK;
+}
+
+gse_status_t gse_set_stream(gse_context_t* c, void* stream) {
+  TRY(check_ctx(c));
+  c->stream = (cudaStream_t)stream;
+  CUFFT(cufftSetStream(c->plan_f, c->stream));
+  CUFFT(cufftSetStream(c->plan_b, c->stream));
+  return GSE_OK;
+}
+
+gse_status_t gse_set_box(gse_context_t* c, double bx, double by, double bz) {
+  TRY(check_ctx(c));
+  if (!(bx > 0.0 && by > 0.0 && bz > 0.0)) return fail(GSE_ERR_INVALID_ARG, "box must be > 0");
+  const gse_params_t old = c->p;
+  c->p.box_x = bx;
+  c->p.box_y = by;
+  c->p.box_z = bz;
+  gse_status_t s = check_stencil(c, ctx_box(c).v, c->sigma1, c->rcut1);
+  if (s != GSE_OK) {
+    c->p = old;
+    return s;
+  }
+  c->phi_valid = c->energy_valid = false;
+  return GSE_OK;
+}
+
+gse_status_t gse_synchronize(gse_context_t* c) {
+  TRY(check_ctx(c));
+  CU(cudaStreamSynchronize(c->stream));
+  return GSE_OK;
+}
+
+gse_status_t gse_spread_charge(gse_context_t* c, int n, const void* xyzq) {
+  TRY(check_ctx(c));
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  if (c->fp64)
+    TRY(do_spread<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
+  else
+    TRY(do_spread<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
+  return finish(c, false);
+}
+
+gse_status_t gse_solve_poisson(gse_context_t* c) {
+  TRY(check_ctx(c));
+  if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "solvePoisson before spreadCharge1");
+  TRY(do_solve(c, c->d_rho, c->d_phi, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true));
+  c->phi_valid = true;
+  c->energy_valid = true;
+  return finish(c, false);
+}
+
+gse_status_t gse_calculate_energy(gse_context_t* c, double* energy) {
+  TRY(check_ctx(c));
+  if (!energy) return fail(GSE_ERR_INVALID_ARG, "NULL energy");
+  if (!c->rho_valid || !c->phi_valid)
+    return fail(GSE_ERR_NOT_READY, "calculateEnergy needs rhoS and phiM");
+  if (!c->energy_valid) {
+    if (c->fp64)
+      CU(launch_dot_energy<double>((const double*)c->d_rho, (const double*)c->d_phi, c->size,
+                                   c->d_partials, kEnergyPartials, energy_factor(c),
+                                   c->d_scalars, c->stream));
+    else
+      CU(launch_dot_energy<float>((const float*)c->d_rho, (const float*)c->d_phi, c->size,
+                                  c->d_partials, kEnergyPartials, energy_factor(c), c->d_scalars,
+                                  c->stream));
+    c->energy_valid = true;
+  }
+  bool host = false;
+  TRY(energy_out(c, energy, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_interpolate_force(gse_context_t* c, int n, const void* xyzq, double* fx,
+                                   double* fy, double* fz) {
+  TRY(check_ctx(c));
+  if (n > 0 && (!fx || !fy || !fz)) return fail(GSE_ERR_INVALID_ARG, "NULL force array");
+  if (!c->phi_valid) return fail(GSE_ERR_NOT_READY, "interpolateForce before solvePoisson");
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  bool host = false;
+  if (c->fp64)
+    TRY(gather_to<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const double*)c->d_phi, c->p.ccelec,
+                          fx, fy, fz, &host));
+  else
+    TRY(gather_to<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const float*)c->d_phi, c->p.ccelec, fx,
+                         fy, fz, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
+                         double* fy, double* fz) {
+  TRY(check_ctx(c));
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  bool host = false;
+  if (c->fp64)
+    TRY(do_spread<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
+  else
+    TRY(do_spread<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
+  TRY(do_solve(c, c->d_rho, c->d_phi, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true));
+  c->phi_valid = true;
+  c->energy_valid = true;
+  if (fx || fy || fz) {
+    if (c->fp64)
+      TRY(gather_to<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const double*)c->d_phi, c->p.ccelec,
+                            fx, fy, fz, &host));
+    else
+      TRY(gather_to<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const float*)c->d_phi, c->p.ccelec,
+                           fx, fy, fz, &host));
+  }
+  TRY(energy_out(c, energy, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_get_grid(gse_context_t* c, int which, void* out) {
+  TRY(check_ctx(c));
+  if (!out) return fail(GSE_ERR_INVALID_ARG, "NULL out");
+  const void* src;
+  if (which == GSE_GRID_RHO) {
+    if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "rhoS not computed");
+    src = c->d_rho;
+  } else if (which == GSE_GRID_PHI) {
+    if (!c->phi_valid) return fail(GSE_ERR_NOT_READY, "phiM not computed");
+    src = c->d_phi;
+  } else {
+    return fail(GSE_ERR_INVALID_ARG, "unknown grid id %d", which);
+  }
+  bool host = false;
+  TRY(copy_out(c, out, src, c->size * c->ct, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_set_grid(gse_context_t* c, int which, const void* in) {
+  TRY(check_ctx(c));
+  if (!in) return fail(GSE_ERR_INVALID_ARG, "NULL in");
+  void* dst;
+  if (which == GSE_GRID_RHO)
+    dst = c->d_rho;
+  else if (which == GSE_GRID_PHI)
+    dst = c->d_phi;
+  else
+    return fail(GSE_ERR_INVALID_ARG, "unknown grid id %d", which);
+  CU(cudaMemcpyAsync(dst, in, c->size * c->ct,
+                     is_device_ptr(in) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     c->stream));
+  if (which == GSE_GRID_RHO) {
+    c->rho_valid = true;
+    c->phi_valid = false;
+  } else {
+    c->phi_valid = true;
+  }
+  c->energy_valid = false;
+  return finish(c, true);
+}
+
+gse_status_t gse_gauss_spread(gse_context_t* c, double sigma, double rcut, int n,
+                              const void* xyzq, double bx, double by, double bz, int normalize,
+                              void* rho_out) {
+  TRY(check_ctx(c));
+  const double box[3] = {bx, by, bz};
+  TRY(check_stencil(c, box, sigma, rcut));
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  if (c->fp64)
+    TRY(do_spread<double>(c, n, dx, box, sigma, rcut, normalize != 0));
+  else
+    TRY(do_spread<float>(c, n, dx, box, sigma, rcut, normalize != 0));
+  bool host = false;
+  if (rho_out && rho_out != c->d_rho) TRY(copy_out(c, rho_out, c->d_rho, c->size * c->ct, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_gauss_interpolate(gse_context_t* c, double sigma, double rcut, int n,
+                                   const void* xyzq, double bx, double by, double bz,
+                                   const void* phi, double* fx, double* fy, double* fz) {
+  TRY(check_ctx(c));
+  if (!phi) return fail(GSE_ERR_INVALID_ARG, "NULL phi");
+  if (n > 0 && (!fx || !fy || !fz)) return fail(GSE_ERR_INVALID_ARG, "NULL force array");
+  const double box[3] = {bx, by, bz};
+  TRY(check_stencil(c, box, sigma, rcut));
+  const void* dphi = phi;
+  if (!is_device_ptr(phi)) {
+    CU(cudaMemcpyAsync(c->d_phi, phi, c->size * c->ct, cudaMemcpyHostToDevice, c->stream));
+    c->phi_valid = true;
+    c->energy_valid = false;
+    dphi = c->d_phi;
+  }
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  bool host = false;
+  if (c->fp64)
+    TRY(gather_to<double>(c, n, dx, box, sigma, rcut, (const double*)dphi, 1.0, fx, fy, fz, &host));
+  else
+    TRY(gather_to<float>(c, n, dx, box, sigma, rcut, (const float*)dphi, 1.0, fx, fy, fz, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_green_mul(gse_context_t* c, double sigma, double bx, double by, double bz,
+                           void* rho_k) {
+  TRY(check_ctx(c));
+  if (!rho_k) return fail(GSE_ERR_INVALID_ARG, "NULL rho_k");
+  if (!(sigma >= 0.0) || !(bx > 0 && by > 0 && bz > 0))
+    return fail(GSE_ERR_INVALID_ARG, "bad sigma or box");
+  const bool dev = is_device_ptr(rho_k);
+  void* k = dev ? rho_k : c->d_rhok;
+  const size_t bytes = c->ksize * 2 * c->ct;
+  if (!dev) CU(cudaMemcpyAsync(k, rho_k, bytes, cudaMemcpyHostToDevice, c->stream));
+  const GreenGeom g = green_geom(c, sigma, bx, by, bz, false);
+  if (c->fp64)
+    CU(launch_green_energy<double>((double2*)k, g, c->d_partials, kEnergyPartials, 1.0,
+                                   c->d_scalars + 1, c->stream));
+  else
+    CU(launch_green_energy<float>((float2*)k, g, c->d_partials, kEnergyPartials, 1.0,
+                                  c->d_scalars + 1, c->stream));
+  bool host = false;
+  if (!dev) TRY(copy_out(c, rho_k, k, bytes, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_fft_solve(gse_context_t* c, double sigma, double bx, double by, double bz,
+                           const void* rho, void* phi) {
+  TRY(check_ctx(c));
+  if (!rho || !phi) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  if (!(sigma >= 0.0) || !(bx > 0 && by > 0 && bz > 0))
+    return fail(GSE_ERR_INVALID_ARG, "bad sigma or box");
+  const size_t bytes = c->size * c->ct;
+  const void* drho = rho;
+  if (!is_device_ptr(rho)) {
+    CU(cudaMemcpyAsync(c->d_rho, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+    drho = c->d_rho;
+    c->rho_valid = true;
+  }
+  const bool pdev = is_device_ptr(phi);
+  void* dphi = pdev ? phi : c->d_phi;
+  TRY(do_solve(c, drho, dphi, sigma, bx, by, bz, false));
+  if (dphi == c->d_phi) c->phi_valid = true;
+  c->energy_valid = false;
+  bool host = false;
+  if (!pdev) TRY(copy_out(c, phi, c->d_phi, bytes, &host));
+  return finish(c, host);
+}
+
+}  // extern "C"

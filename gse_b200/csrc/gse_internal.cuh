@@ -1,0 +1,92 @@
+// gse_internal.cuh -- shared types and device helpers of the GSE-k library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+
+namespace gse {
+
+constexpr double kPi = 3.14159265358979323846;  // pi_dbl, TypesGSE.h:24
+constexpr int kMaxStencil = 64;                  // max 2n+1 per axis
+
+template <typename CT> struct Vec4;
+template <> struct Vec4<double> { typedef double4 type; };
+template <> struct Vec4<float> { typedef float4 type; };
+
+template <typename CT> struct Cplx;
+template <> struct Cplx<double> { typedef double2 type; };
+template <> struct Cplx<float> { typedef float2 type; };
+
+// Stencil constants of one spread or gather call, derived on the host exactly
+// as CpuGaussCharge computes them (CpuGaussCharge.cpp:114-128 and :244-258):
+// the spacing and its inverse in double, then cast to CT.
+template <typename CT>
+struct Stencil {
+  int M[3];      // grid sizes
+  int nst[3];    // n = ceil(rcut / h) per axis
+  CT h[3];       // (CT)(box/M)
+  CT inv_h[3];   // (CT)(1.0 / (box/M))
+  CT rcut2;      // (CT)(rcut*rcut)
+  CT inv_2s2;    // (CT)(1/(2 sigma^2))
+  CT pref;       // spread: (CT)(2 pi sigma^2)^(-3/2); gather: (CT)((2 pi)^(-3/2) h^3 sigma^-5)
+  CT norm_pref1; // (CT)sqrt(2 pi sigma^2), used when normalize != 0
+  int normalize;
+  double fixed_scale;  // mixed form: fixed-point units per unit charge density
+};
+
+template <typename CT>
+inline Stencil<CT> make_stencil(const int M[3], const double box[3], double sigma, double rcut,
+                                bool gather, bool normalize, double fixed_scale) {
+  Stencil<CT> s;
+  double hd[3];
+  for (int d = 0; d < 3; d++) {
+    s.M[d] = M[d];
+    hd[d] = box[d] / (double)M[d];
+    s.nst[d] = (int)std::ceil(rcut / hd[d]);
+    s.h[d] = (CT)hd[d];
+    s.inv_h[d] = (CT)(1.0 / hd[d]);
+  }
+  s.rcut2 = (CT)(rcut * rcut);
+  s.inv_2s2 = (CT)(1.0 / (2.0 * sigma * sigma));
+  if (gather)
+    s.pref = (CT)(std::pow(2.0 * kPi, -3.0 / 2.0) * hd[0] * hd[1] * hd[2] * std::pow(sigma, -5.0));
+  else
+    s.pref = (CT)std::pow(2.0 * kPi * sigma * sigma, -3.0 / 2.0);
+  s.norm_pref1 = (CT)std::sqrt(2.0 * kPi * sigma * sigma);
+  s.normalize = normalize ? 1 : 0;
+  s.fixed_scale = fixed_scale;
+  return s;
+}
+
+// ---- round-to-nearest arithmetic that nvcc may not contract into FMAs ----
+// The stencil origin and the spherical cut must be bit-identical to the
+// reference's separately rounded products and sums.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// C round(): halfway cases away from zero (the reference calls round()).
+__device__ __forceinline__ int round_to_int(double v) { return (int)round(v); }
+__device__ __forceinline__ int round_to_int(float v) { return (int)roundf(v); }
+
+__device__ __forceinline__ double gexp(double v) { return exp(v); }
+__device__ __forceinline__ float gexp(float v) { return expf(v); }
+
+__device__ __forceinline__ int pmod(int a, int m) {
+  int r = a % m;
+  return r < 0 ? r + m : r;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace gse

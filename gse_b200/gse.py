@@ -1,0 +1,367 @@
+"""Python mirror of the reference's GSE-k class API, running on the B200.
+
+Class and method names, argument order and meaning follow ap-hynninen/GSE:
+
+  CpuGrid<T>            Grid.h:12-55, CpuGrid.h:17-108  (host container)
+  CpuGaussCharge<AT,CT> CpuGaussCharge.h:11-49
+  CpuGreensFuncGSE<T>   CpuGreensFuncGSE.h:10-19
+  CpuFFTSolver<T>       CpuFFTSolver.h:12-42
+  CpuGSE<AT,CT>/CpuGSEk CpuGSE.h:19-68, CpuGSEk.h:19-37
+
+The template parameters become a ``precision`` argument: "fp64" is
+<double,double>; "mixed" is <double,float> (FP32 xyzq and grids, double
+forces and energies).  Where the reference asserts or exits, these classes
+raise GseError.  Every computation runs in libgse_b200.so on the GPU; there is
+no CPU fallback.
+
+Arrays: xyzq is an (n, 4) array of the calculation type (numpy on the host,
+or a CUDA torch tensor); forceX/Y/Z are float64 arrays of length n written in
+place (numpy or CUDA torch tensors).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import GseError, check, ptr
+
+CCELEC = 332.0716
+
+
+def _ct(precision: str):
+    if precision not in _lib.PRECISION:
+        raise GseError(1, f"unknown precision {precision!r} (use 'fp64' or 'mixed')")
+    return np.float64 if precision == "fp64" else np.float32
+
+
+class Context:
+    """Owner of one gse_context_t (grids, FFT plans, staging buffers)."""
+
+    def __init__(self, sizeX, sizeY, sizeZ, sigma=1.0, kappa=0.4, lambdaSigma=3.0,
+                 lambdaSigma1=3.0, boxx=1.0, boxy=1.0, boxz=1.0, ccelec=CCELEC,
+                 precision="fp64", device=0):
+        L = _lib.load()
+        p = _lib.gse_params_t()
+        L.gse_params_default(ctypes.byref(p))
+        p.size_x, p.size_y, p.size_z = int(sizeX), int(sizeY), int(sizeZ)
+        p.sigma, p.kappa = float(sigma), float(kappa)
+        p.lambda_sigma, p.lambda_sigma1 = float(lambdaSigma), float(lambdaSigma1)
+        p.box_x, p.box_y, p.box_z = float(boxx), float(boxy), float(boxz)
+        p.ccelec = float(ccelec)
+        _ct(precision)
+        p.precision = _lib.PRECISION[precision]
+        p.device = int(device)
+        h = ctypes.c_void_p()
+        check(L.gse_create(ctypes.byref(p), ctypes.byref(h)))
+        self._L = L
+        self.h = h
+        self.params = p
+        self.precision = precision
+        self.dtype = _ct(precision)
+        self.shape = (int(sizeZ), int(sizeY), int(sizeX))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self._L.gse_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- thin wrappers of the C ABI ---------------------------------------
+    def set_stream(self, stream_handle: int):
+        check(self._L.gse_set_stream(self.h, stream_handle))
+
+    def set_box(self, bx, by, bz):
+        check(self._L.gse_set_box(self.h, bx, by, bz))
+
+    def synchronize(self):
+        check(self._L.gse_synchronize(self.h))
+
+    def spread_charge(self, n, xyzq):
+        check(self._L.gse_spread_charge(self.h, int(n), ptr(xyzq)))
+
+    def solve_poisson(self):
+        check(self._L.gse_solve_poisson(self.h))
+
+    def calculate_energy(self, out=None) -> float:
+        if out is not None:
+            check(self._L.gse_calculate_energy(self.h, ptr(out)))
+            return None
+        e = ctypes.c_double()
+        check(self._L.gse_calculate_energy(self.h, ctypes.addressof(e)))
+        return e.value
+
+    def interpolate_force(self, n, xyzq, fx, fy, fz):
+        check(self._L.gse_interpolate_force(self.h, int(n), ptr(xyzq), ptr(fx), ptr(fy), ptr(fz)))
+
+    def forward(self, n, xyzq, fx=None, fy=None, fz=None, energy_out=None) -> Optional[float]:
+        if energy_out is not None:
+            check(self._L.gse_forward(self.h, int(n), ptr(xyzq), ptr(energy_out), ptr(fx), ptr(fy),
+                                      ptr(fz)))
+            return None
+        e = ctypes.c_double()
+        check(self._L.gse_forward(self.h, int(n), ptr(xyzq), ctypes.addressof(e), ptr(fx),
+                                  ptr(fy), ptr(fz)))
+        return e.value
+
+    def get_grid(self, which, out=None):
+        if out is None:
+            out = np.empty(self.shape, dtype=self.dtype)
+        check(self._L.gse_get_grid(self.h, int(which), ptr(out)))
+        return out
+
+    def set_grid(self, which, data):
+        a = data
+        if isinstance(data, np.ndarray):
+            a = np.ascontiguousarray(data, dtype=self.dtype)
+        check(self._L.gse_set_grid(self.h, int(which), ptr(a)))
+
+    def gauss_spread(self, sigma, rcut, n, xyzq, boxx, boxy, boxz, normalize, rho_out):
+        check(self._L.gse_gauss_spread(self.h, sigma, rcut, int(n), ptr(xyzq), boxx, boxy, boxz,
+                                       int(bool(normalize)), ptr(rho_out)))
+
+    def gauss_interpolate(self, sigma, rcut, n, xyzq, boxx, boxy, boxz, phi, fx, fy, fz):
+        check(self._L.gse_gauss_interpolate(self.h, sigma, rcut, int(n), ptr(xyzq), boxx, boxy,
+                                            boxz, ptr(phi), ptr(fx), ptr(fy), ptr(fz)))
+
+    def green_mul(self, sigma, boxx, boxy, boxz, rho_k):
+        check(self._L.gse_green_mul(self.h, sigma, boxx, boxy, boxz, ptr(rho_k)))
+
+    def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
+        check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
+
+
+def _xyzq_arg(xyzq, dtype):
+    if isinstance(xyzq, np.ndarray):
+        a = np.ascontiguousarray(xyzq, dtype=dtype)
+        if a.ndim != 2 or a.shape[1] != 4:
+            a = a.reshape(-1, 4)
+        return a
+    return xyzq  # device tensor: caller guarantees dtype/layout
+
+
+# ---------------------------------------------------------------------------
+# Reference API mirror
+# ---------------------------------------------------------------------------
+class CpuGrid:
+    """Host grid of sizeX x sizeY x sizeZ values, x fastest (CpuGrid.h:17-108)."""
+
+    def __init__(self, sizeX, sizeY, sizeZ, dtype=np.float64):
+        self.sizeX, self.sizeY, self.sizeZ = int(sizeX), int(sizeY), int(sizeZ)
+        self.size = self.sizeX * self.sizeY * self.sizeZ
+        self.data = np.zeros((self.sizeZ, self.sizeY, self.sizeX), dtype=dtype)
+
+    def getDataPointer(self):
+        return self.data
+
+    def getSizeX(self):
+        return self.sizeX
+
+    def getSizeY(self):
+        return self.sizeY
+
+    def getSizeZ(self):
+        return self.sizeZ
+
+    def getSize(self):
+        return self.size
+
+    def getPos(self, x, y, z):
+        return (x % self.sizeX) + ((y % self.sizeY) + (z % self.sizeZ) * self.sizeY) * self.sizeX
+
+    def clear(self):
+        self.data[...] = 0
+
+    def add(self, other):
+        self.data += other.data
+
+    def sub(self, other):
+        self.data -= other.data.astype(self.data.dtype)
+
+    def copy(self, other):
+        self.data[...] = other.data.astype(self.data.dtype)
+
+    def scale(self, val):
+        self.data *= val
+
+    def sum(self):
+        return self.data.sum()
+
+    def maxAbsValue(self):
+        return np.abs(self.data).max()
+
+    def getDataValue(self, x, y, z):
+        return self.data[z % self.sizeZ, y % self.sizeY, x % self.sizeX]
+
+    def save(self, filename):
+        """One value per line, z outermost (CpuGrid.h:76-106)."""
+        with open(filename, "w") as f:
+            for v in self.data.reshape(-1):
+                f.write(f"{v:g}\n")
+
+
+class CpuGaussCharge:
+    """CpuGaussCharge<AT,CT> (CpuGaussCharge.h:11-49) on the GPU."""
+
+    def __init__(self, sizeX, sizeY, sizeZ, precision="fp64", device=0):
+        self.sizeX, self.sizeY, self.sizeZ = int(sizeX), int(sizeY), int(sizeZ)
+        self.precision = precision
+        self.dtype = _ct(precision)
+        self._ctx = Context(sizeX, sizeY, sizeZ, sigma=1.0, precision=precision, device=device)
+
+    def _check(self, grid: CpuGrid):
+        if (grid.sizeX, grid.sizeY, grid.sizeZ) != (self.sizeX, self.sizeY, self.sizeZ):
+            raise GseError(1, "grid size mismatch (CpuGaussCharge.cpp:240-242)")
+
+    def spreadChargeToGrid(self, sigma, rcut, numCoord, xyzq, boxx, boxy, boxz, rho: CpuGrid,
+                           normalize=False):
+        self._check(rho)
+        if rho.data.dtype != self.dtype:
+            raise GseError(1, "rho grid dtype does not match precision")
+        self._ctx.gauss_spread(sigma, rcut, numCoord, _xyzq_arg(xyzq, self.dtype), boxx, boxy,
+                               boxz, normalize, rho.data)
+
+    def interpolateForce(self, sigma, rcut, numCoord, xyzq, boxx, boxy, boxz, phi: CpuGrid,
+                         forceX, forceY, forceZ):
+        self._check(phi)
+        ph = np.ascontiguousarray(phi.data, dtype=self.dtype)
+        self._ctx.gauss_interpolate(sigma, rcut, numCoord, _xyzq_arg(xyzq, self.dtype), boxx,
+                                    boxy, boxz, ph, forceX, forceY, forceZ)
+
+    def calcSupportSize(self, rcut, boxx, boxy, boxz):
+        """Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56)."""
+        h = np.array([boxx / self.sizeX, boxy / self.sizeY, boxz / self.sizeZ])
+        n = np.ceil(rcut / h).astype(int)
+        t = [(np.abs(np.arange(-k, k + 1)) - 1) * hh for k, hh in zip(n, h)]
+        r2 = t[0][None, None, :] ** 2 + t[1][None, :, None] ** 2 + t[2][:, None, None] ** 2
+        return int(np.count_nonzero(r2 < rcut * rcut))
+
+
+class CpuGreensFunc:
+    """Base class (CpuGreensFunc.h:10-19)."""
+
+    def mul(self, nfftX, nfftY, nfftZ, boxx, boxy, boxz, sigma, rho):
+        raise NotImplementedError
+
+
+class CpuGreensFuncGSE(CpuGreensFunc):
+    """CpuGreensFuncGSE<T>::mul (CpuGreensFuncGSE.cpp:9-57) on the GPU.
+
+    ``rho`` is the k-space grid, a CpuGrid of ((nfftX/2+1)*2, nfftY, nfftZ)
+    reals holding interleaved complex values."""
+
+    def __init__(self, precision="fp64", device=0):
+        self.precision = precision
+        self.device = device
+        self._ctx = None
+
+    def _context(self, nx, ny, nz):
+        if self._ctx is None or self._ctx.shape != (nz, ny, nx):
+            self._ctx = Context(nx, ny, nz, precision=self.precision, device=self.device)
+        return self._ctx
+
+    def mul(self, nfftX, nfftY, nfftZ, boxx, boxy, boxz, sigma, rho: CpuGrid):
+        if (nfftX // 2 + 1) * 2 != rho.sizeX or nfftY != rho.sizeY or nfftZ != rho.sizeZ:
+            raise GseError(1, "k-space grid size mismatch (CpuGreensFuncGSE.cpp:13-15)")
+        ctx = self._context(nfftX, nfftY, nfftZ)
+        if rho.data.dtype != ctx.dtype:
+            raise GseError(1, "k-space grid dtype does not match precision")
+        ctx.green_mul(sigma, boxx, boxy, boxz, rho.data)
+
+
+class CpuFFTSolver:
+    """CpuFFTSolver<T> (CpuFFTSolver.h:12-42): phi = c2r(G r2c(rho))."""
+
+    def __init__(self, greensFunc: CpuGreensFuncGSE, sizeX, sizeY, sizeZ):
+        if not isinstance(greensFunc, CpuGreensFuncGSE):
+            raise GseError(7, "only the GSE Green's function is implemented on the GPU")
+        self.greensFunc = greensFunc
+        self.sizeX, self.sizeY, self.sizeZ = int(sizeX), int(sizeY), int(sizeZ)
+        self._ctx = Context(sizeX, sizeY, sizeZ, precision=greensFunc.precision,
+                            device=greensFunc.device)
+
+    def run(self, phi: CpuGrid, rho: CpuGrid, sigma, boxx, boxy, boxz):
+        for g in (phi, rho):
+            if (g.sizeX, g.sizeY, g.sizeZ) != (self.sizeX, self.sizeY, self.sizeZ):
+                raise GseError(1, "grid size mismatch (CpuFFTSolver.cpp:78-83)")
+        r = np.ascontiguousarray(rho.data, dtype=self._ctx.dtype)
+        self._ctx.fft_solve(sigma, boxx, boxy, boxz, r, phi.data)
+
+
+class CpuGSE:
+    """Common base of the GSE drivers (CpuGSE.h:19-68)."""
+
+    def __init__(self, sizeX, sizeY, sizeZ, sigma, kappa, lambdaSigma, lambdaSigma1, boxx, boxy,
+                 boxz, ccelec=CCELEC, precision="fp64", device=0):
+        if not (0.0 <= kappa <= 0.5):
+            raise GseError(1, "kappa must lie in [0, 0.5] (CpuGSE.cpp:35-36)")
+        self.ccelec = ccelec
+        self.sigma, self.kappa = sigma, kappa
+        self.lambdaSigma, self.lambdaSigma1 = lambdaSigma, lambdaSigma1
+        self.sigma1 = sigma * np.sqrt(kappa)
+        self.sigma2 = sigma * np.sqrt(1.0 - 2.0 * kappa)
+        self.boxx, self.boxy, self.boxz = boxx, boxy, boxz
+        self.precision = precision
+        self.dtype = _ct(precision)
+        self._ctx = Context(sizeX, sizeY, sizeZ, sigma, kappa, lambdaSigma, lambdaSigma1, boxx,
+                            boxy, boxz, ccelec, precision, device)
+        self.rhoS = CpuGrid(sizeX, sizeY, sizeZ, self.dtype)
+        self.phiM = CpuGrid(sizeX, sizeY, sizeZ, self.dtype)
+
+    def printInfo(self):
+        g = self.rhoS
+        print(f"sizeX={g.sizeX} sizeY={g.sizeY} sizeZ={g.sizeZ}")
+        print(f"sigma={self.sigma} sigma1={self.sigma1} sigma2={self.sigma2} kappa={self.kappa}")
+        print(f"lambdaSigma1={self.lambdaSigma1} lambdaSigma={self.lambdaSigma}")
+
+    def setBoxSize(self, boxx, boxy, boxz):
+        self._ctx.set_box(boxx, boxy, boxz)
+        self.boxx, self.boxy, self.boxz = boxx, boxy, boxz
+
+    def interpolateForce(self, numCoord, xyzq, forceX, forceY, forceZ):
+        self._ctx.interpolate_force(numCoord, _xyzq_arg(xyzq, self.dtype), forceX, forceY, forceZ)
+
+    def getRhoS(self) -> CpuGrid:
+        self._ctx.get_grid(_lib.GRID_RHO, self.rhoS.data)
+        return self.rhoS
+
+    def getPhi(self) -> CpuGrid:
+        self._ctx.get_grid(_lib.GRID_PHI, self.phiM.data)
+        return self.phiM
+
+    def getSigma1(self):
+        return self.sigma1
+
+    def getSigma2(self):
+        return self.sigma2
+
+    def getLambdaSigma1(self):
+        return self.lambdaSigma1
+
+    @property
+    def context(self) -> Context:
+        return self._ctx
+
+
+class CpuGSEk(CpuGSE):
+    """CpuGSEk<AT,CT> (CpuGSEk.h:19-37, CpuGSEk.cpp:30-58) on the GPU."""
+
+    def spreadCharge1(self, numCoord, xyzq):
+        self._ctx.spread_charge(numCoord, _xyzq_arg(xyzq, self.dtype))
+
+    def solvePoisson(self):
+        self._ctx.solve_poisson()
+
+    def calculateEnergy(self) -> float:
+        return self._ctx.calculate_energy()
+
+    def forward(self, numCoord, xyzq, forceX=None, forceY=None, forceZ=None) -> float:
+        """spreadCharge1 + solvePoisson + calculateEnergy + interpolateForce in one call."""
+        return self._ctx.forward(numCoord, _xyzq_arg(xyzq, self.dtype), forceX, forceY, forceZ)

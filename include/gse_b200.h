@@ -1,0 +1,179 @@
+/*
+ * gse_b200.h -- C ABI of the B200-native GSE-k reciprocal-space library.
+ *
+ * The library computes Gaussian-Split-Ewald k-space electrostatics on one
+ * NVIDIA B200 (sm_100a): Gaussian charge spreading onto a periodic grid, the
+ * k-space Green's-function multiply around a 3-D real FFT, the mesh energy,
+ * and the Gaussian gather of forces.  Every entry point below replaces one
+ * public method of the reference classes of ap-hynninen/GSE (paths relative
+ * to that project); the C++ drop-in classes in gse_b200/cxx/ and the Python
+ * mirror in gse_b200/gse.py forward to these functions.
+ *
+ * Conventions
+ *  - Every call returns a gse_status_t; GSE_OK is 0.  The library never
+ *    calls exit() or abort().  gse_last_error() describes the last failure
+ *    on the calling thread.
+ *  - Grids are x-fastest, index x + (y + z*size_y)*size_x, periodic, as
+ *    Grid<T>::getPos (Grid.h:32-44).
+ *  - Positions/charges are AoS records {x, y, z, q} of the calculation type
+ *    CT: double for GSE_PRECISION_FP64 (xyzq_t<double>), float for
+ *    GSE_PRECISION_MIXED (xyzq_t<float>) (TypesGSE.h:19-22).
+ *  - Forces and energies are double (the accumulation type AT of both
+ *    reference instances <double,double> and <double,float>).
+ *  - A pointer argument may be host memory (pageable or pinned) or device
+ *    memory of the context's device; the library inspects it.  Calls whose
+ *    outputs are host memory return after the results are written; calls
+ *    whose outputs are all device memory are asynchronous on the context's
+ *    stream.
+ *  - A context is not re-entrant: calls on one context must not overlap.
+ *    Independent contexts may be used from different threads.
+ */
+#ifndef GSE_B200_H
+#define GSE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSE_B200_ABI_VERSION 1
+
+typedef enum gse_status {
+  GSE_OK = 0,
+  GSE_ERR_INVALID_ARG = 1,       /* bad size, NULL pointer, kappa outside [0, 0.5] ... */
+  GSE_ERR_STENCIL_TOO_LARGE = 2, /* 2n+1 > grid size along an axis */
+  GSE_ERR_CUDA = 3,              /* a CUDA runtime / cuFFT call failed */
+  GSE_ERR_OOM = 4,               /* device or pinned allocation failed */
+  GSE_ERR_TIMEOUT = 5,           /* a bounded device-side wait gave up */
+  GSE_ERR_NOT_READY = 6,         /* stage called out of order (e.g. energy before solve) */
+  GSE_ERR_UNSUPPORTED = 7,       /* no GPU, wrong architecture, or feature not built */
+  GSE_ERR_NONFINITE = 8          /* a position or charge is NaN/Inf */
+} gse_status_t;
+
+typedef enum gse_precision {
+  /* plain form: FP64 everywhere (CpuGSEk<double,double>) */
+  GSE_PRECISION_FP64 = 0,
+  /* mixed form: FP32 positions, stencils and FFT; deterministic int64
+   * fixed-point grid accumulation; FP64 Green's-function factors, energy
+   * reduction and force accumulation output (CpuGSEk<double,float>) */
+  GSE_PRECISION_MIXED = 1
+} gse_precision_t;
+
+typedef enum gse_grid_id {
+  GSE_GRID_RHO = 0, /* rhoS: spread charge density (CpuGSE::getRhoS, CpuGSE.h:63) */
+  GSE_GRID_PHI = 1  /* phiM: mesh potential (CpuGSE::getPhi, CpuGSE.h:64) */
+} gse_grid_id_t;
+
+typedef struct gse_params {
+  int size_x, size_y, size_z; /* grid points per side (sizeX/Y/Z) */
+  double sigma;               /* total Gaussian width */
+  double kappa;               /* split: sigma1 = sigma sqrt(kappa), sigma2 = sigma sqrt(1-2 kappa) */
+  double lambda_sigma;        /* kept for API parity (CpuGSE.h:52-54); unused by GSE-k */
+  double lambda_sigma1;       /* gather/spread cut-off rcut = lambda_sigma1 sqrt(2) sigma1 */
+  double box_x, box_y, box_z; /* orthorhombic box lengths */
+  double ccelec;              /* unit conversion, CHARMM 332.0716 by default */
+  int precision;              /* gse_precision_t */
+  int device;                 /* CUDA device ordinal */
+} gse_params_t;
+
+typedef struct gse_context gse_context_t;
+
+/* Fill *p with the reference drivers' defaults: kappa 0.4, lambda_sigma and
+ * lambda_sigma1 3.0, ccelec 332.0716 (cpu_gse.cpp:424-426, CpuGSE.h:55),
+ * FP64 precision, device 0.  Sizes, sigma and box must still be set. */
+void gse_params_default(gse_params_t* p);
+
+const char* gse_status_string(gse_status_t s);
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* gse_last_error(void);
+
+int gse_abi_version(void);
+
+/* ---- context lifetime ------------------------------------------------- */
+
+/* Replaces the constructors CpuGSE(...) / CpuGSEk(...) (CpuGSE.cpp:11-19,
+ * CpuGSEk.cpp:14-22) including CpuGSE::setParam's kappa check
+ * (CpuGSE.cpp:33-44; the reference asserts, this returns
+ * GSE_ERR_INVALID_ARG).  Allocates the grids and FFT plans on the device. */
+gse_status_t gse_create(const gse_params_t* params, gse_context_t** out);
+
+/* Replaces ~CpuGSEk / ~CpuFFTSolver (CpuFFTSolver.cpp:18-21). */
+gse_status_t gse_destroy(gse_context_t* ctx);
+
+/* Run all following work of this context on `cuda_stream` (a cudaStream_t;
+ * NULL selects the legacy default stream). */
+gse_status_t gse_set_stream(gse_context_t* ctx, void* cuda_stream);
+
+/* Replaces CpuGSE::setBoxSize (CpuGSE.cpp:58-64). */
+gse_status_t gse_set_box(gse_context_t* ctx, double box_x, double box_y, double box_z);
+
+/* Block until the context's queued work has finished. */
+gse_status_t gse_synchronize(gse_context_t* ctx);
+
+/* ---- CpuGSEk method equivalents ---------------------------------------- */
+
+/* CpuGSEk::spreadCharge1 (CpuGSEk.cpp:30-33): spread the n charges with
+ * sigma1 and rcut1 onto the context's rhoS grid (cleared first). */
+gse_status_t gse_spread_charge(gse_context_t* ctx, int n, const void* xyzq);
+
+/* CpuGSEk::solvePoisson (CpuGSEk.cpp:48-50) = CpuFFTSolver::run
+ * (CpuFFTSolver.cpp:75-96): phiM = c2r( G(sigma2) * r2c(rhoS) ). */
+gse_status_t gse_solve_poisson(gse_context_t* ctx);
+
+/* CpuGSEk::calculateEnergy (CpuGSEk.cpp:56-58, CpuGSE.cpp:86-103):
+ * 1/2 ccelec hx hy hz sum rhoS*phiM.  `energy` may be host or device. */
+gse_status_t gse_calculate_energy(gse_context_t* ctx, double* energy);
+
+/* CpuGSE::interpolateForce (CpuGSE.cpp:70-80): gather with sigma1 and a
+ * spherical cut rcut1 from phiM, times ccelec.  Outputs are overwritten. */
+gse_status_t gse_interpolate_force(gse_context_t* ctx, int n, const void* xyzq, double* fx,
+                                   double* fy, double* fz);
+
+/* One whole force evaluation: spreadCharge1 -> solvePoisson ->
+ * calculateEnergy -> interpolateForce, as cpu_gse runs them
+ * (cpu_gse.cpp:440-455).  `energy` and the force arrays may be NULL to skip
+ * them. */
+gse_status_t gse_forward(gse_context_t* ctx, int n, const void* xyzq, double* energy, double* fx,
+                         double* fy, double* fz);
+
+/* Copy the rhoS or phiM grid (CT elements, size_x*size_y*size_z) out to
+ * host or device memory (CpuGSE::getRhoS / getPhi, CpuGSE.h:63-64). */
+gse_status_t gse_get_grid(gse_context_t* ctx, int which, void* out);
+
+/* Load a grid into the context (e.g. a potential to gather from). */
+gse_status_t gse_set_grid(gse_context_t* ctx, int which, const void* in);
+
+/* ---- stage entry points with explicit parameters ------------------------ */
+
+/* CpuGaussCharge<AT,CT>::spreadChargeToGrid (CpuGaussCharge.cpp:235-384):
+ * full (2n+1)^3 cube, n = ceil(rcut/h), weights exp(-d^2/(2 sigma^2)),
+ * prefactor (2 pi sigma^2)^(-3/2); with normalize != 0 each 1-D weight row
+ * is rescaled to sum to sqrt(2 pi sigma^2).  rho_out (CT, host or device)
+ * receives the grid; the context's rhoS is also updated. */
+gse_status_t gse_gauss_spread(gse_context_t* ctx, double sigma, double rcut, int n,
+                              const void* xyzq, double box_x, double box_y, double box_z,
+                              int normalize, void* rho_out);
+
+/* CpuGaussCharge<AT,CT>::interpolateForce (CpuGaussCharge.cpp:105-183):
+ * sum over grid points with r^2 < rcut^2 of
+ * q (2 pi)^(-3/2) h^3 sigma^(-5) exp(-r^2/(2 sigma^2)) phi (x - x_p), without
+ * the ccelec factor.  phi (CT) may be host or device. */
+gse_status_t gse_gauss_interpolate(gse_context_t* ctx, double sigma, double rcut, int n,
+                                   const void* xyzq, double box_x, double box_y, double box_z,
+                                   const void* phi, double* fx, double* fy, double* fz);
+
+/* CpuGreensFuncGSE<T>::mul (CpuGreensFuncGSE.cpp:9-57), in place on an
+ * interleaved complex half spectrum of ((size_x/2+1)*2) x size_y x size_z CT
+ * values (host or device). */
+gse_status_t gse_green_mul(gse_context_t* ctx, double sigma, double box_x, double box_y,
+                           double box_z, void* rho_k);
+
+/* CpuFFTSolver<T>::run (CpuFFTSolver.cpp:75-96) with the GSE Green's
+ * function: phi = c2r(G(sigma) r2c(rho)).  rho and phi are CT grids. */
+gse_status_t gse_fft_solve(gse_context_t* ctx, double sigma, double box_x, double box_y,
+                           double box_z, const void* rho, void* phi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSE_B200_H */

@@ -1,0 +1,116 @@
+"""The C-ABI library: it loads on a CPU-only host, exports every symbol the
+header declares, and fails cleanly (a status, never a crash) without a GPU."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(gse_[a-z0-9_]+)\s*\(", text))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from gse_b200 import _lib, build
+    build.build_lib()
+    return _lib.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in sorted(header_functions()):
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header():
+    from gse_b200 import _lib
+    assert set(_lib.SIGNATURES) == header_functions()
+
+
+def test_params_default_and_strings(lib):
+    from gse_b200 import _lib
+    p = _lib.gse_params_t()
+    lib.gse_params_default(ctypes.byref(p))
+    assert p.kappa == 0.4 and p.lambda_sigma == 3.0 and p.lambda_sigma1 == 3.0
+    assert p.ccelec == 332.0716 and p.precision == 0 and p.device == 0
+    for code, name in _lib.STATUS_NAMES.items():
+        assert lib.gse_status_string(code).decode() == name
+    assert lib.gse_abi_version() == 1
+
+
+def test_create_rejects_bad_params_before_touching_a_gpu(lib):
+    from gse_b200 import _lib
+    p = _lib.gse_params_t()
+    lib.gse_params_default(ctypes.byref(p))
+    h = ctypes.c_void_p()
+    # sizes unset
+    assert lib.gse_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    p.size_x = p.size_y = p.size_z = 8
+    p.sigma, p.box_x, p.box_y, p.box_z = 2.0, 8.0, 8.0, 8.0
+    p.kappa = 0.7  # CpuGSE::setParam asserts kappa <= 0.5
+    assert lib.gse_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    assert "kappa" in lib.gse_last_error().decode()
+    assert not h.value
+
+
+def test_create_without_gpu_reports_unsupported(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from gse_b200 import _lib
+    p = _lib.gse_params_t()
+    lib.gse_params_default(ctypes.byref(p))
+    p.size_x = p.size_y = p.size_z = 8
+    p.sigma, p.box_x, p.box_y, p.box_z = 2.0, 8.0, 8.0, 8.0
+    h = ctypes.c_void_p()
+    assert lib.gse_create(ctypes.byref(p), ctypes.byref(h)) == 7
+    assert not h.value
+
+
+def test_null_context_is_an_error(lib):
+    assert lib.gse_solve_poisson(None) == 1
+    assert lib.gse_destroy(None) == 0
+
+
+def test_python_mirror_has_reference_methods():
+    from gse_b200 import gse
+    for cls, methods in {
+        gse.CpuGSEk: ["spreadCharge1", "solvePoisson", "calculateEnergy", "interpolateForce",
+                      "getRhoS", "getPhi", "getSigma1", "getSigma2", "getLambdaSigma1",
+                      "setBoxSize", "printInfo"],
+        gse.CpuGaussCharge: ["spreadChargeToGrid", "interpolateForce", "calcSupportSize"],
+        gse.CpuGreensFuncGSE: ["mul"],
+        gse.CpuFFTSolver: ["run"],
+        gse.CpuGrid: ["clear", "add", "sub", "copy", "scale", "sum", "maxAbsValue",
+                      "getDataValue", "save", "getPos", "getDataPointer"],
+    }.items():
+        for m in methods:
+            assert callable(getattr(cls, m)), (cls, m)
+
+
+def test_support_size_matches_reference_formula():
+    """calcSupportSize (CpuGaussCharge.cpp:28-56) is host arithmetic."""
+    from gse_b200 import gse
+    import numpy as np
+    g = gse.CpuGaussCharge.__new__(gse.CpuGaussCharge)
+    g.sizeX = g.sizeY = g.sizeZ = 20
+    # brute force the reference's loop
+    h = 1.0
+    rcut = 3 * np.sqrt(2.0) * 2.121320344 * np.sqrt(0.4)
+    n = int(np.ceil(rcut / h))
+    cnt = 0
+    for tz in range(-n, n + 1):
+        for ty in range(-n, n + 1):
+            for tx in range(-n, n + 1):
+                dx, dy, dz = (abs(tx) - 1) * h, (abs(ty) - 1) * h, (abs(tz) - 1) * h
+                cnt += (dx * dx + dy * dy + dz * dz) < rcut * rcut
+    assert g.calcSupportSize(rcut, 20.0, 20.0, 20.0) == cnt

@@ -1,0 +1,189 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Tolerances:
+  FP64 form   forces: relative RMS <= 1e-12 (Erms, cpu_gse.cpp:131-146);
+              energy: relative <= 1e-12; grids: max |diff| <= 1e-12 max |grid|.
+  mixed form  forces: relative RMS <= 1e-5 against the FP64 reference;
+              energy: relative <= 1e-5; the int64 grid accumulation makes two
+              runs bit-identical.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_goldens
+
+pytestmark = pytest.mark.gpu
+
+CASES = sorted(load_goldens().keys())
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-5
+
+
+def rms(F, R):
+    d = np.asarray(F, np.float64) - np.asarray(R, np.float64)
+    return float(np.sqrt((d * d).sum() / (np.asarray(R, np.float64) ** 2).sum()))
+
+
+def rel(a, b):
+    return abs(a - b) / abs(b)
+
+
+def run_gsek(g, precision):
+    from gse_b200.gse import CpuGSEk
+    M, box, sigma = tuple(int(v) for v in g["M"]), tuple(float(v) for v in g["box"]), float(g["sigma"])
+    ct = np.float64 if precision == "fp64" else np.float32
+    xyzq = g["xyzq"].astype(ct)
+    n = xyzq.shape[0]
+    gs = CpuGSEk(M[0], M[1], M[2], sigma, 0.4, 3.0, 3.0, box[0], box[1], box[2],
+                 precision=precision)
+    gs.spreadCharge1(n, xyzq)
+    gs.solvePoisson()
+    E = gs.calculateEnergy()
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    gs.interpolateForce(n, xyzq, fx, fy, fz)
+    F = np.stack([fx, fy, fz], axis=1)
+    return gs, E, F
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp64_matches_reference(goldens, case):
+    g = goldens[case]
+    gs, E, F = run_gsek(g, "fp64")
+    rho = gs.getRhoS().data
+    phi = gs.getPhi().data
+    assert np.abs(rho - g["rhoS"]).max() <= FP64_TOL * np.abs(g["rhoS"]).max()
+    assert np.abs(phi - g["phi"]).max() <= FP64_TOL * np.abs(g["phi"]).max()
+    print(case, "fp64 force rms", rms(F, g["F"]), "energy rel", rel(E, float(g["E"])))
+    assert rms(F, g["F"]) <= FP64_TOL
+    assert rel(E, float(g["E"])) <= FP64_TOL
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mixed_matches_reference(goldens, case):
+    g = goldens[case]
+    _, E, F = run_gsek(g, "mixed")
+    print(case, "mixed force rms", rms(F, g["F"]), "energy rel", rel(E, float(g["E"])))
+    assert rms(F, g["F"]) <= MIXED_TOL
+    assert rel(E, float(g["E"])) <= MIXED_TOL
+
+
+def test_water_23559_fp64_and_mixed():
+    from gse_b200 import workloads as W
+    z = np.load(os.path.join(GOLDEN, "water_23559.npz"))
+    s = W.config_water_23k()
+    g = {"M": np.array(s.grid), "box": np.array(s.boxes), "sigma": np.array(s.sigma),
+         "xyzq": s.xyzq.astype(np.float64)}
+    _, E, F = run_gsek(g, "fp64")
+    print("water23559 fp64", rms(F, z["F"]), rel(E, float(z["E"])))
+    assert rms(F, z["F"]) <= FP64_TOL
+    assert rel(E, float(z["E"])) <= FP64_TOL
+    g["xyzq"] = s.xyzq
+    _, Em, Fm = run_gsek(g, "mixed")
+    print("water23559 mixed", rms(Fm, z["F"]), rel(Em, float(z["E"])))
+    assert rms(Fm, z["F"]) <= MIXED_TOL
+    assert rel(Em, float(z["E"])) <= MIXED_TOL
+
+
+def test_mixed_is_deterministic(goldens):
+    g = goldens["water600_L18_M17_odd"]
+    a, Ea, Fa = run_gsek(g, "mixed")
+    b, Eb, Fb = run_gsek(g, "mixed")
+    assert np.array_equal(a.getRhoS().data, b.getRhoS().data)
+    assert np.array_equal(Fa, Fb) and Ea == Eb
+
+
+@pytest.mark.parametrize("case", ["pair_L20_M20", "water300_noncubic", "water96_L9_M10_wide"])
+def test_stage_spread_and_gather(goldens, case):
+    from gse_b200.gse import CpuGaussCharge, CpuGrid
+    import oracle
+    g = goldens[case]
+    M, box, sigma = tuple(int(v) for v in g["M"]), tuple(float(v) for v in g["box"]), float(g["sigma"])
+    s1, s2, rc = oracle.gse_params(sigma)
+    n = g["xyzq"].shape[0]
+    gc = CpuGaussCharge(*M, precision="fp64")
+    rho = CpuGrid(*M)
+    gc.spreadChargeToGrid(s1, rc, n, g["xyzq"], *box, rho)
+    assert np.abs(rho.data - g["rhoS"]).max() <= FP64_TOL * np.abs(g["rhoS"]).max()
+    gc.spreadChargeToGrid(s1, rc, n, g["xyzq"], *box, rho, True)
+    assert np.abs(rho.data - g["rho_norm"]).max() <= FP64_TOL * np.abs(g["rho_norm"]).max()
+    phi = CpuGrid(*M)
+    phi.data[...] = g["phi"]
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    gc.interpolateForce(s1, rc, n, g["xyzq"], *box, phi, fx, fy, fz)
+    F = np.stack([fx, fy, fz], axis=1) * 332.0716
+    assert rms(F, g["F"]) <= FP64_TOL
+    # mixed form against the reference's own <double,float> instance
+    gm = CpuGaussCharge(*M, precision="mixed")
+    rf = CpuGrid(*M, dtype=np.float32)
+    gm.spreadChargeToGrid(s1, rc, n, g["xyzq"].astype(np.float32), *box, rf)
+    assert np.abs(rf.data - g["rho_f"]).max() <= 1e-5 * np.abs(g["rho_f"]).max()
+    pf = CpuGrid(*M, dtype=np.float32)
+    pf.data[...] = g["phi"].astype(np.float32)
+    gm.interpolateForce(s1, rc, n, g["xyzq"].astype(np.float32), *box, pf, fx, fy, fz)
+    assert rms(np.stack([fx, fy, fz], axis=1), g["F_f"]) <= 1e-5
+
+
+@pytest.mark.parametrize("M", [(16, 18, 20), (17, 17, 17), (20, 20, 20), (10, 12, 9)])
+def test_green_mul_and_fft_solve(M):
+    import oracle
+    from gse_b200.gse import CpuFFTSolver, CpuGreensFuncGSE, CpuGrid
+    rng = np.random.default_rng(11)
+    box = (15.0, 16.0, 17.0)
+    nxh = M[0] // 2 + 1
+    k = rng.standard_normal((M[2], M[1], nxh)) + 1j * rng.standard_normal((M[2], M[1], nxh))
+    ref = oracle.green_mul(M, box, 0.9, k)
+    grid = CpuGrid(2 * nxh, M[1], M[2])
+    grid.data[...] = k.view(np.float64).reshape(M[2], M[1], 2 * nxh)
+    gf = CpuGreensFuncGSE("fp64")
+    gf.mul(M[0], M[1], M[2], *box, 0.9, grid)
+    out = grid.data.view(np.complex128)
+    assert np.abs(out - ref).max() <= 1e-14 * np.abs(ref).max()
+    rho = CpuGrid(*M)
+    rho.data[...] = rng.standard_normal((M[2], M[1], M[0]))
+    phi = CpuGrid(*M)
+    CpuFFTSolver(gf, *M).run(phi, rho, 0.9, *box)
+    want = oracle.fft_c2r(oracle.green_mul(M, box, 0.9, oracle.fft_r2c(rho.data)), M[0])
+    assert np.abs(phi.data - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_forward_equals_stages_and_device_pointers(goldens):
+    import torch
+    from gse_b200.gse import CpuGSEk
+    g = goldens["water600_L18_M17_odd"]
+    gs, E, F = run_gsek(g, "fp64")
+    M, box, sigma = tuple(int(v) for v in g["M"]), tuple(float(v) for v in g["box"]), float(g["sigma"])
+    n = g["xyzq"].shape[0]
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    E2 = gs.forward(n, g["xyzq"], fx, fy, fz)
+    assert E2 == E and np.array_equal(np.stack([fx, fy, fz], 1), F)
+    d = torch.from_numpy(g["xyzq"]).cuda()
+    f = torch.zeros(3, n, dtype=torch.float64, device="cuda")
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    gs.context.forward(n, d, f[0], f[1], f[2], energy_out=e)
+    gs.context.synchronize()
+    assert np.array_equal(f.cpu().numpy().T, F)
+    assert float(e.item()) == E
+
+
+def test_errors_are_statuses():
+    from gse_b200 import GseError
+    from gse_b200.gse import CpuGSEk
+    with pytest.raises(GseError) as ei:
+        CpuGSEk(16, 16, 16, 2.0, 0.6, 3.0, 3.0, 16.0, 16.0, 16.0)
+    assert ei.value.name == "GSE_ERR_INVALID_ARG"
+    gs = CpuGSEk(16, 16, 16, 2.0, 0.4, 3.0, 3.0, 16.0, 16.0, 16.0)
+    with pytest.raises(GseError) as ei:
+        gs.solvePoisson()
+    assert ei.value.name == "GSE_ERR_NOT_READY"
+    with pytest.raises(GseError) as ei:
+        gs.calculateEnergy()
+    assert ei.value.name == "GSE_ERR_NOT_READY"
+    # zero atoms: an empty grid, zero energy
+    gs.spreadCharge1(0, np.zeros((0, 4)))
+    gs.solvePoisson()
+    assert gs.calculateEnergy() == 0.0
+    with pytest.raises(GseError) as ei:
+        gs.setBoxSize(-1.0, 16.0, 16.0)
+    assert ei.value.name == "GSE_ERR_INVALID_ARG"

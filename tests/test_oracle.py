@@ -1,0 +1,113 @@
+"""The CPU oracle, pinned: the C restatement against the reference's own
+classes (golden fixtures made by tests/golden/make_goldens.py, and the
+reference build in oracle/_ref when present), the project FFT against
+numpy.fft, and the Ewald restatement against the reference's known answer."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_goldens
+
+CASES = sorted(load_goldens().keys())
+
+
+@pytest.mark.parametrize("shape", [(20, 20, 20), (16, 18, 20), (7, 9, 11), (5, 6, 9), (13, 1, 4),
+                                   (64, 32, 48)])
+def test_fft_matches_numpy(oracle_lib, shape):
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(shape)
+    k = oracle_lib.fft_r2c(x)
+    kn = np.fft.rfftn(x)
+    assert np.abs(k - kn).max() <= 1e-14 * np.abs(kn).max()
+    y = oracle_lib.fft_c2r(kn, shape[2])
+    yn = np.fft.irfftn(kn, s=shape, axes=(0, 1, 2)) * np.prod(shape)
+    assert np.abs(y - yn).max() <= 1e-14 * np.abs(yn).max()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_restatement_forward_equals_reference(oracle_lib, goldens, case):
+    g = goldens[case]
+    E, F, rho, phi = oracle_lib.gsek_forward(tuple(g["M"]), tuple(g["box"]), float(g["sigma"]),
+                                             g["xyzq"], want_grids=True)
+    # same operations in the same order: bit-identical to the reference
+    assert np.array_equal(rho, g["rhoS"])
+    assert np.array_equal(phi, g["phi"])
+    assert np.array_equal(F, g["F"])
+    assert E == float(g["E"])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_restatement_float_stages_equal_reference(oracle_lib, goldens, case):
+    g = goldens[case]
+    M, box, sigma = tuple(g["M"]), tuple(g["box"]), float(g["sigma"])
+    s1, s2, rc = oracle_lib.gse_params(sigma)
+    xf = g["xyzq"].astype(np.float32)
+    rho_f = oracle_lib.spread(M, box, s1, rc, xf, dtype=np.float32)
+    assert np.array_equal(rho_f, g["rho_f"])
+    F = np.stack(oracle_lib.gather(M, box, s1, rc, xf, g["phi"].astype(np.float32),
+                                   dtype=np.float32), axis=1)
+    assert np.array_equal(F, g["F_f"])
+    rho_n = oracle_lib.spread(M, box, s1, rc, g["xyzq"], normalize=True)
+    assert np.array_equal(rho_n, g["rho_norm"])
+
+
+def test_restatement_green_equals_reference(oracle_lib):
+    if not oracle_lib.have_reference():
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(3)
+    for M in [(16, 18, 20), (17, 17, 17), (20, 20, 20)]:
+        k = (rng.standard_normal((M[2], M[1], M[0] // 2 + 1)) +
+             1j * rng.standard_normal((M[2], M[1], M[0] // 2 + 1)))
+        a = oracle_lib.green_mul(M, (15.0, 16.0, 17.0), 0.9, k)
+        b = oracle_lib.ref_green_mul(M, (15.0, 16.0, 17.0), 0.9, k)
+        assert np.array_equal(a, b)
+
+
+def test_water_23559_golden(oracle_lib):
+    from gse_b200 import workloads as W
+    z = np.load(os.path.join(GOLDEN, "water_23559.npz"))
+    s = W.config_water_23k()
+    import hashlib
+    assert hashlib.sha256(s.xyzq.tobytes()).digest() == z["xyzq_sha"].tobytes()
+    E, F = oracle_lib.gsek_forward(s.grid, s.boxes, s.sigma, s.xyzq.astype(np.float64))
+    assert E == float(z["E"])
+    assert np.array_equal(F, z["F"])
+
+
+def test_ewald_recip_restatement_matches_reference(oracle_lib):
+    if not oracle_lib.have_reference():
+        pytest.skip("reference build not present")
+    from gse_b200 import workloads as W
+    for xyzq, L, kcut in [(W.reference_pair(1.0), 20.0, 32), (W.random_charges(40, 12.0, 2), 12.0, 9),
+                          (W.triplets(60, 10.0, 5).astype(np.float64), 10.0, 11)]:
+        e1, f1 = oracle_lib.ewald_recip(2.0, kcut, (L, L, L), xyzq)
+        e2, f2 = oracle_lib.ref_ewald_recip(2.0, kcut, (L, L, L), xyzq)
+        assert abs(e1 - e2) <= 1e-12 * abs(e2)
+        assert oracle_lib.force_rms(f1, f2) <= 1e-12
+
+
+def test_ewald_direct_restatement_matches_reference(oracle_lib):
+    if not oracle_lib.have_reference():
+        pytest.skip("reference build not present")
+    from gse_b200 import workloads as W
+    xyzq = W.triplets(300, 14.0, 6).astype(np.float64)
+    e1, f1 = oracle_lib.ewald_direct(2.0, 6.0, (14.0, 14.0, 14.0), xyzq)
+    e2, f2 = oracle_lib.ref_ewald_direct(2.0, 6.0, (14.0, 14.0, 14.0), xyzq)
+    assert e1 == e2
+    assert np.array_equal(f1, f2)
+
+
+def test_ewald_known_answer():
+    """cpu_gse.cpp:324-330: energy_ew = 1733.61 for data/xyzq_48k.txt,
+    sigma 2.12132034355964, box 80, kcut 64 (tests/golden/make_ewald_kat.py)."""
+    with open(os.path.join(GOLDEN, "ewald_kat_48k.json")) as f:
+        kat = json.load(f)
+    assert round(kat["oracle_energy"], 2) == kat["reference_energy"] == 1733.61
+
+
+def test_force_rms_definition(oracle_lib):
+    F = np.array([[1.0, 0, 0], [0, 2.0, 0]])
+    G = F + np.array([[0.1, 0, 0], [0, 0, 0]])
+    assert abs(oracle_lib.force_rms(G, F) - 0.1 / np.sqrt(5.0)) < 1e-15
