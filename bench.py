@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""GSE-k reciprocal-space force evaluations per second on B200.
+
+One step = one whole GSE-k force evaluation of a 262,143-charge water-like
+box (L = 140 A, M = 144, sigma = 2, kappa = 0.4, lambda_sigma1 = 3):
+spreadCharge1 -> solvePoisson -> calculateEnergy -> interpolateForce.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision mixed|fp64]
+
+`value` is whole-job evals/s with inputs resident in HBM (CUDA events around
+each evaluation; L2 is flushed between timed evaluations).  `e2e` is the same
+metric through the public call with pinned host buffers (host->device copy of
+the positions and device->host copy of forces and energy inside every step).
+With N > 1 (torchrun) every rank evaluates its own independent replica:
+replicas only, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GSE recip force evals/s at 262k charges: mixed vs FP64 GPU at ≤1e-4 rel force RMS"
+UNIT = "force evals/s"
+WORKLOAD = "water_262143_L140_M144"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# algorithmic bytes per launch (262,143 charges, M = 144): positions+charges
+# read once, grid written or read once, forces written once (float64)
+N_ATOMS = 262143
+GRID = 144 ** 3
+
+
+def algorithmic_bytes(stage: str, precision: str) -> float:
+    ct = 4 if precision == "mixed" else 8
+    xyzq = N_ATOMS * 4 * ct
+    grid = GRID * ct
+    forces = N_ATOMS * 3 * 8
+    if stage == "spread":
+        return xyzq + grid
+    if stage == "gather":
+        return xyzq + grid + forces
+    raise ValueError(stage)
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_cpu(xyzq64: np.ndarray, box: float, M: int, sigma: float, budget_s: float,
+                  max_evals: int):
+    """The reference's own CpuGSEk<double,double> (oracle/_ref build) timed on the host."""
+    import oracle
+    R = oracle.ref()
+    n = xyzq64.shape[0]
+    h = R.ref_gsek_create(M, M, M, sigma, 0.4, 3.0, 3.0, box, box, box, 332.0716)
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    e = np.zeros(1)
+    p = oracle._ptr
+    # the reference prints from its spread and gather loops; keep stdout for
+    # the JSON line
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    times = []
+    try:
+        t_start = time.perf_counter()
+        while len(times) < max_evals and (not times or time.perf_counter() - t_start < budget_s):
+            t0 = time.perf_counter()
+            R.ref_gsek_eval(h, n, p(xyzq64), p(e), p(fx), p(fy), p(fz))
+            times.append(time.perf_counter() - t0)
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(devnull)
+        os.close(saved)
+        R.ref_gsek_destroy(h)
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": len(times) / sum(times), "evals": len(times), "seconds": sum(times),
+            "threads": threads, "energy": float(e[0])}
+
+
+def make_workload():
+    from gse_b200 import workloads as W
+    return W.config_water_262k()
+
+
+def run_reference_arm(args):
+    s = make_workload()
+    xyzq = s.xyzq.astype(np.float64)
+    import oracle
+    kind = "reference" if oracle.have_reference() else "port"
+    if kind == "port":
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref was not built (no reference sources)"}))
+        return
+    budget = float(os.environ.get("GSE_REF_BUDGET_S", "120"))
+    warm = reference_cpu(xyzq, s.box, s.M, s.sigma, 0.0, max(1, min(args.warmup, 1)))
+    del warm
+    r = reference_cpu(xyzq, s.box, s.M, s.sigma, budget, max(1, args.steps))
+    sample = (f"{r['evals']} full evaluations of the {s.n}-charge box (of {args.steps} requested "
+              f"steps, stopped after a {budget:.0f} s budget); CpuGSEk<double,double> compiled from "
+              "the reference sources, spread/gather single-threaded as written, FFTs through the "
+              f"project FFTW-API shim on {r['threads']} OpenMP threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": r["evals"], "warmup": 1, "ms_per_step": 1000.0 * r["seconds"] / r["evals"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded water-like triplets)",
+        "config": {"workload": WORKLOAD, "n_charges": s.n, "grid": s.M, "box": s.box,
+                   "sigma": s.sigma, "precision": "fp64 (reference CPU)"},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from gse_b200.gse import Context
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    s = make_workload()
+    n = s.n
+    stream = torch.cuda.current_stream()
+
+    def make_ctx(precision):
+        c = Context(s.M, s.M, s.M, s.sigma, s.kappa, s.lambda_sigma, s.lambda_sigma1, s.box, s.box,
+                    s.box, precision=precision, device=local)
+        c.set_stream(stream.cuda_stream)
+        return c
+
+    def device_inputs(precision):
+        ct = np.float32 if precision == "mixed" else np.float64
+        x = torch.from_numpy(s.xyzq.astype(ct)).cuda()
+        f = torch.empty(3, n, dtype=torch.float64, device="cuda")
+        e = torch.empty(1, dtype=torch.float64, device="cuda")
+        return x, f, e
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed_loop(ctx, x, f, e, steps, with_timing):
+        for _ in range(args.warmup):
+            ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
+        torch.cuda.synchronize()
+        ctx.get_timing(reset=True)
+        launches0 = ctx.launch_count()
+        ctx.set_timing(with_timing)
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(steps):
+            flush.zero_()  # L2 flush, outside the timed interval
+            starts[k].record(stream)
+            ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ctx.set_timing(False)
+        stage = ctx.get_timing(reset=True)
+        launches = ctx.launch_count() - launches0
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        return ms, stage, launches
+
+    # ---- main arm: requested precision, device-resident inputs ----------
+    prec = args.precision
+    ctx = make_ctx(prec)
+    x, f, e = device_inputs(prec)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_local, stage, launches = timed_loop(ctx, x, f, e, args.steps, True)
+    clock_info = clocks.stop()
+    t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1000.0)
+    F_main = f.clone()
+    E_main = float(e.item())
+
+    # ---- e2e: public call with pinned host buffers ----------------------
+    ct = np.float32 if prec == "mixed" else np.float64
+    hx = torch.from_numpy(s.xyzq.astype(ct)).pin_memory()
+    hf = torch.empty(3, n, dtype=torch.float64).pin_memory()
+    hxn, hfn = hx.numpy(), hf.numpy()
+    for _ in range(args.warmup):
+        ctx.forward(n, hxn, hfn[0], hfn[1], hfn[2])
+    e2e_steps = max(3, min(args.steps, 20))
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+    for k in range(e2e_steps):
+        flush.zero_()
+        ev0[k].record(stream)
+        ctx.forward(n, hxn, hfn[0], hfn[1], hfn[2])
+        ev1[k].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(ev0, ev1))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / (float(t.item()) / 1000.0)
+    h2d = n * 4 * np.dtype(ct).itemsize
+    d2h = 3 * n * 8 + 8
+
+    # ---- the other precision, for the mixed-vs-FP64 comparison ----------
+    other = "fp64" if prec == "mixed" else "mixed"
+    ctx2 = make_ctx(other)
+    x2, f2, e2 = device_inputs(other)
+    ms2, stage2, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 20)), False)
+    value2 = world * max(3, min(args.steps, 20)) / (ms2 / 1000.0)
+    F64 = (f2 if other == "fp64" else F_main).double().cpu().numpy()
+    Fmx = (F_main if other == "fp64" else f2).double().cpu().numpy()
+    E64 = float(e2.item()) if other == "fp64" else E_main
+    Emx = E_main if other == "fp64" else float(e2.item())
+    d = Fmx - F64
+    force_rms = float(np.sqrt((d * d).sum() / (F64 * F64).sum()))
+    energy_rel = abs(Emx - E64) / abs(E64)
+
+    if rank == 0:
+        # roofline of the dominant kernel
+        peak, peak_kind = hbm_peak()
+        dom = max(("spread", "gather"), key=lambda k: stage[k][0] / max(stage[k][1], 1))
+        dom_ms = stage[dom][0] / max(stage[dom][1], 1)
+        ab = algorithmic_bytes(dom, prec)
+        achieved = ab / (dom_ms / 1000.0) / 1e9
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", f"{dom}_{prec}_traffic.json")
+        if os.path.exists(prof):
+            try:
+                with open(prof) as fh:
+                    traffic = json.load(fh).get("dram_bytes_per_launch")
+            except Exception:
+                traffic = None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                import oracle
+                if oracle.have_reference():
+                    r = reference_cpu(s.xyzq.astype(np.float64), s.box, s.M, s.sigma, 12.0, 3)
+                    cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"],
+                           "kind": "reference",
+                           "sample": f"{r['evals']} full evaluations of the same {n}-charge box "
+                                     "by CpuGSEk<double,double> compiled from the reference "
+                                     "sources (spread/gather single-threaded as written; FFTs "
+                                     f"through the FFTW-API shim on {r['threads']} threads)"}
+            except Exception as exc:  # noqa: BLE001
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                       "sample": f"failed: {exc}"}
+        per_stage = {k: round(v[0] / max(v[1], 1), 4) for k, v in stage.items()}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == "mixed" else "f64",
+            "data": "synthetic (seeded water-like triplets, 87,381 rigid 3-site molecules)",
+            "config": {"workload": WORKLOAD, "n_charges": n, "grid": s.M, "box": s.box,
+                       "sigma": s.sigma, "kappa": s.kappa, "lambda_sigma1": s.lambda_sigma1,
+                       "precision": prec, "parallelism": f"replicas{world}",
+                       "l2": "flushed between timed evaluations (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": dom,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": ab, "launch_ms": dom_ms},
+            "cpu_baseline": cpu,
+            "clocks": clock_info,
+            "stage_ms": per_stage,
+            f"{other}_value": value2,
+            "mixed_vs_fp64": {"force_rms": force_rms, "energy_rel": energy_rel},
+            "energy": E_main,
+        }
+        print(json.dumps(line), flush=True)
+
+    del ctx, ctx2
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -67,7 +67,11 @@ SIGNATURES = {
     "gse_gauss_interpolate": (_i, [_vp, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "gse_green_mul": (_i, [_vp, _d, _d, _d, _d, _vp]),
     "gse_fft_solve": (_i, [_vp, _d, _d, _d, _d, _vp, _vp]),
+    "gse_set_timing": (_i, [_vp, _i]),
+    "gse_get_timing": (_i, [_vp, _vp, _vp, _i]),
+    "gse_get_launch_count": (_i, [_vp, _vp]),
 }
+STAGES = ["bin", "spread", "fft_forward", "green", "fft_backward", "gather"]
 
 _lib = None
 

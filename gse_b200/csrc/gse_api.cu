@@ -101,9 +101,48 @@ struct gse_context {
   cufftHandle plan_f = 0, plan_b = 0;
   bool plans = false;
   bool rho_valid = false, phi_valid = false, energy_valid = false;
+  // optional per-stage device timing (gse_set_timing)
+  bool timing = false;
+  cudaEvent_t ev[GSE_NUM_STAGES][2] = {};
+  bool ev_pending[GSE_NUM_STAGES] = {};
+  double stage_ms[GSE_NUM_STAGES] = {};
+  long long stage_count[GSE_NUM_STAGES] = {};
+  long long launches = 0;  // kernels of this library launched so far
 };
 
 namespace {
+
+// Fold a completed start/stop pair into the stage totals.
+void harvest(gse_context_t* c, int st) {
+  if (!c->ev_pending[st]) return;
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, c->ev[st][0], c->ev[st][1]) == cudaSuccess) {
+    c->stage_ms[st] += ms;
+    c->stage_count[st] += 1;
+  } else {
+    cudaGetLastError();
+  }
+  c->ev_pending[st] = false;
+}
+
+// RAII bracket of one stage on the context stream.
+struct StageTimer {
+  gse_context_t* c;
+  int st;
+  StageTimer(gse_context_t* c_, int st_) : c(c_), st(st_) {
+    if (!c->timing) return;
+    if (c->ev_pending[st]) {
+      cudaEventSynchronize(c->ev[st][1]);
+      harvest(c, st);
+    }
+    cudaEventRecord(c->ev[st][0], c->stream);
+  }
+  ~StageTimer() {
+    if (!c->timing) return;
+    cudaEventRecord(c->ev[st][1], c->stream);
+    c->ev_pending[st] = true;
+  }
+};
 
 gse_status_t check_ctx(gse_context_t* c) {
   if (!c) return fail(GSE_ERR_INVALID_ARG, "NULL context");
@@ -203,6 +242,7 @@ gse_status_t stage_atoms(gse_context_t* c, int n, const void* xyzq, const void**
 template <typename CT>
 gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s) {
   typedef typename Vec4<CT>::type V;
+  c->launches += 3;
   CU(launch_bin<CT>((const V*)dx, n, c->bg, s.inv_h[0], s.inv_h[1], s.inv_h[2], c->d_keys,
                     c->d_slots, c->d_counts, c->d_offsets, (V*)c->d_sorted, c->d_perm, c->d_bad,
                     c->stream));
@@ -214,6 +254,8 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
                        double rcut, bool normalize) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
+  StageTimer tm(c, GSE_STAGE_SPREAD);
+  c->launches += (n > 0 ? 1 : 0) + (c->fp64 ? 0 : 1);
   CU(launch_spread<CT>((const V*)dx, n, s, (CT*)c->d_rho, c->fp64 ? nullptr : c->d_fixed,
                        c->stream));
   c->rho_valid = true;
@@ -229,7 +271,12 @@ gse_status_t do_gather(gse_context_t* c, int n, const void* dx, const double box
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, true, false);
   if (n == 0) return GSE_OK;
-  TRY(bin_atoms<CT>(c, n, dx, s));
+  {
+    StageTimer tm(c, GSE_STAGE_BIN);
+    TRY(bin_atoms<CT>(c, n, dx, s));
+  }
+  StageTimer tm(c, GSE_STAGE_GATHER);
+  c->launches += 1;
   CU(launch_gather<CT>((const V*)c->d_sorted, c->d_perm, n, s, phi, outscale, fx, fy, fz,
                        c->stream));
   return GSE_OK;
@@ -280,14 +327,22 @@ gse_status_t fft_backward(gse_context_t* c, void* rhok, void* phi) {
 // phi = c2r(G(sigma) r2c(rho)); optionally the k-space energy into d_scalars[0].
 gse_status_t do_solve(gse_context_t* c, const void* rho, void* phi, double sigma, double bx,
                       double by, double bz, bool energy) {
-  TRY(fft_forward(c, rho, c->d_rhok));
-  const GreenGeom g = green_geom(c, sigma, bx, by, bz, energy);
-  if (c->fp64)
-    CU(launch_green_energy<double>((double2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
-                                   energy_factor(c), c->d_scalars, c->stream));
-  else
-    CU(launch_green_energy<float>((float2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
-                                  energy_factor(c), c->d_scalars, c->stream));
+  {
+    StageTimer tm(c, GSE_STAGE_FFT_FORWARD);
+    TRY(fft_forward(c, rho, c->d_rhok));
+  }
+  {
+    StageTimer tm(c, GSE_STAGE_GREEN);
+    const GreenGeom g = green_geom(c, sigma, bx, by, bz, energy);
+    c->launches += energy ? 2 : 1;
+    if (c->fp64)
+      CU(launch_green_energy<double>((double2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
+                                     energy_factor(c), c->d_scalars, c->stream));
+    else
+      CU(launch_green_energy<float>((float2*)c->d_rhok, g, c->d_partials, kEnergyPartials,
+                                    energy_factor(c), c->d_scalars, c->stream));
+  }
+  StageTimer tm(c, GSE_STAGE_FFT_BACKWARD);
   TRY(fft_backward(c, c->d_rhok, phi));
   return GSE_OK;
 }
@@ -484,6 +539,9 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_scalars);
   cudaFree(c->d_bad);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  for (int i = 0; i < GSE_NUM_STAGES; i++)
+    for (int j = 0; j < 2; j++)
+      if (c->ev[i][j]) cudaEventDestroy(c->ev[i][j]);
   delete c;
   return GSE_OK;
 }
@@ -727,6 +785,42 @@ gse_status_t gse_fft_solve(gse_context_t* c, double sigma, double bx, double by,
   bool host = false;
   if (!pdev) TRY(copy_out(c, phi, c->d_phi, bytes, &host));
   return finish(c, host);
+}
+
+gse_status_t gse_set_timing(gse_context_t* c, int enable) {
+  TRY(check_ctx(c));
+  if (enable && !c->ev[0][0]) {
+    for (int i = 0; i < GSE_NUM_STAGES; i++)
+      for (int j = 0; j < 2; j++) CU(cudaEventCreate(&c->ev[i][j]));
+  }
+  if (!enable && c->timing) {
+    CU(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < GSE_NUM_STAGES; i++) harvest(c, i);
+  }
+  c->timing = enable != 0;
+  return GSE_OK;
+}
+
+gse_status_t gse_get_launch_count(gse_context_t* c, long long* launches) {
+  TRY(check_ctx(c));
+  if (!launches) return fail(GSE_ERR_INVALID_ARG, "NULL launches");
+  *launches = c->launches;
+  return GSE_OK;
+}
+
+gse_status_t gse_get_timing(gse_context_t* c, double* ms_total, long long* counts, int reset) {
+  TRY(check_ctx(c));
+  CU(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < GSE_NUM_STAGES; i++) {
+    harvest(c, i);
+    if (ms_total) ms_total[i] = c->stage_ms[i];
+    if (counts) counts[i] = c->stage_count[i];
+    if (reset) {
+      c->stage_ms[i] = 0.0;
+      c->stage_count[i] = 0;
+    }
+  }
+  return GSE_OK;
 }
 
 }  // extern "C"

@@ -137,6 +137,21 @@ class Context:
     def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
         check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
 
+    def set_timing(self, enable: bool):
+        check(self._L.gse_set_timing(self.h, int(bool(enable))))
+
+    def launch_count(self) -> int:
+        c = ctypes.c_longlong()
+        check(self._L.gse_get_launch_count(self.h, ctypes.addressof(c)))
+        return c.value
+
+    def get_timing(self, reset: bool = False):
+        """{stage: (total_ms, launches)} of the device stage timers."""
+        ms = np.zeros(len(_lib.STAGES), dtype=np.float64)
+        cnt = np.zeros(len(_lib.STAGES), dtype=np.int64)
+        check(self._L.gse_get_timing(self.h, ms.ctypes.data, cnt.ctypes.data, int(bool(reset))))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.STAGES)}
+
 
 def _xyzq_arg(xyzq, dtype):
     if isinstance(xyzq, np.ndarray):
@@ -214,7 +229,10 @@ class CpuGaussCharge:
         self.sizeX, self.sizeY, self.sizeZ = int(sizeX), int(sizeY), int(sizeZ)
         self.precision = precision
         self.dtype = _ct(precision)
-        self._ctx = Context(sizeX, sizeY, sizeZ, sigma=1.0, precision=precision, device=device)
+        # the stage calls carry their own sigma, rcut and box; the context's
+        # own parameters only need to describe a valid stencil
+        self._ctx = Context(sizeX, sizeY, sizeZ, sigma=1.0, boxx=sizeX, boxy=sizeY, boxz=sizeZ,
+                            precision=precision, device=device)
 
     def _check(self, grid: CpuGrid):
         if (grid.sizeX, grid.sizeY, grid.sizeZ) != (self.sizeX, self.sizeY, self.sizeZ):
@@ -264,7 +282,8 @@ class CpuGreensFuncGSE(CpuGreensFunc):
 
     def _context(self, nx, ny, nz):
         if self._ctx is None or self._ctx.shape != (nz, ny, nx):
-            self._ctx = Context(nx, ny, nz, precision=self.precision, device=self.device)
+            self._ctx = Context(nx, ny, nz, boxx=nx, boxy=ny, boxz=nz, precision=self.precision,
+                                device=self.device)
         return self._ctx
 
     def mul(self, nfftX, nfftY, nfftZ, boxx, boxy, boxz, sigma, rho: CpuGrid):
@@ -284,8 +303,8 @@ class CpuFFTSolver:
             raise GseError(7, "only the GSE Green's function is implemented on the GPU")
         self.greensFunc = greensFunc
         self.sizeX, self.sizeY, self.sizeZ = int(sizeX), int(sizeY), int(sizeZ)
-        self._ctx = Context(sizeX, sizeY, sizeZ, precision=greensFunc.precision,
-                            device=greensFunc.device)
+        self._ctx = Context(sizeX, sizeY, sizeZ, boxx=sizeX, boxy=sizeY, boxz=sizeZ,
+                            precision=greensFunc.precision, device=greensFunc.device)
 
     def run(self, phi: CpuGrid, rho: CpuGrid, sigma, boxx, boxy, boxz):
         for g in (phi, rho):

@@ -173,6 +173,29 @@ gse_status_t gse_green_mul(gse_context_t* ctx, double sigma, double box_x, doubl
 gse_status_t gse_fft_solve(gse_context_t* ctx, double sigma, double box_x, double box_y,
                            double box_z, const void* rho, void* phi);
 
+/* ---- instrumentation (no reference counterpart) ------------------------ */
+
+typedef enum gse_stage {
+  GSE_STAGE_BIN = 0,          /* cell binning of atoms before the gather */
+  GSE_STAGE_SPREAD = 1,       /* charge spreading (incl. grid clear/convert) */
+  GSE_STAGE_FFT_FORWARD = 2,  /* r2c transform */
+  GSE_STAGE_GREEN = 3,        /* Green's function multiply + k-space energy */
+  GSE_STAGE_FFT_BACKWARD = 4, /* c2r transform */
+  GSE_STAGE_GATHER = 5,       /* force gather */
+  GSE_NUM_STAGES = 6
+} gse_stage_t;
+
+/* Record CUDA events around every stage on the context stream. */
+gse_status_t gse_set_timing(gse_context_t* ctx, int enable);
+
+/* Accumulated device milliseconds and launch counts per stage
+ * (arrays of GSE_NUM_STAGES; either may be NULL); reset != 0 zeroes them. */
+gse_status_t gse_get_timing(gse_context_t* ctx, double* ms_total, long long* counts, int reset);
+
+/* Number of this library's own CUDA kernels the context has launched
+ * (library calls such as cuFFT's are not counted). */
+gse_status_t gse_get_launch_count(gse_context_t* ctx, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif
