@@ -157,14 +157,14 @@ def test_forward_equals_stages_and_device_pointers(goldens):
     n = g["xyzq"].shape[0]
     fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
     E2 = gs.forward(n, g["xyzq"], fx, fy, fz)
-    assert E2 == E and np.array_equal(np.stack([fx, fy, fz], 1), F)
+    assert rel(E2, E) <= FP64_TOL and rms(np.stack([fx, fy, fz], 1), F) <= FP64_TOL
     d = torch.from_numpy(g["xyzq"]).cuda()
     f = torch.zeros(3, n, dtype=torch.float64, device="cuda")
     e = torch.zeros(1, dtype=torch.float64, device="cuda")
     gs.context.forward(n, d, f[0], f[1], f[2], energy_out=e)
     gs.context.synchronize()
-    assert np.array_equal(f.cpu().numpy().T, F)
-    assert float(e.item()) == E
+    assert rms(f.cpu().numpy().T, F) <= FP64_TOL
+    assert rel(float(e.item()), E) <= FP64_TOL
 
 
 def test_errors_are_statuses():
