@@ -71,6 +71,10 @@ bool is_device_ptr(const void* p) {
 
 }  // namespace
 
+namespace gse {
+gse_status_t set_error(gse_status_t s, const char* msg) { return fail(s, "%s", msg); }
+}  // namespace gse
+
 struct gse_context {
   gse_params_t p;
   cudaStream_t stream = nullptr;
@@ -149,19 +153,6 @@ gse_status_t check_ctx(gse_context_t* c) {
   cudaError_t e = cudaSetDevice(c->p.device);
   if (e != cudaSuccess) return fail(GSE_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
   return GSE_OK;
-}
-
-double fixed_scale_for(double spread_pref) {
-  // 2^40 fixed-point units per unit density for the default widths; coarser
-  // when a narrow Gaussian makes single contributions large, so that any sum
-  // of up to 2^22 maximal contributions stays inside int64.
-  int k = 40;
-  double m = std::fabs(spread_pref) / 0.05;
-  while (m > 1.0 && k > 8) {
-    m *= 0.5;
-    k--;
-  }
-  return std::ldexp(1.0, k);
 }
 
 template <typename CT>

@@ -60,6 +60,20 @@ inline Stencil<CT> make_stencil(const int M[3], const double box[3], double sigm
   return s;
 }
 
+// Fixed-point units per unit charge density for the mixed form's int64 grid:
+// 2^40 for the default widths; coarser when a narrow Gaussian makes single
+// contributions large, so that any sum of up to 2^22 maximal contributions
+// stays inside int64.
+inline double fixed_scale_for(double spread_pref) {
+  int k = 40;
+  double m = std::fabs(spread_pref) / 0.05;
+  while (m > 1.0 && k > 8) {
+    m *= 0.5;
+    k--;
+  }
+  return std::ldexp(1.0, k);
+}
+
 // ---- round-to-nearest arithmetic that nvcc may not contract into FMAs ----
 // The stencil origin and the spherical cut must be bit-identical to the
 // reference's separately rounded products and sums.

@@ -196,6 +196,34 @@ gse_status_t gse_get_timing(gse_context_t* ctx, double* ms_total, long long* cou
  * (library calls such as cuFFT's are not counted). */
 gse_status_t gse_get_launch_count(gse_context_t* ctx, long long* launches);
 
+/* ---- spreading without allocation ------------------------------------- */
+
+/* Largest grid (size_x*size_y*size_z points) gse_spread_mixed_noalloc takes. */
+#define GSE_NOALLOC_MAX_GRID_POINTS 1048576
+
+/* Mixed-precision charge spreading (the computation of gse_gauss_spread on a
+ * GSE_PRECISION_MIXED context) that allocates no memory.  No counterpart in
+ * the reference: it exists for callers that may not allocate device memory
+ * while they run, e.g. a host engine whose own memory pool must remain the
+ * only owner of device memory, or a time-step loop that cannot take the
+ * synchronisation of cudaMalloc/cudaFree.
+ *
+ *  - xyzq (n float4 records) and rho_out (size_x*size_y*size_z floats) must
+ *    be device memory of the current device; the call is asynchronous on
+ *    `stream` (a cudaStream_t, NULL = legacy default stream).
+ *  - The int64 accumulation grid lives in a fixed device array of
+ *    GSE_NOALLOC_MAX_GRID_POINTS values (8 MiB) that every GPU loading the
+ *    library holds until the process exits; larger grids are rejected with
+ *    GSE_ERR_INVALID_ARG.
+ *  - The first call on a device looks up that array's device address; make
+ *    the first call on each device before any stream capture begins.
+ *  - All calls on a device share the one array and each call clears it
+ *    first, so calls whose work overlaps on the GPU (different streams, no
+ *    ordering between them) race and corrupt each other's results. */
+gse_status_t gse_spread_mixed_noalloc(int size_x, int size_y, int size_z, double sigma,
+                                      double rcut, int n, const float* xyzq, double box_x,
+                                      double box_y, double box_z, float* rho_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
