@@ -12,10 +12,12 @@
 
 #include <cmath>
 #include <string>
+#include <vector>
 
 #include "gse_b200.h"
 #include "gse_internal.cuh"
 #include "gse_kernels.cuh"
+#include "gse_tiled.cuh"
 
 using namespace gse;
 
@@ -97,6 +99,24 @@ struct gse_context {
   int* d_offsets = nullptr;
   BinGeom bg{};
   int nbins = 0;
+  // binning of the tiled kernels (stable sort by z cell, y cell, x bin)
+  BinLayout bl{};
+  int nbins2 = 0;
+  int* d_bkey = nullptr;
+  int* d_btmp = nullptr;
+  int* d_bcounts = nullptr;
+  int* d_bstart = nullptr;
+  int* d_btiles = nullptr;
+  unsigned* d_qmax = nullptr;
+  // mixed-form scatter spread: halo tiles, per-tile scales, cover tables
+  int scat_w = 0;
+  int* d_halo = nullptr;
+  double* d_hscale = nullptr;
+  short2* d_cover = nullptr;
+  int cover_stride = 0;
+  // Green's function table of the context's own solve (sigma2, box)
+  void* d_gtab = nullptr;
+  bool gtab_valid = false;
   double* d_force = nullptr;  // 3 x atom_cap
   double* d_partials = nullptr;
   double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch
@@ -196,9 +216,12 @@ gse_status_t ensure_atoms(gse_context_t* c, int n) {
   cudaFree(c->d_keys);
   cudaFree(c->d_slots);
   cudaFree(c->d_force);
+  cudaFree(c->d_bkey);
+  cudaFree(c->d_btmp);
   c->d_xyzq = c->d_sorted = nullptr;
   c->d_perm = c->d_keys = c->d_slots = nullptr;
   c->d_force = nullptr;
+  c->d_bkey = c->d_btmp = nullptr;
   c->atom_cap = 0;
   const size_t rec = 4 * c->ct;
   CU(cudaMalloc(&c->d_xyzq, cap * rec));
@@ -207,6 +230,8 @@ gse_status_t ensure_atoms(gse_context_t* c, int n) {
   CU(cudaMalloc(&c->d_keys, cap * sizeof(int)));
   CU(cudaMalloc(&c->d_slots, cap * sizeof(int)));
   CU(cudaMalloc(&c->d_force, 3 * cap * sizeof(double)));
+  CU(cudaMalloc(&c->d_bkey, cap * sizeof(int)));
+  CU(cudaMalloc(&c->d_btmp, cap * sizeof(int)));
   c->atom_cap = cap;
   return GSE_OK;
 }
@@ -230,25 +255,77 @@ gse_status_t stage_atoms(gse_context_t* c, int n, const void* xyzq, const void**
   return GSE_OK;
 }
 
+// Stable counting sort of the atoms into c->d_sorted / c->d_perm by
+// (z cell, y cell, x bin) of their stencil centres; c->d_bstart holds the bin
+// offsets afterwards.
 template <typename CT>
 gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s) {
   typedef typename Vec4<CT>::type V;
-  c->launches += 3;
-  CU(launch_bin<CT>((const V*)dx, n, c->bg, s.inv_h[0], s.inv_h[1], s.inv_h[2], c->d_keys,
-                    c->d_slots, c->d_counts, c->d_offsets, (V*)c->d_sorted, c->d_perm, c->d_bad,
-                    c->stream));
+  StageTimer tm(c, GSE_STAGE_BIN);
+  BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax};
+  c->launches += n > 0 ? 6 : 3;
+  CU(launch_bin_sorted<CT>((const V*)dx, n, c->bl, s.inv_h[0], s.inv_h[1], s.inv_h[2], w,
+                           (V*)c->d_sorted, c->d_perm, c->stream));
+  return GSE_OK;
+}
+
+// Size the scatter buffers for stencil width W (once per width).
+gse_status_t ensure_scatter(gse_context_t* c, int W) {
+  if (c->scat_w == W) return GSE_OK;
+  std::vector<short2> cov;
+  int stride = 0;
+  if (!scatter_cover_table(c->bl, W, cov, &stride))
+    return fail(GSE_ERR_UNSUPPORTED, "grid too small for the scatter spread");
+  cudaFree(c->d_halo);
+  cudaFree(c->d_hscale);
+  cudaFree(c->d_cover);
+  cudaFree(c->d_gtab);
+  c->d_halo = nullptr;
+  c->d_hscale = nullptr;
+  c->d_cover = nullptr;
+  c->scat_w = 0;
+  CU(cudaMalloc(&c->d_halo, sizeof(int) * scatter_halo_words(c->bl, W)));
+  CU(cudaMalloc(&c->d_hscale, sizeof(double) * scatter_brick_count(c->bl)));
+  CU(cudaMalloc(&c->d_cover, sizeof(short2) * cov.size()));
+  CU(cudaMemcpy(c->d_cover, cov.data(), sizeof(short2) * cov.size(), cudaMemcpyHostToDevice));
+  c->cover_stride = stride;
+  c->scat_w = W;
   return GSE_OK;
 }
 
 template <typename CT>
+bool tiled_ok(const gse_context_t* c, const Stencil<CT>& s) {
+  return spread_tiled_supported<CT>(s) && c->p.size_x >= kMinTiledGrid &&
+         c->p.size_y >= kMinTiledGrid && c->p.size_z >= kMinTiledGrid;
+}
+
+// Spread into c->d_rho.  `presorted`: c->d_sorted / d_bstart already hold the
+// binned atoms of this call.
+template <typename CT>
 gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
-                       double rcut, bool normalize) {
+                       double rcut, bool normalize, bool presorted = false) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
-  StageTimer tm(c, GSE_STAGE_SPREAD);
-  c->launches += (n > 0 ? 1 : 0) + (c->fp64 ? 0 : 1);
-  CU(launch_spread<CT>((const V*)dx, n, s, (CT*)c->d_rho, c->fp64 ? nullptr : c->d_fixed,
-                       c->stream));
+  if (!normalize && tiled_ok<CT>(c, s)) {
+    if (!presorted) TRY(bin_atoms<CT>(c, n, dx, s));
+    if (!c->fp64) TRY(ensure_scatter(c, 2 * s.nst[0] + 1));
+    StageTimer tm(c, GSE_STAGE_SPREAD);
+    if (c->fp64) {
+      c->launches += 1;
+      CU(launch_spread_tiled<CT>((const V*)c->d_sorted, c->d_bstart, c->d_qmax, c->bl, s,
+                                 (CT*)c->d_rho, c->stream));
+    } else {
+      c->launches += 2;
+      ScatterBuffers sb{c->d_halo, c->d_hscale, c->d_cover, c->cover_stride};
+      CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl,
+                               *(const Stencil<float>*)&s, sb, (float*)c->d_rho, c->stream));
+    }
+  } else {
+    StageTimer tm(c, GSE_STAGE_SPREAD);
+    c->launches += (n > 0 ? 1 : 0) + (c->fp64 ? 0 : 1);
+    CU(launch_spread<CT>((const V*)dx, n, s, (CT*)c->d_rho, c->fp64 ? nullptr : c->d_fixed,
+                         c->stream));
+  }
   c->rho_valid = true;
   c->phi_valid = false;
   c->energy_valid = false;
@@ -258,18 +335,19 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
 template <typename CT>
 gse_status_t do_gather(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
                        double rcut, const CT* phi, double outscale, double* fx, double* fy,
-                       double* fz) {
+                       double* fz, bool presorted = false) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, true, false);
   if (n == 0) return GSE_OK;
-  {
-    StageTimer tm(c, GSE_STAGE_BIN);
-    TRY(bin_atoms<CT>(c, n, dx, s));
-  }
+  if (!presorted) TRY(bin_atoms<CT>(c, n, dx, s));
   StageTimer tm(c, GSE_STAGE_GATHER);
   c->launches += 1;
-  CU(launch_gather<CT>((const V*)c->d_sorted, c->d_perm, n, s, phi, outscale, fx, fy, fz,
-                       c->stream));
+  if (tiled_ok<CT>(c, s))
+    CU(launch_gather_tiled<CT>((const V*)c->d_sorted, c->d_perm, c->d_bstart, c->bl, s, phi,
+                               outscale, fx, fy, fz, c->stream));
+  else
+    CU(launch_gather<CT>((const V*)c->d_sorted, c->d_perm, n, s, phi, outscale, fx, fy, fz,
+                         c->stream));
   return GSE_OK;
 }
 
@@ -338,6 +416,38 @@ gse_status_t do_solve(gse_context_t* c, const void* rho, void* phi, double sigma
   return GSE_OK;
 }
 
+// The context's own solve (sigma2, context box) with the tabulated Green's
+// function: r2c -> multiply + energy -> c2r.
+gse_status_t do_solve_ctx(gse_context_t* c) {
+  const GreenGeom g = green_geom(c, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true);
+  if (!c->gtab_valid) {
+    if (!c->d_gtab) CU(cudaMalloc(&c->d_gtab, c->ksize * c->ct));
+    if (c->fp64)
+      CU(launch_green_table<double>(g, (double*)c->d_gtab, c->stream));
+    else
+      CU(launch_green_table<float>(g, (float*)c->d_gtab, c->stream));
+    c->gtab_valid = true;
+  }
+  {
+    StageTimer tm(c, GSE_STAGE_FFT_FORWARD);
+    TRY(fft_forward(c, c->d_rho, c->d_rhok));
+  }
+  {
+    StageTimer tm(c, GSE_STAGE_GREEN);
+    c->launches += 2;
+    if (c->fp64)
+      CU(launch_green_apply<double>((double2*)c->d_rhok, (const double*)c->d_gtab, g,
+                                    c->d_partials, kEnergyPartials, energy_factor(c),
+                                    c->d_scalars, c->stream));
+    else
+      CU(launch_green_apply<float>((float2*)c->d_rhok, (const float*)c->d_gtab, g, c->d_partials,
+                                   kEnergyPartials, energy_factor(c), c->d_scalars, c->stream));
+  }
+  StageTimer tm(c, GSE_STAGE_FFT_BACKWARD);
+  TRY(fft_backward(c, c->d_rhok, c->d_phi));
+  return GSE_OK;
+}
+
 // Copy `bytes` from device src to dst (host or device) on the stream.
 gse_status_t copy_out(gse_context_t* c, void* dst, const void* src, size_t bytes, bool* host) {
   const bool dev = is_device_ptr(dst);
@@ -357,12 +467,14 @@ gse_status_t finish(gse_context_t* c, bool host_outputs) {
 template <typename CT>
 gse_status_t gather_to(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
                        double rcut, const CT* phi, double outscale, double* fx, double* fy,
-                       double* fz, bool* host) {
+                       double* fz, bool* host, bool presorted = false) {
   const bool direct = fx && fy && fz && is_device_ptr(fx) && is_device_ptr(fy) && is_device_ptr(fz);
-  if (direct) return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz);
+  if (direct)
+    return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz, presorted);
   double* f = c->d_force;
   const size_t cap = c->atom_cap;
-  TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + cap, f + 2 * cap));
+  TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + cap, f + 2 * cap,
+                    presorted));
   if (n == 0) return GSE_OK;
   if (fx) TRY(copy_out(c, fx, f, n * sizeof(double), host));
   if (fy) TRY(copy_out(c, fy, f + cap, n * sizeof(double), host));
@@ -487,6 +599,12 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_rhok, c->ksize * 2 * c->ct));
   if (!c->fp64) CUC(cudaMalloc(&c->d_fixed, c->size * sizeof(long long)));
   CUC(cudaMalloc(&c->d_counts, sizeof(int) * c->nbins));
+  c->bl = make_bin_layout(M);
+  c->nbins2 = bin_count(c->bl);
+  CUC(cudaMalloc(&c->d_bcounts, sizeof(int) * c->nbins2));
+  CUC(cudaMalloc(&c->d_bstart, sizeof(int) * (c->nbins2 + 1)));
+  CUC(cudaMalloc(&c->d_btiles, sizeof(int) * (c->nbins2 / 4096 + 2)));
+  CUC(cudaMalloc(&c->d_qmax, sizeof(unsigned)));
   CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
   CUC(cudaMalloc(&c->d_partials, sizeof(double) * kEnergyPartials));
   CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 4));
@@ -526,6 +644,16 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_force);
   cudaFree(c->d_counts);
   cudaFree(c->d_offsets);
+  cudaFree(c->d_bkey);
+  cudaFree(c->d_btmp);
+  cudaFree(c->d_bcounts);
+  cudaFree(c->d_bstart);
+  cudaFree(c->d_btiles);
+  cudaFree(c->d_qmax);
+  cudaFree(c->d_halo);
+  cudaFree(c->d_hscale);
+  cudaFree(c->d_cover);
+  cudaFree(c->d_gtab);
   cudaFree(c->d_partials);
   cudaFree(c->d_scalars);
   cudaFree(c->d_bad);
@@ -558,6 +686,7 @@ gse_status_t gse_set_box(gse_context_t* c, double bx, double by, double bz) {
     return s;
   }
   c->phi_valid = c->energy_valid = false;
+  c->gtab_valid = false;
   return GSE_OK;
 }
 
@@ -581,7 +710,7 @@ gse_status_t gse_spread_charge(gse_context_t* c, int n, const void* xyzq) {
 gse_status_t gse_solve_poisson(gse_context_t* c) {
   TRY(check_ctx(c));
   if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "solvePoisson before spreadCharge1");
-  TRY(do_solve(c, c->d_rho, c->d_phi, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true));
+  TRY(do_solve_ctx(c));
   c->phi_valid = true;
   c->energy_valid = true;
   return finish(c, false);
@@ -631,20 +760,26 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
   const void* dx;
   TRY(stage_atoms(c, n, xyzq, &dx));
   bool host = false;
+  const Box3 box = ctx_box(c);
+  // one stable sort serves the spread and the gather
   if (c->fp64)
-    TRY(do_spread<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
+    TRY(bin_atoms<double>(c, n, dx, stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false)));
   else
-    TRY(do_spread<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, false));
-  TRY(do_solve(c, c->d_rho, c->d_phi, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true));
+    TRY(bin_atoms<float>(c, n, dx, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false)));
+  if (c->fp64)
+    TRY(do_spread<double>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));
+  else
+    TRY(do_spread<float>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));
+  TRY(do_solve_ctx(c));
   c->phi_valid = true;
   c->energy_valid = true;
   if (fx || fy || fz) {
     if (c->fp64)
-      TRY(gather_to<double>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const double*)c->d_phi, c->p.ccelec,
-                            fx, fy, fz, &host));
+      TRY(gather_to<double>(c, n, dx, box.v, c->sigma1, c->rcut1, (const double*)c->d_phi,
+                            c->p.ccelec, fx, fy, fz, &host, true));
     else
-      TRY(gather_to<float>(c, n, dx, ctx_box(c).v, c->sigma1, c->rcut1, (const float*)c->d_phi, c->p.ccelec,
-                           fx, fy, fz, &host));
+      TRY(gather_to<float>(c, n, dx, box.v, c->sigma1, c->rcut1, (const float*)c->d_phi,
+                           c->p.ccelec, fx, fy, fz, &host, true));
   }
   TRY(energy_out(c, energy, &host));
   return finish(c, host);

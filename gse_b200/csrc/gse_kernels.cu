@@ -224,6 +224,56 @@ __global__ void __launch_bounds__(256)
   if (g.want_energy) block_sum_to(e, partials);
 }
 
+// G(k) of CpuGreensFuncGSE.cpp:28-56 evaluated once in FP64 for every bin of
+// the half spectrum and stored in CT (0 at k = 0).
+template <typename CT>
+__global__ void k_green_table(GreenGeom g, CT* __restrict__ tab) {
+  const long long total = (long long)g.sizeX * g.nfft[1] * g.nfft[2];
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    if (idx == 0) {
+      tab[0] = (CT)0;
+      continue;
+    }
+    const int ix = (int)(idx % g.sizeX);
+    const long long r = idx / g.sizeX;
+    const int iy = (int)(r % g.nfft[1]);
+    const int iz = (int)(r / g.nfft[1]);
+    const int kx = (ix >= g.half[0]) ? ix - g.nfft[0] : ix;
+    const int ky = (iy >= g.half[1]) ? iy - g.nfft[1] : iy;
+    const int kz = (iz >= g.half[2]) ? iz - g.nfft[2] : iz;
+    const double kxd = (double)kx * g.twopi_box[0];
+    const double kyd = (double)ky * g.twopi_box[1];
+    const double kzd = (double)kz * g.twopi_box[2];
+    const double kd2 = add_rn(add_rn(mul_rn(kxd, kxd), mul_rn(kyd, kyd)), mul_rn(kzd, kzd));
+    tab[idx] = (CT)(g.fourpi_vol * exp(-g.sigmafac * kd2) / kd2);
+  }
+}
+
+// rhok *= G (table) with the energy sum_k G |rho(k)|^2 over the full
+// spectrum; one block row per (ky, kz) line so the kx weight needs no division.
+template <typename CT>
+__global__ void __launch_bounds__(256)
+    k_green_apply(typename Cplx<CT>::type* __restrict__ rhok, const CT* __restrict__ tab,
+                  GreenGeom g, double* __restrict__ partials) {
+  const int lines = g.nfft[1] * g.nfft[2];
+  double e = 0.0;
+  for (int line = blockIdx.x; line < lines; line += gridDim.x) {
+    const long long base = (long long)line * g.sizeX;
+    for (int ix = threadIdx.x; ix < g.sizeX; ix += blockDim.x) {
+      auto v = rhok[base + ix];
+      const CT f = tab[base + ix];
+      const double re = (double)v.x, im = (double)v.y;
+      const double wgt = (ix == 0 || (g.nx_even && ix == g.nfft[0] / 2)) ? 1.0 : 2.0;
+      e += wgt * (double)f * (re * re + im * im);
+      v.x *= f;
+      v.y *= f;
+      rhok[base + ix] = v;
+    }
+  }
+  block_sum_to(e, partials);
+}
+
 // sum_i (double)(a[i]*b[i]) per block (the product in CT, as CpuGSE.cpp:97)
 template <typename CT>
 __global__ void __launch_bounds__(256)
@@ -387,6 +437,21 @@ cudaError_t launch_green_energy(typename Cplx<CT>::type* rhok, const GreenGeom& 
 }
 
 template <typename CT>
+cudaError_t launch_green_table(const GreenGeom& g, CT* tab, cudaStream_t st) {
+  k_green_table<CT><<<148 * 8, 256, 0, st>>>(g, tab);
+  return cudaGetLastError();
+}
+
+template <typename CT>
+cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
+                               double* partials, int np, double factor, double* energy_out,
+                               cudaStream_t st) {
+  k_green_apply<CT><<<np, 128, 0, st>>>(rhok, tab, g, partials);
+  k_energy_finalize<<<1, 1024, 0, st>>>(partials, np, factor, energy_out);
+  return cudaGetLastError();
+}
+
+template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st) {
   k_dot<CT><<<np, 256, 0, st>>>(a, b, size, partials);
@@ -413,6 +478,9 @@ cudaError_t launch_gather(const typename Vec4<CT>::type* xyzq, const int* perm, 
                                          long long*, cudaStream_t);                            \
   template cudaError_t launch_green_energy<CT>(Cplx<CT>::type*, const GreenGeom&, double*,     \
                                                int, double, double*, cudaStream_t);            \
+  template cudaError_t launch_green_table<CT>(const GreenGeom&, CT*, cudaStream_t);             \
+  template cudaError_t launch_green_apply<CT>(Cplx<CT>::type*, const CT*, const GreenGeom&,     \
+                                              double*, int, double, double*, cudaStream_t);     \
   template cudaError_t launch_dot_energy<CT>(const CT*, const CT*, long long, double*, int,    \
                                              double, double*, cudaStream_t);                   \
   template cudaError_t launch_gather<CT>(const Vec4<CT>::type*, const int*, int,               \

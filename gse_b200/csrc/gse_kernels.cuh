@@ -41,6 +41,14 @@ cudaError_t launch_green_energy(typename Cplx<CT>::type* rhok, const GreenGeom& 
                                 cudaStream_t st);
 
 template <typename CT>
+cudaError_t launch_green_table(const GreenGeom& g, CT* tab, cudaStream_t st);
+
+template <typename CT>
+cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
+                               double* partials, int np, double factor, double* energy_out,
+                               cudaStream_t st);
+
+template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st);
 

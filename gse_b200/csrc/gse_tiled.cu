@@ -1,0 +1,1036 @@
+// gse_tiled.cu -- the tiled spread and gather kernels of the GSE-k path.
+//
+//  binning   atoms are counting-sorted by (z cell, y cell, x-bin of kBinX cells)
+//            of their stencil centre round(x/h) mod M, stable in the original
+//            index, so every later sum runs in a fixed order.
+//  spread    CpuGaussCharge::spreadChargeToGrid (CpuGaussCharge.cpp:235-384):
+//            output-stationary.  A CTA owns a kTX x kTY x TZ block of the grid;
+//            each thread owns one (x, y) column of it with TZ accumulators in
+//            registers.  The atoms whose (2n+1)^3 cube reaches the block
+//            stream through shared memory in chunks; each warp keeps the ones
+//            that touch its 8 x 4 column patch and adds their 2n+1 z weights
+//            into its registers.  No atomics; every grid point is written
+//            once.
+//  gather    CpuGaussCharge::interpolateLoop (CpuGaussCharge.cpp:105-172): a
+//            CTA owns the atoms of a kBG^3-cell brick and stages the potential
+//            of the brick plus its n-cell halo in shared memory; one warp per
+//            atom, lanes over the non-empty (y, z) rows of its sphere.
+#include "gse_internal.cuh"
+#include "gse_tiled.cuh"
+
+namespace gse {
+
+// ===========================================================================
+// Binning
+// ===========================================================================
+template <typename CT>
+__device__ __forceinline__ int centre_cell(CT v, CT inv_h) {
+  return round_to_int(mul_rn(v, inv_h));
+}
+
+template <typename CT>
+__global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, int n, BinLayout b,
+                            CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
+                            int* __restrict__ counts, unsigned* __restrict__ qmax_bits) {
+  float qm = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const auto a = xyzq[i];
+    qm = fmaxf(qm, fabsf((float)a.w));
+    const int cx = pmod(centre_cell(a.x, inv_hx), b.M[0]);
+    const int cy = pmod(centre_cell(a.y, inv_hy), b.M[1]);
+    const int cz = pmod(centre_cell(a.z, inv_hz), b.M[2]);
+    const int k = (cz * b.M[1] + cy) * b.nbx + cx / kBinX;
+    key[i] = k;
+    atomicAdd(&counts[k], 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
+  // non-negative floats order like their bit patterns (NaN compares largest)
+  if ((threadIdx.x & 31) == 0) atomicMax(qmax_bits, __float_as_uint(qm));
+}
+
+// Three-phase exclusive scan of counts[0..nb) into start[0..nb].
+constexpr int kScanPer = 4;
+constexpr int kScanThreads = 1024;
+constexpr int kScanTile = kScanPer * kScanThreads;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int ws[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    int s = (lane < nw) ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    ws[lane] = s;
+  }
+  __syncthreads();
+  const int before = (w > 0 ? ws[w - 1] : 0) + x - v;
+  if (total) *total = ws[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_tiles(const int* __restrict__ counts, int nb, int* __restrict__ start,
+                 int* __restrict__ tile_sums) {
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+  int v[kScanPer];
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; j++) {
+    v[j] = (base + j < nb) ? counts[base + j] : 0;
+    s += v[j];
+  }
+  int total;
+  int run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int j = 0; j < kScanPer; j++) {
+    if (base + j < nb) start[base + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_sums(int* __restrict__ tile_sums, int ntiles, int* __restrict__ start, int nb) {
+  // ntiles <= kScanTile (checked by the launcher)
+  const int base = threadIdx.x * kScanPer;
+  int v[kScanPer];
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanPer; j++) {
+    v[j] = (base + j < ntiles) ? tile_sums[base + j] : 0;
+    s += v[j];
+  }
+  int total;
+  int run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int j = 0; j < kScanPer; j++) {
+    if (base + j < ntiles) tile_sums[base + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) start[nb] = total;
+}
+
+__global__ void k_scan_add(int* __restrict__ start, int nb, const int* __restrict__ tile_sums) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nb) start[i] += tile_sums[i / kScanTile];
+}
+
+// Unordered placement: fill[] counts up from zero per bin.
+__global__ void k_bin_place_any(int n, const int* __restrict__ key, const int* __restrict__ start,
+                                int* __restrict__ fill, int* __restrict__ tmp) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = key[i];
+    tmp[start[k] + atomicAdd(&fill[k], 1)] = i;
+  }
+}
+
+// Stable placement: an atom's rank in its bin is the number of bin members
+// with a smaller original index.
+template <typename CT>
+__global__ void k_bin_place_stable(const typename Vec4<CT>::type* __restrict__ xyzq, int n,
+                                   const int* __restrict__ key, const int* __restrict__ start,
+                                   const int* __restrict__ tmp,
+                                   typename Vec4<CT>::type* __restrict__ sorted,
+                                   int* __restrict__ perm) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = key[i];
+    const int s = start[k], e = start[k + 1];
+    int r = 0;
+    for (int j = s; j < e; j++) r += (tmp[j] < i);
+    sorted[s + r] = xyzq[i];
+    perm[s + r] = i;
+  }
+}
+
+// ===========================================================================
+// Spread
+// ===========================================================================
+// Accumulator / z-weight types of the spread.  FP64 form: double
+// accumulators and weights.  Mixed form: the z weights are int32 fixed point
+// (kWzBits fraction bits), the (x, y) factor t = q pref wx wy is rounded to
+// int32 with a per-launch scale, and each product t_int * wz_int is added
+// exactly into an int64 accumulator (one mad.wide.s32), so the grid sum is
+// independent of the order of the contributions.
+template <typename CT> struct SpreadTypes;
+template <> struct SpreadTypes<double> {
+  typedef double Acc;
+  typedef double Wz;
+  typedef double T;
+};
+template <> struct SpreadTypes<float> {
+  typedef long long Acc;
+  typedef int Wz;
+  typedef int T;
+};
+constexpr int kWzBits = 26;
+
+__device__ __forceinline__ double madd(double t, double w, double a) { return fma(t, w, a); }
+__device__ __forceinline__ long long madd(int t, int w, long long a) {
+  return a + (long long)t * (long long)w;
+}
+
+template <typename CT>
+struct SpreadRec {
+  int s[3];                                // first stencil cell relative to the block origin
+  CT qp;                                   // q * (2 pi sigma^2)^(-3/2)
+  CT w[2][kWPad];                          // x and y weights
+  typename SpreadTypes<CT>::Wz wz[kWPad];  // z weights (fixed point in the mixed form)
+};
+
+// acc[OZ + k] += t * wz[k] for the k that land inside the block (compile-time
+// indices, so the accumulators stay in registers).
+template <typename A, typename T, typename WZ, int TZ, int W, int OZ>
+__device__ __forceinline__ void add_column(A (&acc)[TZ], T t, const WZ (&wz)[kWPad]) {
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    if (OZ + k >= 0 && OZ + k < TZ) acc[OZ + k] = madd(t, wz[k], acc[OZ + k]);
+  }
+}
+
+#define GSE_ZC(i) \
+  case i: add_column<A, T, WZ, TZ, W, (i) - (W - 1)>(acc, t, wz); break;
+#define GSE_ZC8(i) GSE_ZC(i) GSE_ZC(i + 1) GSE_ZC(i + 2) GSE_ZC(i + 3) GSE_ZC(i + 4) GSE_ZC(i + 5) \
+  GSE_ZC(i + 6) GSE_ZC(i + 7)
+
+// The block-relative z offset oz is the same for the whole warp: one
+// indirect branch selects the unrolled case.
+template <typename A, typename T, typename WZ, int TZ, int W>
+__device__ __forceinline__ void add_column_dispatch(int oz, A (&acc)[TZ], T t,
+                                                    const WZ (&wz)[kWPad]) {
+  static_assert(TZ + W - 1 <= 96, "z dispatch covers 96 offsets");
+  switch (oz + W - 1) {
+    GSE_ZC8(0) GSE_ZC8(8) GSE_ZC8(16) GSE_ZC8(24) GSE_ZC8(32) GSE_ZC8(40)
+    GSE_ZC8(48) GSE_ZC8(56) GSE_ZC8(64) GSE_ZC8(72) GSE_ZC8(80) GSE_ZC8(88)
+    default: break;
+  }
+}
+#undef GSE_ZC8
+#undef GSE_ZC
+
+// 1-D weights w[j] = exp(-(dc + (j - n) h)^2 / (2 sigma^2)), j < W = 2n+1,
+// where dc = c h - x is the offset of the stencil centre (the reference's
+// d0 + j h with d0 = (c - n) h - x, CpuGaussCharge.cpp:311-329).  Evaluated
+// outward from the centre by the exact ratio recurrence
+//   w[n+k] = w[n+k-1] ru[k-1],  ru[k] = ru[k-1] exp(-2 h^2/(2 sigma^2)),
+// and the mirror image below the centre.  The decay factor is applied as an
+// unevaluated sum hi + lo so that its rounding does not compound.
+template <typename CT, int W>
+__device__ __forceinline__ void gauss_row(CT dc, CT h, CT inv_2s2, CT dec_hi, CT dec_lo,
+                                          CT (&w)[kWPad]) {
+  constexpr int n = (W - 1) / 2;
+  const CT wc = gexp(mul_rn(mul_rn(-dc, dc), inv_2s2));
+  const CT hh = h * h;
+  CT ru = gexp(-(2 * dc * h + hh) * inv_2s2);   // w[n+1] / w[n]
+  CT rd = gexp(-(hh - 2 * dc * h) * inv_2s2);   // w[n-1] / w[n]
+  w[n] = wc;
+  CT wu = wc, wd = wc;
+#pragma unroll
+  for (int k = 1; k <= n; k++) {
+    wu *= ru;
+    wd *= rd;
+    w[n + k] = wu;
+    w[n - k] = wd;
+    ru = fma(ru, dec_hi, ru * dec_lo);
+    rd = fma(rd, dec_hi, rd * dec_lo);
+  }
+#pragma unroll
+  for (int j = W; j < kWPad; j++) w[j] = (CT)0;
+}
+
+template <typename CT, int TZ, int W>
+__global__ void __launch_bounds__(kSpreadThreads)
+    k_spread_tiled(const typename Vec4<CT>::type* __restrict__ sorted,
+                   const int* __restrict__ start, const unsigned* __restrict__ qmax_bits,
+                   BinLayout b, Stencil<CT> s, Decay<CT> dec, CT* __restrict__ grid) {
+  constexpr int n = (W - 1) / 2;
+  constexpr int CH = sizeof(CT) == 8 ? kSpreadChunk : 2 * kSpreadChunk;
+  constexpr int NT = kSpreadThreads;
+  constexpr bool FIXED = sizeof(CT) == 4;
+  typedef typename Vec4<CT>::type V;
+  typedef typename SpreadTypes<CT>::Acc A;
+  typedef typename SpreadTypes<CT>::T T;
+  typedef typename SpreadTypes<CT>::Wz WZ;
+  __shared__ SpreadRec<CT> rec[CH];
+  __shared__ int chunk_atom[CH];
+  __shared__ short chunk_shift[CH][3];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * TZ;
+  const int ex = min(kTX, b.M[0] - x0), ey = min(kTY, b.M[1] - y0), ez = min(TZ, b.M[2] - z0);
+  // warp patch: 8 (x) x 4 (y); lane -> one column
+  const int px0 = (warp & 1) * 8, py0 = (warp >> 1) * 4;
+  const int cx = px0 + (lane & 7), cy = py0 + (lane >> 3);
+
+  // mixed form: t is rounded to int32 at 2^st; choose st so that
+  // |q pref| 2^st < 2^31 for every atom of the launch
+  int st = 0;
+  float tscale = 1.f;
+  if (FIXED) {
+    const float qpm = __uint_as_float(*qmax_bits) * fabsf((float)s.pref);
+    st = 30;
+    if (!(qpm < 3.0e38f)) {
+      st = 0;
+    } else {
+      while (st > 0 && qpm * exp2f((float)st) >= 2.0e9f) st--;
+    }
+    tscale = exp2f((float)st);
+  }
+
+  A acc[TZ];
+#pragma unroll
+  for (int z = 0; z < TZ; z++) acc[z] = (A)0;
+
+  // rows (uy, uz) of the relevant region, unwrapped cell coordinates
+  const int ry0 = y0 - n, rz0 = z0 - n;
+  const int nry = ey + 2 * n, nrz = ez + 2 * n;
+  const int nrows = nry * nrz;
+  const int ux_lo = x0 - n, ux_hi = x0 + ex + n;  // [lo, hi)
+
+  for (int rbase = 0; rbase < nrows; rbase += NT) {
+    // --- this thread's row: wrapped x segments -> atom ranges ---
+    const int r = rbase + tid;
+    int seg_a[kMaxSeg], seg_e[kMaxSeg], seg_sh[kMaxSeg];
+    int nseg = 0, cnt = 0, shy = 0, shz = 0;
+    if (r < nrows) {
+      const int uy = ry0 + r % nry, uz = rz0 + r / nry;
+      const int ccy = pmod(uy, b.M[1]), ccz = pmod(uz, b.M[2]);
+      shy = uy - ccy;
+      shz = uz - ccz;
+      const int rowkey = (ccz * b.M[1] + ccy) * b.nbx;
+      int u = ux_lo;
+      while (u < ux_hi && nseg < kMaxSeg) {
+        const int cu = pmod(u, b.M[0]);
+        const int seg_end = min(ux_hi, u + (b.M[0] - cu));  // end of this period
+        const int c1 = cu + (seg_end - u);                  // exclusive cell end
+        const int a0 = start[rowkey + cu / kBinX];
+        const int a1 = start[rowkey + (c1 - 1) / kBinX + 1];
+        seg_a[nseg] = a0;
+        seg_e[nseg] = a1;
+        seg_sh[nseg] = u - cu;
+        cnt += a1 - a0;
+        nseg++;
+        u = seg_end;
+      }
+    }
+    int total;
+    const int pos0 = block_exclusive_scan(cnt, &total);
+    for (int sub = 0; sub < total; sub += CH) {
+      // --- copy this thread's atoms with group positions in [sub, sub+CH) ---
+      int p = pos0;
+      for (int g = 0; g < nseg; g++) {
+        for (int j = seg_a[g]; j < seg_e[g]; j++, p++) {
+          if (p >= sub && p < sub + CH) {
+            chunk_atom[p - sub] = j;
+            chunk_shift[p - sub][0] = (short)seg_sh[g];
+            chunk_shift[p - sub][1] = (short)shy;
+            chunk_shift[p - sub][2] = (short)shz;
+          }
+        }
+      }
+      __syncthreads();
+      const int cntc = min(CH, total - sub);
+      // --- per-atom records ---
+      for (int i = tid; i < cntc; i += NT) {
+        const V a = sorted[chunk_atom[i]];
+        const CT pos[3] = {a.x, a.y, a.z};
+        const int org[3] = {x0, y0, z0};
+        CT wz[kWPad];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const int c = centre_cell(pos[d], s.inv_h[d]);
+          const CT dc = sub_rn(mul_rn((CT)c, s.h[d]), pos[d]);
+          CT w[kWPad];
+          gauss_row<CT, W>(dc, s.h[d], s.inv_2s2, dec.hi[d], dec.lo[d], w);
+          if (d < 2) {
+#pragma unroll
+            for (int j = 0; j < kWPad; j++) rec[i].w[d][j] = w[j];
+          } else {
+#pragma unroll
+            for (int j = 0; j < kWPad; j++) wz[j] = w[j];
+          }
+          rec[i].s[d] = pmod(c, s.M[d]) + chunk_shift[i][d] - n - org[d];
+        }
+#pragma unroll
+        for (int j = 0; j < kWPad; j++) {
+          if (FIXED)
+            rec[i].wz[j] = (WZ)__float2int_rn((float)wz[j] * (float)(1 << kWzBits));
+          else
+            rec[i].wz[j] = (WZ)wz[j];
+        }
+        rec[i].qp = a.w * s.pref;
+      }
+      __syncthreads();
+      // --- each warp: atoms that touch its patch ---
+      for (int base = 0; base < cntc; base += 32) {
+        const int i = base + lane;
+        bool rel = false;
+        if (i < cntc) {
+          const int sx = rec[i].s[0], sy = rec[i].s[1], sz = rec[i].s[2];
+          rel = sx <= px0 + 7 && sx + W - 1 >= px0 && sy <= py0 + 3 && sy + W - 1 >= py0 &&
+                sz <= ez - 1 && sz + W - 1 >= 0;
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, rel);
+        while (mask) {
+          const int ia = base + __ffs(mask) - 1;
+          mask &= mask - 1;
+          const int kx = cx - rec[ia].s[0], ky = cy - rec[ia].s[1];
+          CT tf = (CT)0;
+          if ((unsigned)kx < (unsigned)W && (unsigned)ky < (unsigned)W)
+            tf = rec[ia].qp * rec[ia].w[0][kx] * rec[ia].w[1][ky];
+          T t;
+          if (FIXED)
+            t = (T)__float2int_rn((float)tf * tscale);
+          else
+            t = (T)tf;
+          WZ wz[kWPad];
+#pragma unroll
+          for (int k = 0; k < kWPad; k++) wz[k] = rec[ia].wz[k];
+          add_column_dispatch<A, T, WZ, TZ, W>(rec[ia].s[2], acc, t, wz);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // --- write the block: every point exactly once ---
+  if (cx < ex && cy < ey) {
+    CT* col = grid + (long long)(x0 + cx) + (long long)(y0 + cy) * b.M[0];
+    const long long zs = (long long)b.M[0] * b.M[1];
+    const double unscale = FIXED ? exp2(-(double)(st + kWzBits)) : 1.0;
+#pragma unroll
+    for (int z = 0; z < TZ; z++) {
+      if (z < ez) {
+        if (FIXED)
+          col[(long long)(z0 + z) * zs] = (CT)((double)acc[z] * unscale);
+        else
+          col[(long long)(z0 + z) * zs] = (CT)acc[z];
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// Mixed-form spread: atom-stationary scatter into a shared int32 brick tile
+// ===========================================================================
+// A CTA owns the atoms of one kSB^3-cell brick and a shared tile of the brick
+// plus its n-cell halo, T = kSB + 2n points per axis, in int32 fixed point at
+// a scale 2^S chosen for this brick so that no partial sum can overflow
+// (|q| pref summed over the brick's atoms, times 2^S, stays below 2^30).
+// One warp per atom: lanes take (x, z) pairs of the (2n+1)^2 plane, form
+// t = round(q pref wx wz 2^(S+1)) and add round(t wy_int / 2^32) with
+// wy_int = round(wy (2^31 - 1)) for each of the 2n+1 y values -- one
+// mad.wide.s32 and one shared-memory integer reduction per cube point.
+// The z-plane pitch is congruent to 2n+1 mod 32, so the 32 lanes of an
+// instruction (consecutive (x, z) pairs) hit 32 different banks.
+// The tile goes to its slot of a halo buffer; k_spread_fold sums the
+// overlapping tiles in a fixed order into the grid.
+template <int W>
+struct ScatterGeom {
+  static constexpr int n = (W - 1) / 2;
+  static constexpr int T = kSB + 2 * n;
+  static constexpr int RP = T;                              // y pitch
+  static constexpr int PP = ((T * T + 31) / 32) * 32 + W;   // z pitch, = W (mod 32)
+  static constexpr int words = T * PP;
+};
+
+template <int W>
+__global__ void __launch_bounds__(kScatterThreads)
+    k_spread_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
+                     BinLayout b, Stencil<float> s, int* __restrict__ halo,
+                     double* __restrict__ halo_scale) {
+  typedef ScatterGeom<W> G;
+  constexpr int n = G::n, T = G::T;
+  constexpr int NT = kScatterThreads, NW = NT / 32;
+  constexpr int NPASS = (W * W + 31) / 32;
+  extern __shared__ int tile[];
+  __shared__ int rng_a[kSB * kSB], rng_p[kSB * kSB];
+  __shared__ int alist[kScatterList];
+  __shared__ float qsum_w[NW], qmax_w[NW];
+  __shared__ int s_shift;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = blockIdx.x * kSB, y0 = blockIdx.y * kSB, z0 = blockIdx.z * kSB;
+  const int brick = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const int ex = min(kSB, b.M[0] - x0), ey = min(kSB, b.M[1] - y0), ez = min(kSB, b.M[2] - z0);
+
+  // the brick's atoms: one range per (y, z) cell row
+  int cnt = 0, a0 = 0;
+  if (tid < kSB * kSB) {
+    const int yy = tid % kSB, zz = tid / kSB;
+    if (yy < ey && zz < ez) {
+      const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
+      a0 = start[rowkey + x0 / kBinX];
+      cnt = start[rowkey + (x0 + ex - 1) / kBinX + 1] - a0;
+    }
+  }
+  int total;
+  const int pos = block_exclusive_scan(cnt, &total);
+  if (tid < kSB * kSB) {
+    rng_a[tid] = a0;
+    rng_p[tid] = pos;
+  }
+  for (int i = tid; i < G::words / 4; i += NT)
+    reinterpret_cast<int4*>(tile)[i] = make_int4(0, 0, 0, 0);
+  for (int i = (G::words / 4) * 4 + tid; i < G::words; i += NT) tile[i] = 0;
+  // fixed-point scale of this brick: every contribution below 2^22 and every
+  // partial sum below 2^30
+  float qs = 0.f, qm = 0.f;
+  for (int j = 0; j < cnt; j++) {
+    const float q = fabsf(sorted[a0 + j].w);
+    qs += q;
+    qm = fmaxf(qm, q);
+  }
+  qs = warp_sum(qs);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
+  if (lane == 0) {
+    qsum_w[warp] = qs;
+    qmax_w[warp] = qm;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float q = 0.f, m = 0.f;
+    for (int w = 0; w < NW; w++) {
+      q += qsum_w[w];
+      m = fmaxf(m, qmax_w[w]);
+    }
+    const double pref = fabs((double)s.pref);
+    const double sum_b = (double)q * pref * 1.0001 + 1e-30;
+    const double one_b = (double)m * pref * 1.0001 + 1e-30;
+    int sh = 40;
+    while (sh > -60 && (sum_b * exp2((double)sh) >= 1073741824.0 ||
+                        one_b * exp2((double)sh) >= 4194304.0))
+      sh--;
+    s_shift = sh;
+    halo_scale[brick] = exp2(-(double)sh);
+  }
+  __syncthreads();
+  const float tscale = exp2f((float)s_shift);
+
+  // per-lane (x, z) pair of each pass and its tile offset: the same for all atoms
+  int poff[NPASS], psx[NPASS], psz[NPASS];
+#pragma unroll
+  for (int pass = 0; pass < NPASS; pass++) {
+    const int p = pass * 32 + lane;
+    const int pz = p < W * W ? p / W : 0, px = p < W * W ? p - (p / W) * W : 0;
+    psx[pass] = px;
+    psz[pass] = pz;
+    poff[pass] = pz * G::PP + px;
+  }
+
+  for (int c0 = 0; c0 < total; c0 += kScatterList) {
+    // flat list of this chunk's atoms
+    for (int r = tid; r < kSB * kSB; r += NT) {
+      const int p0 = rng_p[r];
+      const int p1 = (r + 1 < kSB * kSB) ? rng_p[r + 1] : total;
+      for (int p = max(p0, c0); p < min(p1, c0 + kScatterList); p++)
+        alist[p - c0] = rng_a[r] + (p - p0);
+    }
+    __syncthreads();
+    const int nc = min(kScatterList, total - c0);
+    for (int q = warp; q < nc; q += NW) {
+      const float4 a = sorted[alist[q]];
+      const float pos3[3] = {a.x, a.y, a.z};
+      const int org[3] = {x0, y0, z0};
+      int loc[3];
+      float wl[3];  // lane j < W: weight j along each axis
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int c = centre_cell(pos3[d], s.inv_h[d]);
+        loc[d] = pmod(c, s.M[d]) - org[d];  // window start in tile coordinates
+        const float dd = sub_rn(mul_rn((float)(c - n + lane), s.h[d]), pos3[d]);
+        wl[d] = (lane < W) ? expf(mul_rn(mul_rn(-dd, dd), s.inv_2s2)) : 0.f;
+      }
+      float wy[W];
+#pragma unroll
+      for (int k = 0; k < W; k++) wy[k] = __shfl_sync(0xffffffffu, wl[1], k);
+      const float qp = a.w * s.pref * tscale;
+      int* base = tile + loc[2] * G::PP + loc[1] * G::RP + loc[0];
+#pragma unroll
+      for (int pass = 0; pass < NPASS; pass++) {
+        const float wx = __shfl_sync(0xffffffffu, wl[0], psx[pass]);
+        const float wz = __shfl_sync(0xffffffffu, wl[2], psz[pass]);
+        if (pass * 32 + lane < W * W) {
+          const float t = qp * wx * wz;
+          int* cell = base + poff[pass];
+#pragma unroll
+          for (int k = 0; k < W; k++) {
+            // round(t wy): |t wy| < 2^22, so 1.5*2^23 + t wy has unit spacing
+            const int v = __float_as_int(fmaf(t, wy[k], 12582912.0f)) - 0x4B400000;
+            atomicAdd(cell + k * G::RP, v);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // tile -> halo slot [z][y][x], T^3 ints
+  int* dst = halo + (long long)brick * (T * T * T);
+  for (int i = tid; i < T * T * T; i += NT) {
+    const int zz = i / (T * T);
+    dst[i] = tile[zz * G::PP + (i - zz * T * T)];
+  }
+}
+
+// rho(x, y, z) = sum over the brick tiles covering the point of
+// tile value * 2^-S(brick), in a fixed order (the cover lists).
+template <int W>
+__global__ void k_spread_fold(const int* __restrict__ halo, const double* __restrict__ halo_scale,
+                              BinLayout b, int nbx, int nby, const short2* __restrict__ cover,
+                              int cov_stride, float* __restrict__ rho) {
+  constexpr int T = ScatterGeom<W>::T;
+  constexpr int kFast = 2;  // covers per axis handled without a loop
+  constexpr int ZP = kFoldZ;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, zb = blockIdx.z * ZP;
+  if (x >= b.M[0]) return;
+  const short2* cx = cover + (0 * cov_stride + x) * kMaxCover;
+  const short2* cy = cover + (1 * cov_stride + y) * kMaxCover;
+  const bool fast_xy = cx[kFast].x < 0 && cy[kFast].x < 0;
+  short2 ex[kFast], ey[kFast];
+#pragma unroll
+  for (int i = 0; i < kFast; i++) {
+    ex[i] = cx[i];
+    ey[i] = cy[i];
+  }
+#pragma unroll
+  for (int zi = 0; zi < ZP; zi++) {
+    const int z = zb + zi;
+    if (z >= b.M[2]) break;
+    const short2* cz = cover + (2 * cov_stride + z) * kMaxCover;
+    double acc = 0.0;
+    if (fast_xy && cz[kFast].x < 0) {
+      int v[kFast * kFast * kFast];
+      int br[kFast * kFast * kFast];
+#pragma unroll
+      for (int i = 0; i < kFast; i++) {
+        const short2 ez = cz[i];
+#pragma unroll
+        for (int j = 0; j < kFast; j++)
+#pragma unroll
+          for (int k = 0; k < kFast; k++) {
+            const int e = (i * kFast + j) * kFast + k;
+            const bool ok = ez.x >= 0 && ey[j].x >= 0 && ex[k].x >= 0;
+            br[e] = ok ? (ez.x * nby + ey[j].x) * nbx + ex[k].x : -1;
+            v[e] = ok ? halo[(long long)br[e] * (T * T * T) + (ez.y * T + ey[j].y) * T + ex[k].y]
+                      : 0;
+          }
+      }
+#pragma unroll
+      for (int e = 0; e < kFast * kFast * kFast; e++)
+        if (br[e] >= 0) acc += (double)v[e] * halo_scale[br[e]];
+    } else {
+      for (int i = 0; i < kMaxCover && cz[i].x >= 0; i++)
+        for (int j = 0; j < kMaxCover && cy[j].x >= 0; j++)
+          for (int k = 0; k < kMaxCover && cx[k].x >= 0; k++) {
+            const int brk = (cz[i].x * nby + cy[j].x) * nbx + cx[k].x;
+            acc += (double)halo[(long long)brk * (T * T * T) + (cz[i].y * T + cy[j].y) * T +
+                                cx[k].y] *
+                   halo_scale[brk];
+          }
+    }
+    rho[x + ((long long)y + (long long)z * b.M[1]) * b.M[0]] = (float)acc;
+  }
+}
+
+// ===========================================================================
+// Gather
+// ===========================================================================
+// Sphere test of one stencil point.  FP64 form: the reference's own sum and
+// order, (dx^2 + dy^2) + dz^2 < rcut^2 (CpuGaussCharge.cpp:157-158), so the
+// point set is bit-identical.  Mixed form: dx^2 < rcut^2 - (dy^2 + dz^2).
+template <typename CT>
+__device__ __forceinline__ bool in_sphere(CT dx2, CT dy2, CT dz2, CT rem, CT rcut2);
+template <>
+__device__ __forceinline__ bool in_sphere<double>(double dx2, double dy2, double dz2, double,
+                                                  double rcut2) {
+  return add_rn(add_rn(dx2, dy2), dz2) < rcut2;
+}
+template <>
+__device__ __forceinline__ bool in_sphere<float>(float dx2, float, float, float rem, float) {
+  return dx2 < rem;
+}
+
+// s0 = sum_k m_k wx[k] row[k], s1 = sum_k m_k wx[k] dx[k] row[k] over the
+// 2n+1 points of one stencil row, m_k the sphere test.
+template <typename CT, int W>
+__device__ __forceinline__ void row_sums(const CT* row, const CT (&dx2)[W], const CT (&wx)[W],
+                                         const CT (&wdx)[W], CT dy2, CT dz2, CT rem, CT rcut2,
+                                         CT& s0, CT& s1) {
+  s0 = (CT)0;
+  s1 = (CT)0;
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    const CT ph = in_sphere<CT>(dx2[k], dy2, dz2, rem, rcut2) ? row[k] : (CT)0;
+    s0 = fma(wx[k], ph, s0);
+    s1 = fma(wdx[k], ph, s1);
+  }
+}
+
+// FP32: both sums in one packed fma.rn.f32x2 per point (sm_100).
+template <>
+__device__ __forceinline__ void row_sums<float, 13>(const float* row, const float (&dx2)[13],
+                                                    const float (&wx)[13], const float (&wdx)[13],
+                                                    float, float, float rem, float, float& s0,
+                                                    float& s1) {
+  unsigned long long acc = 0ull;  // (s0, s1) packed, both +0.0f
+#pragma unroll
+  for (int k = 0; k < 13; k++) {
+    const float ph = dx2[k] < rem ? row[k] : 0.f;
+    unsigned long long w2, p2;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(w2) : "f"(wx[k]), "f"(wdx[k]));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(p2) : "f"(ph));
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2), "l"(p2));
+  }
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(acc));
+}
+
+template <typename CT, int W>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_gather_tiled(const typename Vec4<CT>::type* __restrict__ sorted,
+                   const int* __restrict__ perm, const int* __restrict__ start, BinLayout b,
+                   Stencil<CT> s, const CT* __restrict__ phi, double outscale,
+                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  constexpr int n = (W - 1) / 2;
+  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
+  constexpr int TP = TX | 1;  // odd row pitch: rows fall in different banks
+  constexpr int NW = kGatherThreads / 32;
+  constexpr int NR = kGY * kGZ;  // cell rows of the brick
+  typedef typename Vec4<CT>::type V;
+  extern __shared__ __align__(16) unsigned char gsm[];
+  CT* tile = (CT*)gsm;                                   // [TZ][TY][TP]
+  CT* tabs = tile + TZ * TY * TP;                        // [NW][3][3][kWPad]
+  int* rowl = (int*)(tabs + NW * 3 * 3 * kWPad);         // [NW][W*W]
+  __shared__ int rng_a[NR], rng_p[NR + 1];
+  __shared__ int alist[kGatherList];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = blockIdx.x * kGX, y0 = blockIdx.y * kGY, z0 = blockIdx.z * kGZ;
+  const int ex = min(kGX, b.M[0] - x0), ey = min(kGY, b.M[1] - y0), ez = min(kGZ, b.M[2] - z0);
+
+  // atoms of the brick: one range per (y, z) cell row
+  int cnt = 0;
+  if (tid < NR) {
+    const int yy = tid % kGY, zz = tid / kGY;
+    int a0 = 0, a1 = 0;
+    if (yy < ey && zz < ez) {
+      const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
+      a0 = start[rowkey + x0 / kBinX];
+      a1 = start[rowkey + (x0 + ex - 1) / kBinX + 1];
+    }
+    rng_a[tid] = a0;
+    cnt = a1 - a0;
+  }
+  int natoms;
+  const int pos = block_exclusive_scan(cnt, &natoms);
+  if (tid < NR) rng_p[tid] = pos;
+  if (tid == 0) rng_p[NR] = natoms;
+  if (natoms == 0) return;  // uniform: natoms is the same in every thread
+
+  // potential of the brick plus halo, one (y, z) row per warp iteration
+  const long long zs = (long long)b.M[0] * b.M[1];
+  for (int r = warp; r < TY * TZ; r += NW) {
+    const int ty = r % TY, tz = r / TY;
+    const int gy = pmod(y0 - n + ty, b.M[1]);
+    const int gz = pmod(z0 - n + tz, b.M[2]);
+    const CT* src = phi + (long long)gy * b.M[0] + gz * zs;
+    CT* dst = tile + (tz * TY + ty) * TP;
+    for (int tx = lane; tx < TX; tx += 32) dst[tx] = src[pmod(x0 - n + tx, b.M[0])];
+  }
+  __syncthreads();
+
+  CT* tb = tabs + warp * 9 * kWPad;  // [axis][d, d^2, w][j]
+  int* rl = rowl + warp * W * W;
+  // (jy, jz) of the rows each lane tests, the same for every atom
+  constexpr int NG = (W * W + 31) / 32;
+  int gjy[NG], gjz[NG];
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    const int r = g * 32 + lane;
+    gjz[g] = r < W * W ? r / W : 0;
+    gjy[g] = r < W * W ? r - (r / W) * W : 0;
+  }
+  for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
+  for (int r = tid; r < NR; r += kGatherThreads) {
+    const int p0 = rng_p[r], p1 = rng_p[r + 1];
+    for (int p = max(p0, c0); p < min(p1, c0 + kGatherList); p++) alist[p - c0] = rng_a[r] + (p - p0);
+  }
+  __syncthreads();
+  const int nc = min(kGatherList, natoms - c0);
+  for (int q = warp; q < nc; q += NW) {
+    const int ai = alist[q];
+    const V a = sorted[ai];
+    const CT pos3[3] = {a.x, a.y, a.z};
+    const int org[3] = {x0, y0, z0};
+    int loc[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const int c = centre_cell(pos3[d], s.inv_h[d]);
+      loc[d] = pmod(c, s.M[d]) - org[d];  // first stencil cell in tile coordinates
+      if (lane < W) {
+        const CT dd = sub_rn(pos3[d], mul_rn((CT)(c - n + lane), s.h[d]));
+        const CT d2 = mul_rn(dd, dd);
+        tb[(d * 3 + 0) * kWPad + lane] = dd;
+        tb[(d * 3 + 1) * kWPad + lane] = d2;
+        tb[(d * 3 + 2) * kWPad + lane] = gexp(mul_rn(-d2, s.inv_2s2));
+      }
+    }
+    __syncwarp();
+    // non-empty rows (the whole row is outside the sphere when dy^2+dz^2 >= rcut^2)
+    int nrow = 0;
+#pragma unroll
+    for (int g = 0; g < NG; g++) {
+      const int r = g * 32 + lane;
+      bool ne = false;
+      if (r < W * W)
+        ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) < s.rcut2;
+      const unsigned m = __ballot_sync(0xffffffffu, ne);
+      if (ne) rl[nrow + __popc(m & ((1u << lane) - 1u))] = (gjz[g] << 8) | gjy[g];
+      nrow += __popc(m);
+    }
+    __syncwarp();
+    CT dx2[W], wx[W], wdx[W];
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+      dx2[k] = tb[(0 * 3 + 1) * kWPad + k];
+      wx[k] = tb[(0 * 3 + 2) * kWPad + k];
+      wdx[k] = wx[k] * tb[(0 * 3 + 0) * kWPad + k];
+    }
+    // rows accumulate in double (the reference's AT), each row's 2n+1 terms in CT
+    double ax = 0, ay = 0, az = 0;
+    for (int i = lane; i < nrow; i += 32) {
+      const int r = rl[i];
+      const int jz = r >> 8, jy = r & 255;
+      const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
+      const CT rem = s.rcut2 - (dy2 + dz2);
+      const CT* row = tile + ((loc[2] + jz) * TY + (loc[1] + jy)) * TP + loc[0];
+      CT s0, s1;
+      row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
+      const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
+      ax += (double)(wyz * s1);
+      ay += (double)(wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0);
+      az += (double)(wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0);
+    }
+    ax = warp_sum(ax);
+    ay = warp_sum(ay);
+    az = warp_sum(az);
+    if (lane == 0) {
+      const int o = perm[ai];
+      const double f = outscale * (double)(a.w * s.pref);
+      fx[o] = f * ax;
+      fy[o] = f * ay;
+      fz[o] = f * az;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  }
+}
+
+// ===========================================================================
+// Launchers
+// ===========================================================================
+template <typename CT>
+cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const BinLayout& b,
+                              CT inv_hx, CT inv_hy, CT inv_hz, BinScratch w,
+                              typename Vec4<CT>::type* sorted, int* perm, cudaStream_t st) {
+  const int nb = b.M[1] * b.M[2] * b.nbx;
+  const int ntiles = (nb + kScanTile - 1) / kScanTile;
+  if (ntiles > kScanTile) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(w.qmax_bits, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
+  if (n > 0)
+    k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
+                                        w.qmax_bits);
+  k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.start, w.tile_sums);
+  k_scan_sums<<<1, kScanThreads, 0, st>>>(w.tile_sums, ntiles, w.start, nb);
+  k_scan_add<<<(nb + 255) / 256, 256, 0, st>>>(w.start, nb, w.tile_sums);
+  if (n > 0) {
+    e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
+    if (e != cudaSuccess) return e;
+    k_bin_place_any<<<gb, 256, 0, st>>>(n, w.key, w.start, w.counts, w.tmp);
+    k_bin_place_stable<CT><<<gb, 256, 0, st>>>(xyzq, n, w.key, w.start, w.tmp, sorted, perm);
+  }
+  return cudaGetLastError();
+}
+
+template <typename CT, int TZ, int W>
+static cudaError_t spread_w(const typename Vec4<CT>::type* sorted, const int* start,
+                            const unsigned* qmax_bits, const BinLayout& b, const Stencil<CT>& s,
+                            CT* grid, cudaStream_t st) {
+  const Decay<CT> dec = make_decay<CT>(s);
+  dim3 grd((b.M[0] + kTX - 1) / kTX, (b.M[1] + kTY - 1) / kTY, (b.M[2] + TZ - 1) / TZ);
+  k_spread_tiled<CT, TZ, W><<<grd, kSpreadThreads, 0, st>>>(sorted, start, qmax_bits, b, s, dec,
+                                                             grid);
+  return cudaGetLastError();
+}
+
+template <typename CT>
+bool spread_tiled_supported(const Stencil<CT>& s) {
+  for (int d = 0; d < 3; d++)
+    if (s.nst[d] != s.nst[0]) return false;
+  const int W = 2 * s.nst[0] + 1;
+  return W == 9 || W == 11 || W == 13 || W == 15;
+}
+
+template <typename CT>
+cudaError_t launch_spread_tiled(const typename Vec4<CT>::type* sorted, const int* start,
+                                const unsigned* qmax_bits, const BinLayout& b,
+                                const Stencil<CT>& s, CT* grid, cudaStream_t st) {
+  constexpr int TZ = sizeof(CT) == 8 ? kTZ64 : kTZ32;
+  switch (2 * s.nst[0] + 1) {
+    case 9: return spread_w<CT, TZ, 9>(sorted, start, qmax_bits, b, s, grid, st);
+    case 11: return spread_w<CT, TZ, 11>(sorted, start, qmax_bits, b, s, grid, st);
+    case 13: return spread_w<CT, TZ, 13>(sorted, start, qmax_bits, b, s, grid, st);
+    case 15: return spread_w<CT, TZ, 15>(sorted, start, qmax_bits, b, s, grid, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename CT, int W>
+static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* perm,
+                            const int* start, const BinLayout& b, const Stencil<CT>& s,
+                            const CT* phi, double outscale, double* fx, double* fy, double* fz,
+                            cudaStream_t st) {
+  constexpr int n = (W - 1) / 2;
+  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
+  constexpr int TP = TX | 1, NW = kGatherThreads / 32;
+  const size_t smem = sizeof(CT) * (TZ * TY * TP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_gather_tiled<CT, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr[dev] = true;
+  }
+  dim3 grd((b.M[0] + kGX - 1) / kGX, (b.M[1] + kGY - 1) / kGY, (b.M[2] + kGZ - 1) / kGZ);
+  k_gather_tiled<CT, W><<<grd, kGatherThreads, smem, st>>>(sorted, perm, start, b, s, phi,
+                                                          outscale, fx, fy, fz);
+  return cudaGetLastError();
+}
+
+template <typename CT>
+cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int* perm,
+                                const int* start, const BinLayout& b, const Stencil<CT>& s,
+                                const CT* phi, double outscale, double* fx, double* fy,
+                                double* fz, cudaStream_t st) {
+  switch (2 * s.nst[0] + 1) {
+    case 9: return gather_w<CT, 9>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
+    case 11: return gather_w<CT, 11>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
+    case 13: return gather_w<CT, 13>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
+    case 15: return gather_w<CT, 15>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int W>
+static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLayout& b,
+                             const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                             cudaStream_t st) {
+  typedef ScatterGeom<W> G;
+  const size_t smem = sizeof(int) * G::words;
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_spread_scatter<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr[dev] = true;
+  }
+  const int nb[3] = {(b.M[0] + kSB - 1) / kSB, (b.M[1] + kSB - 1) / kSB,
+                     (b.M[2] + kSB - 1) / kSB};
+  k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(
+      sorted, start, b, s, buf.halo, buf.scale);
+  dim3 fg((b.M[0] + 127) / 128, b.M[1], (b.M[2] + kFoldZ - 1) / kFoldZ);
+  k_spread_fold<W><<<fg, 128, 0, st>>>(buf.halo, buf.scale, b, nb[0], nb[1], buf.cover,
+                                        buf.cover_stride, rho);
+  return cudaGetLastError();
+}
+
+size_t scatter_halo_words(const BinLayout& b, int W) {
+  const int T = kSB + (W - 1);
+  const size_t nb = (size_t)((b.M[0] + kSB - 1) / kSB) * ((b.M[1] + kSB - 1) / kSB) *
+                    ((b.M[2] + kSB - 1) / kSB);
+  return nb * (size_t)T * T * T;
+}
+
+size_t scatter_brick_count(const BinLayout& b) {
+  return (size_t)((b.M[0] + kSB - 1) / kSB) * ((b.M[1] + kSB - 1) / kSB) *
+         ((b.M[2] + kSB - 1) / kSB);
+}
+
+bool scatter_cover_table(const BinLayout& b, int W, std::vector<short2>& out, int* stride) {
+  const int n = (W - 1) / 2, T = kSB + 2 * n;
+  int mx = 0;
+  for (int d = 0; d < 3; d++) mx = b.M[d] > mx ? b.M[d] : mx;
+  *stride = mx;
+  out.assign((size_t)3 * mx * kMaxCover, make_short2(-1, -1));
+  for (int d = 0; d < 3; d++) {
+    const int M = b.M[d], nb = (M + kSB - 1) / kSB;
+    for (int x = 0; x < M; x++) {
+      int cnt = 0;
+      for (int bb = 0; bb < nb; bb++) {
+        const int u0 = bb * kSB - n;  // unwrapped start of the tile
+        for (int k = -((T + M) / M) - 1; k <= (T + M) / M + 1; k++) {
+          const int o = x + k * M - u0;
+          if (o >= 0 && o < T) {
+            if (cnt >= kMaxCover) return false;
+            out[((size_t)d * mx + x) * kMaxCover + cnt] = make_short2((short)bb, (short)o);
+            cnt++;
+          }
+        }
+      }
+    }
+  }
+  return true;
+}
+
+cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
+                                  const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                                  cudaStream_t st) {
+  switch (2 * s.nst[0] + 1) {
+    case 9: return scatter_w<9>(sorted, start, b, s, buf, rho, st);
+    case 11: return scatter_w<11>(sorted, start, b, s, buf, rho, st);
+    case 13: return scatter_w<13>(sorted, start, b, s, buf, rho, st);
+    case 15: return scatter_w<15>(sorted, start, b, s, buf, rho, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+#define GSE_TILED_INST(CT)                                                                      \
+  template cudaError_t launch_bin_sorted<CT>(const Vec4<CT>::type*, int, const BinLayout&, CT,  \
+                                             CT, CT, BinScratch, Vec4<CT>::type*, int*,         \
+                                             cudaStream_t);                                     \
+  template bool spread_tiled_supported<CT>(const Stencil<CT>&);                                 \
+  template cudaError_t launch_spread_tiled<CT>(const Vec4<CT>::type*, const int*,               \
+                                               const unsigned*, const BinLayout&,               \
+                                               const Stencil<CT>&, CT*, cudaStream_t);          \
+  template cudaError_t launch_gather_tiled<CT>(const Vec4<CT>::type*, const int*, const int*,   \
+                                               const BinLayout&, const Stencil<CT>&, const CT*, \
+                                               double, double*, double*, double*, cudaStream_t);
+
+GSE_TILED_INST(double)
+GSE_TILED_INST(float)
+
+}  // namespace gse

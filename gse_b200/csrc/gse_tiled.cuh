@@ -1,0 +1,105 @@
+// gse_tiled.cuh -- tiled spread / gather kernels and the atom binning they use.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "gse_internal.cuh"
+
+namespace gse {
+
+constexpr int kBinX = 4;            // x cells per bin (y and z bins are single cells)
+constexpr int kWPad = 16;           // padded stencil width (2n+1 <= 15 on the tiled path)
+constexpr int kTX = 16, kTY = 8;    // spread block columns (x, y)
+constexpr int kTZ32 = 32;           // spread block depth, mixed form (int64 accumulators)
+constexpr int kTZ64 = 24;           // spread block depth, FP64 accumulators
+constexpr int kSpreadThreads = 128; // 4 warps, each an 8 x 4 column patch
+constexpr int kSpreadChunk = 64;    // atoms staged per round
+constexpr int kMaxSeg = 4;          // periodic images of one row segment
+constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX
+constexpr int kGatherThreads = 256;          // >= kGY * kGZ
+constexpr int kFoldZ = 4;                    // z planes per fold thread
+constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
+constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
+constexpr int kScatterThreads = 512;  // >= kSB * kSB
+constexpr int kMaxCover = 8;        // brick tiles covering one coordinate
+constexpr int kScatterList = 1024;  // atoms per scatter round (per brick)
+constexpr int kGatherList = 512;    // atoms per gather round (per brick)
+
+// Atoms sorted by key (z cell, y cell, x bin); start[k] .. start[k+1] is bin k.
+struct BinLayout {
+  int M[3];
+  int nbx;  // ceil(Mx / kBinX)
+};
+
+struct BinScratch {
+  int* key;        // [n]
+  int* counts;     // [nbins]
+  int* start;      // [nbins + 1]
+  int* tile_sums;  // [ceil(nbins / 4096)]
+  int* tmp;        // [n]
+  unsigned* qmax_bits;  // max |q| over the atoms (float bits), written by the binning
+};
+
+// exp(-2 h^2 / (2 sigma^2)) per axis as an unevaluated sum hi + lo in CT
+template <typename CT>
+struct Decay {
+  CT hi[3], lo[3];
+};
+template <typename CT>
+inline Decay<CT> make_decay(const Stencil<CT>& s) {
+  Decay<CT> d;
+  for (int a = 0; a < 3; a++) {
+    const double hd = (double)s.h[a];
+    const double v = std::exp(-2.0 * hd * hd * (double)s.inv_2s2);
+    d.hi[a] = (CT)v;
+    d.lo[a] = (CT)(v - (double)d.hi[a]);
+  }
+  return d;
+}
+
+inline BinLayout make_bin_layout(const int M[3]) {
+  BinLayout b;
+  for (int d = 0; d < 3; d++) b.M[d] = M[d];
+  b.nbx = (M[0] + kBinX - 1) / kBinX;
+  return b;
+}
+
+inline int bin_count(const BinLayout& b) { return b.M[1] * b.M[2] * b.nbx; }
+
+// Buffers of the mixed-form scatter spread.
+struct ScatterBuffers {
+  int* halo;          // [bricks][T][T][T] int32 tiles
+  double* scale;      // [bricks] 2^-S of each tile
+  const short2* cover;  // [3][cover_stride][kMaxCover] (brick, tile offset), -1 = end
+  int cover_stride;
+};
+
+size_t scatter_halo_words(const BinLayout& b, int W);
+size_t scatter_brick_count(const BinLayout& b);
+bool scatter_cover_table(const BinLayout& b, int W, std::vector<short2>& out, int* stride);
+cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
+                                  const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                                  cudaStream_t st);
+
+template <typename CT>
+cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const BinLayout& b,
+                              CT inv_hx, CT inv_hy, CT inv_hz, BinScratch w,
+                              typename Vec4<CT>::type* sorted, int* perm, cudaStream_t st);
+
+template <typename CT>
+bool spread_tiled_supported(const Stencil<CT>& s);
+
+template <typename CT>
+cudaError_t launch_spread_tiled(const typename Vec4<CT>::type* sorted, const int* start,
+                                const unsigned* qmax_bits, const BinLayout& b,
+                                const Stencil<CT>& s, CT* grid, cudaStream_t st);
+
+template <typename CT>
+cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int* perm,
+                                const int* start, const BinLayout& b, const Stencil<CT>& s,
+                                const CT* phi, double outscale, double* fx, double* fy,
+                                double* fz, cudaStream_t st);
+
+}  // namespace gse
