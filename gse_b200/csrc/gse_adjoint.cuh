@@ -1,0 +1,22 @@
+// gse_adjoint.cuh -- launchers of the reverse-mode kernels (gse_adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gse_internal.cuh"
+
+namespace gse {
+
+template <typename CT>
+cudaError_t launch_adj_source(const typename Vec4<CT>::type* xyzq, const int* perm, int n,
+                              const Stencil<CT>& s, double c, const double* gfx,
+                              const double* gfy, const double* gfz, CT* lambda, cudaStream_t st);
+
+template <typename CT>
+cudaError_t launch_adj_gather(const typename Vec4<CT>::type* xyzq, const int* perm, int n,
+                              const Stencil<CT>& sp, const Stencil<CT>& sg, double c,
+                              double gE_ch3, const CT* psi, const CT* phi, const double* gfx,
+                              const double* gfy, const double* gfz, double* dq, double* dx,
+                              double* dy, double* dz, cudaStream_t st);
+
+}  // namespace gse

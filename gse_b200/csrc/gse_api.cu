@@ -17,6 +17,7 @@
 #include "gse_b200.h"
 #include "gse_internal.cuh"
 #include "gse_kernels.cuh"
+#include "gse_adjoint.cuh"
 #include "gse_tiled.cuh"
 
 using namespace gse;
@@ -117,6 +118,9 @@ struct gse_context {
   // Green's function table of the context's own solve (sigma2, box)
   void* d_gtab = nullptr;
   bool gtab_valid = false;
+  // adjoint staging: upstream force gradients (3 x cap) and outputs (4 x cap)
+  double* d_adj = nullptr;
+  size_t adj_cap = 0;
   double* d_force = nullptr;  // 3 x atom_cap
   double* d_partials = nullptr;
   double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch
@@ -280,6 +284,7 @@ gse_status_t ensure_scatter(gse_context_t* c, int W) {
   cudaFree(c->d_hscale);
   cudaFree(c->d_cover);
   cudaFree(c->d_gtab);
+  cudaFree(c->d_adj);
   c->d_halo = nullptr;
   c->d_hscale = nullptr;
   c->d_cover = nullptr;
@@ -314,11 +319,11 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
       c->launches += 1;
       CU(launch_spread_tiled<CT>((const V*)c->d_sorted, c->d_bstart, c->d_qmax, c->bl, s,
                                  (CT*)c->d_rho, c->stream));
-    } else {
+    } else if constexpr (sizeof(CT) == 4) {
       c->launches += 2;
       ScatterBuffers sb{c->d_halo, c->d_hscale, c->d_cover, c->cover_stride};
-      CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl,
-                               *(const Stencil<float>*)&s, sb, (float*)c->d_rho, c->stream));
+      CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl, s, sb,
+                               (float*)c->d_rho, c->stream));
     }
   } else {
     StageTimer tm(c, GSE_STAGE_SPREAD);
@@ -654,6 +659,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_hscale);
   cudaFree(c->d_cover);
   cudaFree(c->d_gtab);
+  cudaFree(c->d_adj);
   cudaFree(c->d_partials);
   cudaFree(c->d_scalars);
   cudaFree(c->d_bad);
@@ -947,6 +953,102 @@ gse_status_t gse_get_timing(gse_context_t* c, double* ms_total, long long* count
     }
   }
   return GSE_OK;
+}
+
+gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
+                         const double* gfx, const double* gfy, const double* gfz, double* dq,
+                         double* dx, double* dy, double* dz) {
+  TRY(check_ctx(c));
+  if (n > 0 && (!dq || !dx || !dy || !dz)) return fail(GSE_ERR_INVALID_ARG, "NULL output");
+  const bool have_g = gfx || gfy || gfz;
+  if (have_g && !(gfx && gfy && gfz))
+    return fail(GSE_ERR_INVALID_ARG, "force gradients: give all three components or none");
+  const void* dxq;
+  TRY(stage_atoms(c, n, xyzq, &dxq));
+  if (n == 0) return finish(c, false);
+  if (c->adj_cap < c->atom_cap) {
+    cudaFree(c->d_adj);
+    c->d_adj = nullptr;
+    c->adj_cap = 0;
+    CU(cudaMalloc(&c->d_adj, 7 * c->atom_cap * sizeof(double)));
+    c->adj_cap = c->atom_cap;
+  }
+  const size_t cap = c->adj_cap;
+  double* g = c->d_adj;           // upstream dL/dF (3 x cap)
+  double* o = c->d_adj + 3 * cap; // dq, dx, dy, dz (4 x cap)
+  const double* gd[3] = {nullptr, nullptr, nullptr};
+  if (have_g) {
+    const double* gin[3] = {gfx, gfy, gfz};
+    for (int d = 0; d < 3; d++) {
+      if (is_device_ptr(gin[d])) {
+        gd[d] = gin[d];
+      } else {
+        CU(cudaMemcpyAsync(g + d * cap, gin[d], n * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+        gd[d] = g + d * cap;
+      }
+    }
+  } else {
+    CU(cudaMemsetAsync(g, 0, 3 * cap * sizeof(double), c->stream));
+    for (int d = 0; d < 3; d++) gd[d] = g + d * cap;
+  }
+  const Box3 box = ctx_box(c);
+  const double h3 = (c->p.box_x / c->p.size_x) * (c->p.box_y / c->p.size_y) *
+                    (c->p.box_z / c->p.size_z);
+  const double gE_ch3 = dLdE * c->p.ccelec * h3;
+  // forward grids, recomputed from the inputs (rho -> phi)
+  if (c->fp64)
+    TRY(bin_atoms<double>(c, n, dxq, stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false)));
+  else
+    TRY(bin_atoms<float>(c, n, dxq, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false)));
+  if (c->fp64)
+    TRY(do_spread<double>(c, n, dxq, box.v, c->sigma1, c->rcut1, false, true));
+  else
+    TRY(do_spread<float>(c, n, dxq, box.v, c->sigma1, c->rcut1, false, true));
+  TRY(do_solve_ctx(c));
+  c->phi_valid = true;
+  c->energy_valid = true;
+  // adjoint source lambda into the rho buffer, then psi = K lambda in place
+  CU(cudaMemsetAsync(c->d_rho, 0, c->size * c->ct, c->stream));
+  c->launches += 3;
+  if (c->fp64) {
+    const Stencil<double> sg = stencil_of<double>(c, box.v, c->sigma1, c->rcut1, true, false);
+    CU(launch_adj_source<double>((const double4*)c->d_sorted, c->d_perm, n, sg, c->p.ccelec,
+                                 gd[0], gd[1], gd[2], (double*)c->d_rho, c->stream));
+  } else {
+    const Stencil<float> sg = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, true, false);
+    CU(launch_adj_source<float>((const float4*)c->d_sorted, c->d_perm, n, sg, c->p.ccelec, gd[0],
+                                gd[1], gd[2], (float*)c->d_rho, c->stream));
+  }
+  TRY(do_solve(c, c->d_rho, c->d_rho, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, false));
+  c->rho_valid = false;
+  const bool dev_out = is_device_ptr(dq) && is_device_ptr(dx) && is_device_ptr(dy) &&
+                       is_device_ptr(dz);
+  double* od[4];
+  if (dev_out) {
+    od[0] = dq; od[1] = dx; od[2] = dy; od[3] = dz;
+  } else {
+    for (int k = 0; k < 4; k++) od[k] = o + k * cap;
+  }
+  if (c->fp64) {
+    const Stencil<double> sp = stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false);
+    const Stencil<double> sg = stencil_of<double>(c, box.v, c->sigma1, c->rcut1, true, false);
+    CU(launch_adj_gather<double>((const double4*)c->d_sorted, c->d_perm, n, sp, sg, c->p.ccelec,
+                                 gE_ch3, (const double*)c->d_rho, (const double*)c->d_phi, gd[0],
+                                 gd[1], gd[2], od[0], od[1], od[2], od[3], c->stream));
+  } else {
+    const Stencil<float> sp = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false);
+    const Stencil<float> sg = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, true, false);
+    CU(launch_adj_gather<float>((const float4*)c->d_sorted, c->d_perm, n, sp, sg, c->p.ccelec,
+                                gE_ch3, (const float*)c->d_rho, (const float*)c->d_phi, gd[0],
+                                gd[1], gd[2], od[0], od[1], od[2], od[3], c->stream));
+  }
+  bool host = false;
+  if (!dev_out) {
+    double* outs[4] = {dq, dx, dy, dz};
+    for (int k = 0; k < 4; k++) TRY(copy_out(c, outs[k], od[k], n * sizeof(double), &host));
+  }
+  return finish(c, host);
 }
 
 }  // extern "C"

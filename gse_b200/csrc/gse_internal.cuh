@@ -96,6 +96,14 @@ __device__ __forceinline__ int pmod(int a, int m) {
   return r < 0 ? r + m : r;
 }
 
+// pmod for values that are almost always within one period of [0, m)
+__device__ __forceinline__ int wrap1(int a, int m) {
+  if (a >= 0 && a < m) return a;
+  if (a < 0 && a >= -m) return a + m;
+  if (a >= m && a < 2 * m) return a - m;
+  return pmod(a, m);
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -251,25 +251,26 @@ __global__ void k_green_table(GreenGeom g, CT* __restrict__ tab) {
 }
 
 // rhok *= G (table) with the energy sum_k G |rho(k)|^2 over the full
-// spectrum; one block row per (ky, kz) line so the kx weight needs no division.
+// spectrum: every bin counts twice except kx = 0 and the kx Nyquist bin.
 template <typename CT>
 __global__ void __launch_bounds__(256)
     k_green_apply(typename Cplx<CT>::type* __restrict__ rhok, const CT* __restrict__ tab,
                   GreenGeom g, double* __restrict__ partials) {
-  const int lines = g.nfft[1] * g.nfft[2];
+  const unsigned total = (unsigned)g.sizeX * g.nfft[1] * g.nfft[2];
+  const unsigned sx = (unsigned)g.sizeX;
+  const unsigned nyq = g.nx_even ? (unsigned)(g.nfft[0] / 2) : 0xffffffffu;
   double e = 0.0;
-  for (int line = blockIdx.x; line < lines; line += gridDim.x) {
-    const long long base = (long long)line * g.sizeX;
-    for (int ix = threadIdx.x; ix < g.sizeX; ix += blockDim.x) {
-      auto v = rhok[base + ix];
-      const CT f = tab[base + ix];
-      const double re = (double)v.x, im = (double)v.y;
-      const double wgt = (ix == 0 || (g.nx_even && ix == g.nfft[0] / 2)) ? 1.0 : 2.0;
-      e += wgt * (double)f * (re * re + im * im);
-      v.x *= f;
-      v.y *= f;
-      rhok[base + ix] = v;
-    }
+  for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += gridDim.x * blockDim.x) {
+    auto v = rhok[idx];
+    const CT f = tab[idx];
+    const unsigned ix = idx % sx;
+    const double re = (double)v.x, im = (double)v.y;
+    const double wgt = (ix == 0 || ix == nyq) ? 1.0 : 2.0;
+    e += wgt * (double)f * (re * re + im * im);
+    v.x *= f;
+    v.y *= f;
+    rhok[idx] = v;
   }
   block_sum_to(e, partials);
 }
@@ -446,7 +447,7 @@ template <typename CT>
 cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
                                double* partials, int np, double factor, double* energy_out,
                                cudaStream_t st) {
-  k_green_apply<CT><<<np, 128, 0, st>>>(rhok, tab, g, partials);
+  k_green_apply<CT><<<np, 256, 0, st>>>(rhok, tab, g, partials);
   k_energy_finalize<<<1, 1024, 0, st>>>(partials, np, factor, energy_out);
   return cudaGetLastError();
 }

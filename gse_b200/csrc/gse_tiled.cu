@@ -36,9 +36,9 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const auto a = xyzq[i];
     qm = fmaxf(qm, fabsf((float)a.w));
-    const int cx = pmod(centre_cell(a.x, inv_hx), b.M[0]);
-    const int cy = pmod(centre_cell(a.y, inv_hy), b.M[1]);
-    const int cz = pmod(centre_cell(a.z, inv_hz), b.M[2]);
+    const int cx = wrap1(centre_cell(a.x, inv_hx), b.M[0]);
+    const int cy = wrap1(centre_cell(a.y, inv_hy), b.M[1]);
+    const int cz = wrap1(centre_cell(a.z, inv_hz), b.M[2]);
     const int k = (cz * b.M[1] + cy) * b.nbx + cx / kBinX;
     key[i] = k;
     atomicAdd(&counts[k], 1);
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(kScatterThreads)
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         const int c = centre_cell(pos3[d], s.inv_h[d]);
-        loc[d] = pmod(c, s.M[d]) - org[d];  // window start in tile coordinates
+        loc[d] = wrap1(c, s.M[d]) - org[d];  // window start in tile coordinates
         const float dd = sub_rn(mul_rn((float)(c - n + lane), s.h[d]), pos3[d]);
         wl[d] = (lane < W) ? expf(mul_rn(mul_rn(-dd, dd), s.inv_2s2)) : 0.f;
       }
@@ -608,8 +608,7 @@ __global__ void k_spread_fold(const int* __restrict__ halo, const double* __rest
   }
 #pragma unroll
   for (int zi = 0; zi < ZP; zi++) {
-    const int z = zb + zi;
-    if (z >= b.M[2]) break;
+    const int z = min(zb + zi, b.M[2] - 1);  // planes past the end repeat the last one
     const short2* cz = cover + (2 * cov_stride + z) * kMaxCover;
     double acc = 0.0;
     if (fast_xy && cz[kFast].x < 0) {
@@ -699,20 +698,23 @@ __device__ __forceinline__ void row_sums<float, 13>(const float* row, const floa
 }
 
 template <typename CT, int W>
-__global__ void __launch_bounds__(kGatherThreads)
+__global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
     k_gather_tiled(const typename Vec4<CT>::type* __restrict__ sorted,
                    const int* __restrict__ perm, const int* __restrict__ start, BinLayout b,
                    Stencil<CT> s, const CT* __restrict__ phi, double outscale,
                    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
   constexpr int n = (W - 1) / 2;
   constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
-  constexpr int TP = TX | 1;  // odd row pitch: rows fall in different banks
+  constexpr int TP = TX | 1;  // odd row pitch
+  // plane pitch = W*TP (mod 32): row (jy, jz) starts in bank TP*(jy + W*jz) mod 32,
+  // distinct for 32 consecutive (jy, jz)
+  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
   constexpr int NW = kGatherThreads / 32;
   constexpr int NR = kGY * kGZ;  // cell rows of the brick
   typedef typename Vec4<CT>::type V;
   extern __shared__ __align__(16) unsigned char gsm[];
-  CT* tile = (CT*)gsm;                                   // [TZ][TY][TP]
-  CT* tabs = tile + TZ * TY * TP;                        // [NW][3][3][kWPad]
+  CT* tile = (CT*)gsm;                                   // [TZ][ZP]
+  CT* tabs = tile + TZ * ZP;                             // [NW][3][3][kWPad]
   int* rowl = (int*)(tabs + NW * 3 * 3 * kWPad);         // [NW][W*W]
   __shared__ int rng_a[NR], rng_p[NR + 1];
   __shared__ int alist[kGatherList];
@@ -744,11 +746,11 @@ __global__ void __launch_bounds__(kGatherThreads)
   const long long zs = (long long)b.M[0] * b.M[1];
   for (int r = warp; r < TY * TZ; r += NW) {
     const int ty = r % TY, tz = r / TY;
-    const int gy = pmod(y0 - n + ty, b.M[1]);
-    const int gz = pmod(z0 - n + tz, b.M[2]);
+    const int gy = wrap1(y0 - n + ty, b.M[1]);
+    const int gz = wrap1(z0 - n + tz, b.M[2]);
     const CT* src = phi + (long long)gy * b.M[0] + gz * zs;
-    CT* dst = tile + (tz * TY + ty) * TP;
-    for (int tx = lane; tx < TX; tx += 32) dst[tx] = src[pmod(x0 - n + tx, b.M[0])];
+    CT* dst = tile + tz * ZP + ty * TP;
+    for (int tx = lane; tx < TX; tx += 32) dst[tx] = src[wrap1(x0 - n + tx, b.M[0])];
   }
   __syncthreads();
 
@@ -779,7 +781,7 @@ __global__ void __launch_bounds__(kGatherThreads)
 #pragma unroll
     for (int d = 0; d < 3; d++) {
       const int c = centre_cell(pos3[d], s.inv_h[d]);
-      loc[d] = pmod(c, s.M[d]) - org[d];  // first stencil cell in tile coordinates
+      loc[d] = wrap1(c, s.M[d]) - org[d];  // first stencil cell in tile coordinates
       if (lane < W) {
         const CT dd = sub_rn(pos3[d], mul_rn((CT)(c - n + lane), s.h[d]));
         const CT d2 = mul_rn(dd, dd);
@@ -816,7 +818,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       const int jz = r >> 8, jy = r & 255;
       const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
       const CT rem = s.rcut2 - (dy2 + dz2);
-      const CT* row = tile + ((loc[2] + jz) * TY + (loc[1] + jy)) * TP + loc[0];
+      const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
       CT s0, s1;
       row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
       const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
@@ -911,7 +913,8 @@ static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* pe
   constexpr int n = (W - 1) / 2;
   constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
   constexpr int TP = TX | 1, NW = kGatherThreads / 32;
-  const size_t smem = sizeof(CT) * (TZ * TY * TP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
+  const size_t smem = sizeof(CT) * (TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
   static bool attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);

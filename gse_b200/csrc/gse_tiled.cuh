@@ -19,7 +19,7 @@ constexpr int kSpreadChunk = 64;    // atoms staged per round
 constexpr int kMaxSeg = 4;          // periodic images of one row segment
 constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX
 constexpr int kGatherThreads = 256;          // >= kGY * kGZ
-constexpr int kFoldZ = 4;                    // z planes per fold thread
+constexpr int kFoldZ = 8;                    // z planes per fold thread
 constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
 constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
 constexpr int kScatterThreads = 512;  // >= kSB * kSB

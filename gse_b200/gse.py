@@ -137,6 +137,11 @@ class Context:
     def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
         check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
 
+    def adjoint(self, n, xyzq, dLdE, gfx, gfy, gfz, dq, dx, dy, dz):
+        """dL/dq and dL/dx for dL/dE = dLdE and dL/dF = (gfx, gfy, gfz) (may be None)."""
+        check(self._L.gse_adjoint(self.h, int(n), ptr(xyzq), float(dLdE), ptr(gfx), ptr(gfy),
+                                  ptr(gfz), ptr(dq), ptr(dx), ptr(dy), ptr(dz)))
+
     def set_timing(self, enable: bool):
         check(self._L.gse_set_timing(self.h, int(bool(enable))))
 

@@ -173,6 +173,21 @@ gse_status_t gse_green_mul(gse_context_t* ctx, double sigma, double box_x, doubl
 gse_status_t gse_fft_solve(gse_context_t* ctx, double sigma, double box_x, double box_y,
                            double box_z, const void* rho, void* phi);
 
+/* ---- reverse mode (no reference counterpart) ---------------------------- */
+
+/* Vector-Jacobian product of one force evaluation (gse_forward) for the
+ * scalar L with dL/dE = dLdE and dL/dF_i = (gfx[i], gfy[i], gfz[i]):
+ * writes dq[i] = dL/dq_i and (dx, dy, dz)[i] = dL/dx_i.  The force-gradient
+ * arrays may all be NULL (energy only).  The charge density and potential
+ * grids are recomputed from xyzq (nothing is kept from an earlier forward
+ * call); the adjoint source is spread with the gather's spherical cut,
+ * solved with the same Green's function and gathered together with the
+ * potential.  With dLdE = 1 and no force gradients, dq[i] is the potential
+ * at atom i (dE/dq) and -(dx, dy, dz)[i] the cube-spread force. */
+gse_status_t gse_adjoint(gse_context_t* ctx, int n, const void* xyzq, double dLdE,
+                         const double* gfx, const double* gfy, const double* gfz, double* dq,
+                         double* dx, double* dy, double* dz);
+
 /* ---- instrumentation (no reference counterpart) ------------------------ */
 
 typedef enum gse_stage {
