@@ -309,13 +309,31 @@ def main():
     x2, f2, e2 = device_inputs(other)
     ms2, stage2, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 20)), False)
     value2 = world * max(3, min(args.steps, 20)) / (ms2 / 1000.0)
-    F64 = (f2 if other == "fp64" else F_main).double().cpu().numpy()
-    Fmx = (F_main if other == "fp64" else f2).double().cpu().numpy()
+    F64 = (f2 if other == "fp64" else F_main).double().cpu().numpy().T
+    Fmx = (F_main if other == "fp64" else f2).double().cpu().numpy().T
     E64 = float(e2.item()) if other == "fp64" else E_main
     Emx = E_main if other == "fp64" else float(e2.item())
     d = Fmx - F64
     force_rms = float(np.sqrt((d * d).sum() / (F64 * F64).sum()))
     energy_rel = abs(Emx - E64) / abs(E64)
+
+    # accuracy of both forms against the FP64 Ewald reciprocal sum (converged k cut)
+    accuracy = None
+    if rank == 0:
+        from gse_b200.gse import ewald_kcut, ewald_recip
+        kc = ewald_kcut(s.sigma, s.boxes)
+        t0 = time.perf_counter()
+        e_ew, f_ew = ewald_recip(s.sigma, kc, s.boxes, s.xyzq.astype(np.float64), device=local)
+        t_ew = time.perf_counter() - t0
+
+        def rel_rms(F):
+            dd = F - f_ew
+            return float(np.sqrt((dd * dd).sum() / (f_ew * f_ew).sum()))
+
+        accuracy = {"oracle": f"FP64 Ewald reciprocal sum on the GPU, kcut {kc}",
+                    "oracle_seconds": t_ew,
+                    "mixed": {"force_rms": rel_rms(Fmx), "energy_rel": abs(Emx - e_ew) / abs(e_ew)},
+                    "fp64": {"force_rms": rel_rms(F64), "energy_rel": abs(E64 - e_ew) / abs(e_ew)}}
 
     if rank == 0:
         # roofline of the dominant kernel
@@ -369,6 +387,7 @@ def main():
             "stage_ms": per_stage,
             f"{other}_value": value2,
             "mixed_vs_fp64": {"force_rms": force_rms, "energy_rel": energy_rel},
+            "vs_ewald": accuracy,
             "energy": E_main,
         }
         print(json.dumps(line), flush=True)

@@ -72,6 +72,7 @@ SIGNATURES = {
     "gse_get_launch_count": (_i, [_vp, _vp]),
     "gse_spread_mixed_noalloc": (_i, [_i, _i, _i, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp]),
     "gse_adjoint": (_i, [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gse_ewald_recip": (_i, [_i, _vp, _d, _i, _d, _d, _d, _d, _i, _vp, _vp, _vp, _vp, _vp]),
 }
 STAGES = ["bin", "spread", "fft_forward", "green", "fft_backward", "gather"]
 

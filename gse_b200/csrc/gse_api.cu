@@ -18,6 +18,7 @@
 #include "gse_internal.cuh"
 #include "gse_kernels.cuh"
 #include "gse_adjoint.cuh"
+#include "gse_ewald.cuh"
 #include "gse_tiled.cuh"
 
 using namespace gse;
@@ -1049,6 +1050,89 @@ gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
     for (int k = 0; k < 4; k++) TRY(copy_out(c, outs[k], od[k], n * sizeof(double), &host));
   }
   return finish(c, host);
+}
+
+gse_status_t gse_ewald_recip(int device, void* stream, double sigma, int kcut, double box_x,
+                             double box_y, double box_z, double ccelec, int n, const double* xyzq,
+                             double* energy, double* fx, double* fy, double* fz) {
+  g_last_error.clear();
+  if (!(sigma > 0.0) || kcut < 1 || kcut > 255 || !(box_x > 0 && box_y > 0 && box_z > 0) ||
+      n < 0 || (n > 0 && !xyzq) || !energy)
+    return fail(GSE_ERR_INVALID_ARG, "bad Ewald arguments (kcut must lie in [1, 255])");
+  const bool want_f = fx || fy || fz;
+  if (want_f && !(fx && fy && fz)) return fail(GSE_ERR_INVALID_ARG, "give all force arrays or none");
+  CU(cudaSetDevice(device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const std::vector<EwRowHost> rows = ewald_rows(kcut);
+  long long nk = 0;
+  for (const EwRowHost& r : rows) nk += r.nk;
+  EwGeom g;
+  g.inv_box[0] = 1.0 / box_x;
+  g.inv_box[1] = 1.0 / box_y;
+  g.inv_box[2] = 1.0 / box_z;
+  g.pref = 2.0 * kPi * g.inv_box[0] * g.inv_box[1] * g.inv_box[2] * ccelec;
+  g.half_sigmasq = 0.5 * sigma * sigma;
+  // scratch: rows, P S(k), row energies, and staged atoms/forces
+  void* rows_d = nullptr;
+  double2* S = nullptr;
+  double* re = nullptr;
+  double4* xd = nullptr;
+  double* fd = nullptr;
+  gse_status_t status = GSE_OK;
+  std::vector<double> rh(rows.size());
+  auto cleanup = [&]() {
+    cudaFree(rows_d);
+    cudaFree(S);
+    cudaFree(re);
+    cudaFree(xd);
+    cudaFree(fd);
+  };
+#define CUE(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      status = fail(_e == cudaErrorMemoryAllocation ? GSE_ERR_OOM : GSE_ERR_CUDA,          \
+                    "gse_ewald_recip: %s: %s", #call, cudaGetErrorString(_e));             \
+      cleanup();                                                                           \
+      return status;                                                                       \
+    }                                                                                      \
+  } while (0)
+  if (n == 0 || rows.empty()) {
+    *energy = 0.0;
+    return GSE_OK;
+  }
+  CUE(cudaMalloc(&rows_d, sizeof(EwRowHost) * rows.size()));
+  CUE(cudaMalloc(&S, sizeof(double2) * nk));
+  CUE(cudaMalloc(&re, sizeof(double) * rows.size()));
+  const double4* xin = (const double4*)xyzq;
+  if (!is_device_ptr(xyzq)) {
+    CUE(cudaMalloc(&xd, sizeof(double4) * n));
+    CUE(cudaMemcpyAsync(xd, xyzq, sizeof(double4) * n, cudaMemcpyHostToDevice, st));
+    xin = xd;
+  }
+  double* f[3] = {fx, fy, fz};
+  const bool fdev = want_f && is_device_ptr(fx) && is_device_ptr(fy) && is_device_ptr(fz);
+  if (want_f && !fdev) {
+    CUE(cudaMalloc(&fd, sizeof(double) * 3 * n));
+    f[0] = fd;
+    f[1] = fd + n;
+    f[2] = fd + 2 * n;
+  }
+  EwScratch w{rows_d, S, re};
+  CUE(launch_ewald(xin, n, rows, g, w, want_f ? f[0] : nullptr, f[1], f[2], st));
+  CUE(cudaMemcpyAsync(rh.data(), re, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, st));
+  if (want_f && !fdev) {
+    CUE(cudaMemcpyAsync(fx, fd, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUE(cudaMemcpyAsync(fy, fd + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUE(cudaMemcpyAsync(fz, fd + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
+  CUE(cudaStreamSynchronize(st));
+#undef CUE
+  double e = 0.0;
+  for (double v : rh) e += v;
+  *energy = e;
+  cleanup();
+  return GSE_OK;
 }
 
 }  // extern "C"

@@ -389,3 +389,28 @@ class CpuGSEk(CpuGSE):
     def forward(self, numCoord, xyzq, forceX=None, forceY=None, forceZ=None) -> float:
         """spreadCharge1 + solvePoisson + calculateEnergy + interpolateForce in one call."""
         return self._ctx.forward(numCoord, _xyzq_arg(xyzq, self.dtype), forceX, forceY, forceZ)
+
+
+def ewald_recip(sigma, kcut, box, xyzq, ccelec=CCELEC, forces=True, device=0, stream=None):
+    """FP64 Ewald reciprocal sum on the GPU (CpuEwaldRecip::calcForceEnergy,
+    CpuEwaldRecip.cpp:87-147).  Returns (E, F[n, 3]) or (E, None)."""
+    L = _lib.load()
+    a = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    n = a.shape[0]
+    e = ctypes.c_double()
+    if forces:
+        f = np.zeros((3, n))
+        check(L.gse_ewald_recip(device, stream, sigma, int(kcut), box[0], box[1], box[2], ccelec,
+                                n, a.ctypes.data, ctypes.addressof(e), f[0].ctypes.data,
+                                f[1].ctypes.data, f[2].ctypes.data))
+        return e.value, f.T.copy()
+    check(L.gse_ewald_recip(device, stream, sigma, int(kcut), box[0], box[1], box[2], ccelec, n,
+                            a.ctypes.data, ctypes.addressof(e), None, None, None))
+    return e.value, None
+
+
+def ewald_kcut(sigma, box, tol=1e-12):
+    """Smallest integer k cut-off with exp(-sigma^2 k^2 / 2) below tol along the longest box side."""
+    import math
+    kmax = math.sqrt(2.0 * math.log(1.0 / tol)) / sigma
+    return int(math.ceil(kmax * max(box) / (2.0 * math.pi)))

@@ -188,6 +188,18 @@ gse_status_t gse_adjoint(gse_context_t* ctx, int n, const void* xyzq, double dLd
                          const double* gfx, const double* gfy, const double* gfz, double* dq,
                          double* dx, double* dy, double* dz);
 
+/* ---- Ewald reference sum --------------------------------------------------- */
+
+/* CpuEwaldRecip::calcForceEnergy (CpuEwaldRecip.cpp:87-147) on the GPU in FP64:
+ * E = sum over integer k != 0 with |k|^2 <= kcut^2 of
+ * (2 pi / V) ccelec exp(-sigma^2 |k|^2 / 2) / |k|^2 |S(k)|^2 and the forces
+ * -dE/dr (force arrays may all be NULL).  Independent of any context; it
+ * allocates its own scratch and returns after the results are written.
+ * kcut must lie in [1, 255]. */
+gse_status_t gse_ewald_recip(int device, void* stream, double sigma, int kcut, double box_x,
+                             double box_y, double box_z, double ccelec, int n, const double* xyzq,
+                             double* energy, double* fx, double* fy, double* fz);
+
 /* ---- instrumentation (no reference counterpart) ------------------------ */
 
 typedef enum gse_stage {
