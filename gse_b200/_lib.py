@@ -40,6 +40,26 @@ class gse_params_t(ctypes.Structure):
     ]
 
 
+class gse_system_t(ctypes.Structure):
+    _fields_ = [
+        ("size_x", ctypes.c_int), ("size_y", ctypes.c_int), ("size_z", ctypes.c_int),
+        ("box_x", ctypes.c_double), ("box_y", ctypes.c_double), ("box_z", ctypes.c_double),
+        ("n", ctypes.c_int),
+    ]
+
+
+class gse_batch_info_t(ctypes.Structure):
+    _fields_ = [
+        ("n_total", ctypes.c_int), ("n_systems", ctypes.c_int), ("n_size_classes", ctypes.c_int),
+        ("grid_points", ctypes.c_longlong),
+        ("scatter_items", ctypes.c_int), ("gather_items", ctypes.c_int),
+        ("scatter_ctas", ctypes.c_int), ("gather_ctas", ctypes.c_int),
+        ("largest_first", ctypes.c_int),
+        ("xyzq", ctypes.c_void_p), ("energies", ctypes.c_void_p), ("forces", ctypes.c_void_p),
+        ("dLdE", ctypes.c_void_p), ("grad_forces", ctypes.c_void_p), ("grad_out", ctypes.c_void_p),
+    ]
+
+
 # Every exported symbol with (restype, argtypes); used both to bind and by
 # the CPU test that checks the library exports what the header declares.
 _vp = ctypes.c_void_p
@@ -73,6 +93,16 @@ SIGNATURES = {
     "gse_spread_mixed_noalloc": (_i, [_i, _i, _i, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp]),
     "gse_adjoint": (_i, [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gse_ewald_recip": (_i, [_i, _vp, _d, _i, _d, _d, _d, _d, _i, _vp, _vp, _vp, _vp, _vp]),
+    "gse_batch_create": (_i, [ctypes.POINTER(gse_params_t), _i, ctypes.POINTER(gse_system_t),
+                              ctypes.POINTER(_vp)]),
+    "gse_batch_destroy": (_i, [_vp]),
+    "gse_batch_set_stream": (_i, [_vp, _vp]),
+    "gse_batch_info": (_i, [_vp, ctypes.POINTER(gse_batch_info_t)]),
+    "gse_batch_forward": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "gse_batch_adjoint": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gse_batch_capture": (_i, [_vp, _i]),
+    "gse_batch_launch": (_i, [_vp]),
+    "gse_batch_autotune": (_i, [_vp, ctypes.c_char_p, _i]),
 }
 STAGES = ["bin", "spread", "fft_forward", "green", "fft_backward", "gather"]
 

@@ -20,23 +20,22 @@
 // derivative is zero almost everywhere).
 #include "gse_adjoint.cuh"
 #include "gse_internal.cuh"
+#include "gse_tiled.cuh"
 
 namespace gse {
 
-// lambda(r) += c q_i A e (G_i . u) over the sphere of atom i (global atomics).
+// lambda(r) += c q_i A e (G_i . u) over the sphere of atom i (global atomics);
+// one warp per atom.
 template <typename CT>
-__global__ void __launch_bounds__(256)
-    k_adj_source(const typename Vec4<CT>::type* __restrict__ xyzq, const int* __restrict__ perm,
-                 int n, Stencil<CT> s, double c, const double* __restrict__ gfx,
-                 const double* __restrict__ gfy, const double* __restrict__ gfz,
-                 CT* __restrict__ lambda) {
+__device__ __forceinline__ void adj_source_atom(const typename Vec4<CT>::type& a, int i,
+                                                const Stencil<CT>& s, double c,
+                                                const double* __restrict__ gfx,
+                                                const double* __restrict__ gfy,
+                                                const double* __restrict__ gfz,
+                                                CT* __restrict__ lambda) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const int W0 = 2 * s.nst[0] + 1, W1 = 2 * s.nst[1] + 1, W2 = 2 * s.nst[2] + 1;
-  for (int ii = gw; ii < n; ii += nw) {
-    const int i = perm[ii];
-    const auto a = xyzq[ii];
+  {
     const CT pos[3] = {a.x, a.y, a.z};
     const CT G[3] = {(CT)gfx[i], (CT)gfy[i], (CT)gfz[i]};
     const CT amp = (CT)(c * (double)a.w * (double)s.pref);
@@ -61,24 +60,31 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <typename CT>
+__global__ void __launch_bounds__(256)
+    k_adj_source(const typename Vec4<CT>::type* __restrict__ xyzq, const int* __restrict__ perm,
+                 int n, Stencil<CT> s, double c, const double* __restrict__ gfx,
+                 const double* __restrict__ gfy, const double* __restrict__ gfz,
+                 CT* __restrict__ lambda) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ii = gw; ii < n; ii += nw)
+    adj_source_atom<CT>(xyzq[ii], perm[ii], s, c, gfx, gfy, gfz, lambda);
+}
+
 // Per atom: the cube gather of Psi = psi + gE c h^3 phi and the sphere
 // gather of phi, combined into dL/dq and dL/dx.
 template <typename CT>
-__global__ void __launch_bounds__(256)
-    k_adj_gather(const typename Vec4<CT>::type* __restrict__ xyzq, const int* __restrict__ perm,
-                 int n, Stencil<CT> sp /*spread*/, Stencil<CT> sg /*gather*/, double c,
-                 double gE_ch3, const CT* __restrict__ psi, const CT* __restrict__ phi,
-                 const double* __restrict__ gfx, const double* __restrict__ gfy,
-                 const double* __restrict__ gfz, double* __restrict__ dq,
-                 double* __restrict__ dx, double* __restrict__ dy, double* __restrict__ dz) {
+__device__ __forceinline__ void adj_gather_atom(
+    const typename Vec4<CT>::type& a, int i, const Stencil<CT>& sp, const Stencil<CT>& sg,
+    double c, double gE_ch3, const CT* __restrict__ psi, const CT* __restrict__ phi,
+    const double* __restrict__ gfx, const double* __restrict__ gfy,
+    const double* __restrict__ gfz, double* __restrict__ dq, double* __restrict__ dx,
+    double* __restrict__ dy, double* __restrict__ dz) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   const int W0 = 2 * sp.nst[0] + 1, W1 = 2 * sp.nst[1] + 1, W2 = 2 * sp.nst[2] + 1;
   const double inv_s2 = 2.0 * (double)sp.inv_2s2;
-  for (int ii = gw; ii < n; ii += nw) {
-    const int i = perm[ii];
-    const auto a = xyzq[ii];
+  {
     const CT pos[3] = {a.x, a.y, a.z};
     const double G[3] = {gfx ? gfx[i] : 0.0, gfy ? gfy[i] : 0.0, gfz ? gfz[i] : 0.0};
     int c0[3];
@@ -129,6 +135,84 @@ __global__ void __launch_bounds__(256)
       dz[i] = q * V[2] + cA * q * (G[2] * T0 - T2[2] * inv_s2);
     }
   }
+}
+
+template <typename CT>
+__global__ void __launch_bounds__(256)
+    k_adj_gather(const typename Vec4<CT>::type* __restrict__ xyzq, const int* __restrict__ perm,
+                 int n, Stencil<CT> sp /*spread*/, Stencil<CT> sg /*gather*/, double c,
+                 double gE_ch3, const CT* __restrict__ psi, const CT* __restrict__ phi,
+                 const double* __restrict__ gfx, const double* __restrict__ gfy,
+                 const double* __restrict__ gfz, double* __restrict__ dq,
+                 double* __restrict__ dx, double* __restrict__ dy, double* __restrict__ dz) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ii = gw; ii < n; ii += nw)
+    adj_gather_atom<CT>(xyzq[ii], perm[ii], sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx,
+                        dy, dz);
+}
+
+// ---- batched systems: system of a sorted atom by its offset range ----
+__device__ __forceinline__ int adj_sys_of(const int* __restrict__ first, int nsys, int i) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256)
+    k_batch_adj_source(const float4* __restrict__ xyzq, const int* __restrict__ perm, int ntot,
+                       const BatchSys* __restrict__ sys, const int* __restrict__ first, int nsys,
+                       double c, const double* __restrict__ gfx, const double* __restrict__ gfy,
+                       const double* __restrict__ gfz, float* __restrict__ lambda) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ii = gw; ii < ntot; ii += nw) {
+    const BatchSys& S = sys[adj_sys_of(first, nsys, ii)];
+    adj_source_atom<float>(xyzq[ii], perm[ii], S.sg, c, gfx, gfy, gfz, lambda + S.grid_off);
+  }
+}
+
+__global__ void __launch_bounds__(256)
+    k_batch_adj_gather(const float4* __restrict__ xyzq, const int* __restrict__ perm, int ntot,
+                       const BatchSys* __restrict__ sys, const int* __restrict__ first, int nsys,
+                       double c, const double* __restrict__ dLdE, const float* __restrict__ psi,
+                       const float* __restrict__ phi, const double* __restrict__ gfx,
+                       const double* __restrict__ gfy, const double* __restrict__ gfz,
+                       double* __restrict__ dq, double* __restrict__ dx, double* __restrict__ dy,
+                       double* __restrict__ dz) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int ii = gw; ii < ntot; ii += nw) {
+    const int si = adj_sys_of(first, nsys, ii);
+    const BatchSys& S = sys[si];
+    adj_gather_atom<float>(xyzq[ii], perm[ii], S.sp, S.sg, c, dLdE[si] * c * S.h3,
+                           psi + S.grid_off, phi + S.grid_off, gfx, gfy, gfz, dq, dx, dy, dz);
+  }
+}
+
+cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int ntot,
+                                    const BatchSys* sys, const int* first, int nsys, double c,
+                                    const double* gfx, const double* gfy, const double* gfz,
+                                    float* lambda, cudaStream_t st) {
+  if (ntot <= 0) return cudaSuccess;
+  k_batch_adj_source<<<148 * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, gfx, gfy,
+                                               gfz, lambda);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_adj_gather(const float4* xyzq, const int* perm, int ntot,
+                                    const BatchSys* sys, const int* first, int nsys, double c,
+                                    const double* dLdE, const float* psi, const float* phi,
+                                    const double* gfx, const double* gfy, const double* gfz,
+                                    double* dq, double* dx, double* dy, double* dz,
+                                    cudaStream_t st) {
+  if (ntot <= 0) return cudaSuccess;
+  k_batch_adj_gather<<<148 * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, dLdE, psi,
+                                               phi, gfx, gfy, gfz, dq, dx, dy, dz);
+  return cudaGetLastError();
 }
 
 template <typename CT>

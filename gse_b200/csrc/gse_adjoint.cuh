@@ -4,8 +4,20 @@
 #include <cuda_runtime.h>
 
 #include "gse_internal.cuh"
+#include "gse_tiled.cuh"
 
 namespace gse {
+
+cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int ntot,
+                                    const BatchSys* sys, const int* first, int nsys, double c,
+                                    const double* gfx, const double* gfy, const double* gfz,
+                                    float* lambda, cudaStream_t st);
+cudaError_t launch_batch_adj_gather(const float4* xyzq, const int* perm, int ntot,
+                                    const BatchSys* sys, const int* first, int nsys, double c,
+                                    const double* dLdE, const float* psi, const float* phi,
+                                    const double* gfx, const double* gfy, const double* gfz,
+                                    double* dq, double* dx, double* dy, double* dz,
+                                    cudaStream_t st);
 
 template <typename CT>
 cudaError_t launch_adj_source(const typename Vec4<CT>::type* xyzq, const int* perm, int n,

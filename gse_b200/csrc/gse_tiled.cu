@@ -446,24 +446,33 @@ struct ScatterGeom {
   static constexpr int words = T * PP;
 };
 
+// Where a finished brick tile goes: its slot of the halo buffer (summed later
+// by k_spread_fold), or straight into an int64 grid at 2^kFlushBits by
+// integer reductions (order-independent, so still deterministic).
+struct ScatterOut {
+  int* halo;            // halo mode: [bricks][T^3] slots, with
+  double* halo_scale;   //            2^-S per brick
+  int brick;
+  long long* grid64;    // flush mode: the system's int64 grid
+};
+constexpr int kFlushBits = 40;
+
 template <int W>
-__global__ void __launch_bounds__(kScatterThreads)
-    k_spread_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
-                     BinLayout b, Stencil<float> s, int* __restrict__ halo,
-                     double* __restrict__ halo_scale) {
+__device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
+                                              const int* __restrict__ start, const BinLayout& b,
+                                              const Stencil<float>& s, int bxi, int byi, int bzi,
+                                              int* __restrict__ tile, const ScatterOut& out) {
   typedef ScatterGeom<W> G;
   constexpr int n = G::n, T = G::T;
   constexpr int NT = kScatterThreads, NW = NT / 32;
   constexpr int NPASS = (W * W + 31) / 32;
-  extern __shared__ int tile[];
   __shared__ int rng_a[kSB * kSB], rng_p[kSB * kSB];
   __shared__ int alist[kScatterList];
   __shared__ float qsum_w[NW], qmax_w[NW];
   __shared__ int s_shift;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int x0 = blockIdx.x * kSB, y0 = blockIdx.y * kSB, z0 = blockIdx.z * kSB;
-  const int brick = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const int x0 = bxi * kSB, y0 = byi * kSB, z0 = bzi * kSB;
   const int ex = min(kSB, b.M[0] - x0), ey = min(kSB, b.M[1] - y0), ez = min(kSB, b.M[2] - z0);
 
   // the brick's atoms: one range per (y, z) cell row
@@ -510,12 +519,12 @@ __global__ void __launch_bounds__(kScatterThreads)
     const double pref = fabs((double)s.pref);
     const double sum_b = (double)q * pref * 1.0001 + 1e-30;
     const double one_b = (double)m * pref * 1.0001 + 1e-30;
-    int sh = 40;
+    int sh = kFlushBits;
     while (sh > -60 && (sum_b * exp2((double)sh) >= 1073741824.0 ||
                         one_b * exp2((double)sh) >= 4194304.0))
       sh--;
     s_shift = sh;
-    halo_scale[brick] = exp2(-(double)sh);
+    if (out.halo_scale) out.halo_scale[out.brick] = exp2(-(double)sh);
   }
   __syncthreads();
   const float tscale = exp2f((float)s_shift);
@@ -577,12 +586,39 @@ __global__ void __launch_bounds__(kScatterThreads)
     }
     __syncthreads();
   }
-  // tile -> halo slot [z][y][x], T^3 ints
-  int* dst = halo + (long long)brick * (T * T * T);
-  for (int i = tid; i < T * T * T; i += NT) {
-    const int zz = i / (T * T);
-    dst[i] = tile[zz * G::PP + (i - zz * T * T)];
+  if (out.halo) {
+    // tile -> halo slot [z][y][x], T^3 ints
+    int* dst = out.halo + (long long)out.brick * (T * T * T);
+    for (int i = tid; i < T * T * T; i += NT) {
+      const int zz = i / (T * T);
+      dst[i] = tile[zz * G::PP + (i - zz * T * T)];
+    }
+  } else {
+    // tile -> int64 grid at 2^kFlushBits (S <= kFlushBits, so the shift is exact)
+    const long long mul = 1LL << (kFlushBits - s_shift);
+    for (int i = tid; i < T * T * T; i += NT) {
+      const int zz = i / (T * T), r = i - zz * T * T, yy = r / T, xx = r - yy * T;
+      const int v = tile[zz * G::PP + r];
+      if (v != 0) {
+        const int gx = wrap1(x0 - n + xx, b.M[0]), gy = wrap1(y0 - n + yy, b.M[1]),
+                  gz = wrap1(z0 - n + zz, b.M[2]);
+        atomicAdd((unsigned long long*)(out.grid64 + gx +
+                                        ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
+                  (unsigned long long)((long long)v * mul));
+      }
+    }
   }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kScatterThreads)
+    k_spread_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
+                     BinLayout b, Stencil<float> s, int* __restrict__ halo,
+                     double* __restrict__ halo_scale) {
+  extern __shared__ int tile[];
+  const int brick = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  ScatterOut out{halo, halo_scale, brick, nullptr};
+  scatter_brick<W>(sorted, start, b, s, blockIdx.x, blockIdx.y, blockIdx.z, tile, out);
 }
 
 // rho(x, y, z) = sum over the brick tiles covering the point of
@@ -698,11 +734,13 @@ __device__ __forceinline__ void row_sums<float, 13>(const float* row, const floa
 }
 
 template <typename CT, int W>
-__global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
-    k_gather_tiled(const typename Vec4<CT>::type* __restrict__ sorted,
-                   const int* __restrict__ perm, const int* __restrict__ start, BinLayout b,
-                   Stencil<CT> s, const CT* __restrict__ phi, double outscale,
-                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+__device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __restrict__ sorted,
+                                             const int* __restrict__ perm,
+                                             const int* __restrict__ start, const BinLayout& b,
+                                             const Stencil<CT>& s, const CT* __restrict__ phi,
+                                             double outscale, double* __restrict__ fx,
+                                             double* __restrict__ fy, double* __restrict__ fz,
+                                             int bxi, int byi, int bzi, unsigned char* gsm) {
   constexpr int n = (W - 1) / 2;
   constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
   constexpr int TP = TX | 1;  // odd row pitch
@@ -712,7 +750,6 @@ __global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
   constexpr int NW = kGatherThreads / 32;
   constexpr int NR = kGY * kGZ;  // cell rows of the brick
   typedef typename Vec4<CT>::type V;
-  extern __shared__ __align__(16) unsigned char gsm[];
   CT* tile = (CT*)gsm;                                   // [TZ][ZP]
   CT* tabs = tile + TZ * ZP;                             // [NW][3][3][kWPad]
   int* rowl = (int*)(tabs + NW * 3 * 3 * kWPad);         // [NW][W*W]
@@ -720,7 +757,7 @@ __global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
   __shared__ int alist[kGatherList];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int x0 = blockIdx.x * kGX, y0 = blockIdx.y * kGY, z0 = blockIdx.z * kGZ;
+  const int x0 = bxi * kGX, y0 = byi * kGY, z0 = bzi * kGZ;
   const int ex = min(kGX, b.M[0] - x0), ey = min(kGY, b.M[1] - y0), ez = min(kGZ, b.M[2] - z0);
 
   // atoms of the brick: one range per (y, z) cell row
@@ -842,6 +879,17 @@ __global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
   }
 }
 
+template <typename CT, int W>
+__global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
+    k_gather_tiled(const typename Vec4<CT>::type* __restrict__ sorted,
+                   const int* __restrict__ perm, const int* __restrict__ start, BinLayout b,
+                   Stencil<CT> s, const CT* __restrict__ phi, double outscale,
+                   double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  gather_brick<CT, W>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, blockIdx.x,
+                      blockIdx.y, blockIdx.z, gsm);
+}
+
 // ===========================================================================
 // Launchers
 // ===========================================================================
@@ -860,6 +908,18 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
                                         w.qmax_bits);
+  return launch_bin_scan_place<CT>(xyzq, n, nb, w, sorted, perm, st);
+}
+
+// counts (filled) -> start offsets -> stable placement of the atoms.
+template <typename CT>
+cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, int nb,
+                                  BinScratch w, typename Vec4<CT>::type* sorted, int* perm,
+                                  cudaStream_t st) {
+  const int ntiles = (nb + kScanTile - 1) / kScanTile;
+  if (ntiles > kScanTile) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.start, w.tile_sums);
   k_scan_sums<<<1, kScanThreads, 0, st>>>(w.tile_sums, ntiles, w.start, nb);
   k_scan_add<<<(nb + 255) / 256, 256, 0, st>>>(w.start, nb, w.tile_sums);
@@ -1021,10 +1081,216 @@ cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const 
   return cudaErrorInvalidValue;
 }
 
+// ===========================================================================
+// Batched systems: persistent kernels over (system, brick) work items
+// ===========================================================================
+__device__ __forceinline__ int batch_sys_of(const int* __restrict__ first, int nsys, int i) {
+  int lo = 0, hi = nsys - 1;  // last s with first[s] <= i
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
+                                  const BatchSys* __restrict__ sys, const int* __restrict__ first,
+                                  int nsys, int* __restrict__ key, int* __restrict__ counts,
+                                  unsigned* __restrict__ qmax_bits) {
+  float qm = 0.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
+    const float4 a = xyzq[i];
+    qm = fmaxf(qm, fabsf(a.w));
+    const BatchSys& S = sys[batch_sys_of(first, nsys, i)];
+    const int cx = wrap1(centre_cell(a.x, S.sp.inv_h[0]), S.b.M[0]);
+    const int cy = wrap1(centre_cell(a.y, S.sp.inv_h[1]), S.b.M[1]);
+    const int cz = wrap1(centre_cell(a.z, S.sp.inv_h[2]), S.b.M[2]);
+    const int k = S.bin_off + (cz * S.b.M[1] + cy) * S.b.nbx + cx / kBinX;
+    key[i] = k;
+    atomicAdd(&counts[k], 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(qmax_bits, __float_as_uint(qm));
+}
+
+__global__ void __launch_bounds__(kScatterThreads)
+    k_batch_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
+                    const BatchSys* __restrict__ sys, const BatchItem* __restrict__ items,
+                    int nitems, long long* __restrict__ grid64) {
+  extern __shared__ int tile[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const BatchItem item = items[it];
+    const BatchSys& S = sys[item.sys];
+    const ScatterOut out{nullptr, nullptr, 0, grid64 + S.grid_off};
+    const int* st = start + S.bin_off;
+    switch (S.W) {
+      case 9: scatter_brick<9>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
+      case 11: scatter_brick<11>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
+      case 13: scatter_brick<13>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
+      case 15: scatter_brick<15>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_batch_fixed_to_real(const long long* __restrict__ g64, long long size,
+                                      float* __restrict__ out) {
+  const double unscale = exp2(-(double)kFlushBits);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)((double)g64[i] * unscale);
+}
+
+// rhok *= G per bin; energy[s] += efac_s * sum_k G |rho(k)|^2 (full spectrum).
+// kfirst: ascending first bins of the systems' spectra, ksys: the system of
+// each of those slots (grids are grouped by size, not in system order).
+__global__ void __launch_bounds__(256)
+    k_batch_green_apply(float2* __restrict__ rhok, const float* __restrict__ tab,
+                        long long ktot, const BatchSys* __restrict__ sys,
+                        const long long* __restrict__ kfirst, const int* __restrict__ ksys,
+                        int nsys, double* __restrict__ energy) {
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < ktot;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long idx = base + threadIdx.x;
+    int s = 0;
+    double e = 0.0;
+    if (idx < ktot) {
+      int lo = 0, hi = nsys - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (kfirst[mid] <= idx) lo = mid; else hi = mid - 1;
+      }
+      s = ksys[lo];
+      const BatchSys& S = sys[s];
+      float2 v = rhok[idx];
+      const float f = tab[idx];
+      const int sx = S.b.M[0] / 2 + 1;
+      const int ix = (int)((idx - kfirst[lo]) % sx);
+      const double wgt = (ix == 0 || ((S.b.M[0] & 1) == 0 && ix == S.b.M[0] / 2)) ? 1.0 : 2.0;
+      const double re = v.x, im = v.y;
+      if (energy) e = S.efac * wgt * (double)f * (re * re + im * im);
+      v.x *= f;
+      v.y *= f;
+      rhok[idx] = v;
+    }
+    if (energy) {
+      const int s0 = __shfl_sync(0xffffffffu, s, 0);
+      if (__all_sync(0xffffffffu, s == s0)) {
+        e = warp_sum(e);
+        if (lane == 0 && idx < ktot) atomicAdd(&energy[s0], e);
+        else if (lane == 0) atomicAdd(&energy[s0], e);
+      } else if (idx < ktot) {
+        atomicAdd(&energy[s], e);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kGatherThreads, 2)
+    k_batch_gather(const float4* __restrict__ sorted, const int* __restrict__ perm,
+                   const int* __restrict__ start, const BatchSys* __restrict__ sys,
+                   const BatchItem* __restrict__ items, int nitems, const float* __restrict__ phi,
+                   double outscale, double* __restrict__ fx, double* __restrict__ fy,
+                   double* __restrict__ fz) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const BatchItem item = items[it];
+    const BatchSys& S = sys[item.sys];
+    const int* st = start + S.bin_off;
+    const float* ph = phi + S.grid_off;
+    switch (S.W) {
+      case 9: gather_brick<float, 9>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
+      case 11: gather_brick<float, 11>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
+      case 13: gather_brick<float, 13>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
+      case 15: gather_brick<float, 15>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
+    }
+    __syncthreads();
+  }
+}
+
+size_t batch_scatter_smem() { return sizeof(int) * ScatterGeom<15>::words; }
+
+size_t batch_gather_smem() {
+  constexpr int W = 15, n = 7;
+  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
+  constexpr int TP = TX | 1, NW = kGatherThreads / 32;
+  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
+  return sizeof(float) * (TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+}
+
+cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
+                             int nsys, int nbins, BinScratch w, float4* sorted, int* perm,
+                             cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nbins, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(w.qmax_bits, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  const int gb = (int)std::min<long long>(148 * 8, (ntot + 255) / 256 > 0 ? (ntot + 255) / 256 : 1);
+  if (ntot > 0)
+    k_batch_bin_count<<<gb, 256, 0, st>>>(xyzq, ntot, sys, first, nsys, w.key, w.counts,
+                                          w.qmax_bits);
+  return launch_bin_scan_place<float>(xyzq, ntot, nbins, w, sorted, perm, st);
+}
+
+cudaError_t launch_batch_spread(const float4* sorted, const int* start, const BatchSys* sys,
+                                const BatchItem* items, int nitems, int ctas, long long* grid64,
+                                long long gsize, float* rho, cudaStream_t st) {
+  const size_t smem = batch_scatter_smem();
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    const cudaError_t e = cudaFuncSetAttribute(k_batch_scatter,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr[dev] = true;
+  }
+  cudaError_t e = cudaMemsetAsync(grid64, 0, sizeof(long long) * gsize, st);
+  if (e != cudaSuccess) return e;
+  if (nitems > 0)
+    k_batch_scatter<<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(sorted, start, sys, items,
+                                                                         nitems, grid64);
+  k_batch_fixed_to_real<<<148 * 8, 256, 0, st>>>(grid64, gsize, rho);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_green(float2* rhok, const float* tab, long long ktot, const BatchSys* sys,
+                               const long long* kfirst, const int* ksys, int nsys, double* energy,
+                               cudaStream_t st) {
+  k_batch_green_apply<<<148 * 8, 256, 0, st>>>(rhok, tab, ktot, sys, kfirst, ksys, nsys, energy);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int* start,
+                                const BatchSys* sys, const BatchItem* items, int nitems, int ctas,
+                                const float* phi, double outscale, double* fx, double* fy,
+                                double* fz, cudaStream_t st) {
+  const size_t smem = batch_gather_smem();
+  static bool attr[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev]) {
+    const cudaError_t e = cudaFuncSetAttribute(k_batch_gather,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr[dev] = true;
+  }
+  if (nitems > 0)
+    k_batch_gather<<<std::min(ctas, nitems), kGatherThreads, smem, st>>>(
+        sorted, perm, start, sys, items, nitems, phi, outscale, fx, fy, fz);
+  return cudaGetLastError();
+}
+
 #define GSE_TILED_INST(CT)                                                                      \
   template cudaError_t launch_bin_sorted<CT>(const Vec4<CT>::type*, int, const BinLayout&, CT,  \
                                              CT, CT, BinScratch, Vec4<CT>::type*, int*,         \
                                              cudaStream_t);                                     \
+  template cudaError_t launch_bin_scan_place<CT>(const Vec4<CT>::type*, int, int, BinScratch,   \
+                                                 Vec4<CT>::type*, int*, cudaStream_t);          \
   template bool spread_tiled_supported<CT>(const Stencil<CT>&);                                 \
   template cudaError_t launch_spread_tiled<CT>(const Vec4<CT>::type*, const int*,               \
                                                const unsigned*, const BinLayout&,               \

@@ -68,6 +68,41 @@ inline BinLayout make_bin_layout(const int M[3]) {
 
 inline int bin_count(const BinLayout& b) { return b.M[1] * b.M[2] * b.nbx; }
 
+// One system of a batch (mixed form).  Atoms of all systems are binned with
+// one global key: bin_off + the system's own (z cell, y cell, x bin) key.
+struct BatchSys {
+  BinLayout b;
+  int bin_off;          // first bin of the system
+  int atom_off, n;      // atom range in the caller's concatenated order
+  int W;                // stencil width 2n+1
+  long long grid_off;   // first point of the system's real grids
+  long long kgrid_off;  // first bin of its half spectrum
+  double efac;          // 1/2 ccelec hx hy hz
+  double h3;            // hx hy hz
+  Stencil<float> sp;    // spread stencil (sigma1, rcut1)
+  Stencil<float> sg;    // gather stencil
+};
+
+struct BatchItem {
+  int sys, bx, by, bz;  // brick of one system
+};
+
+size_t batch_scatter_smem();
+size_t batch_gather_smem();
+cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
+                             int nsys, int nbins, BinScratch w, float4* sorted, int* perm,
+                             cudaStream_t st);
+cudaError_t launch_batch_spread(const float4* sorted, const int* start, const BatchSys* sys,
+                                const BatchItem* items, int nitems, int ctas, long long* grid64,
+                                long long gsize, float* rho, cudaStream_t st);
+cudaError_t launch_batch_green(float2* rhok, const float* tab, long long ktot, const BatchSys* sys,
+                               const long long* kfirst, const int* ksys, int nsys, double* energy,
+                               cudaStream_t st);
+cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int* start,
+                                const BatchSys* sys, const BatchItem* items, int nitems, int ctas,
+                                const float* phi, double outscale, double* fx, double* fy,
+                                double* fz, cudaStream_t st);
+
 // Buffers of the mixed-form scatter spread.
 struct ScatterBuffers {
   int* halo;          // [bricks][T][T][T] int32 tiles
@@ -87,6 +122,11 @@ template <typename CT>
 cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const BinLayout& b,
                               CT inv_hx, CT inv_hy, CT inv_hz, BinScratch w,
                               typename Vec4<CT>::type* sorted, int* perm, cudaStream_t st);
+
+template <typename CT>
+cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, int nb,
+                                  BinScratch w, typename Vec4<CT>::type* sorted, int* perm,
+                                  cudaStream_t st);
 
 template <typename CT>
 bool spread_tiled_supported(const Stencil<CT>& s);

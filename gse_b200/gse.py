@@ -414,3 +414,130 @@ def ewald_kcut(sigma, box, tol=1e-12):
     import math
     kmax = math.sqrt(2.0 * math.log(1.0 / tol)) / sigma
     return int(math.ceil(kmax * max(box) / (2.0 * math.pi)))
+
+
+class Batch:
+    """Many independent GSE-k systems of uneven size evaluated together (mixed
+    form).  ``systems`` is a list of dicts with keys size (Mx, My, Mz), box
+    (Lx, Ly, Lz) and n.  Atoms are numbered system after system.
+
+    forward(xyzq) -> (energies[S], forces[n_total, 3]); adjoint(...) gives the
+    reverse pass; capture()/launch() replay one evaluation from a CUDA graph on
+    the batch's own device buffers (``buffers()``); autotune() picks the
+    persistent-CTA counts and work order, cached in a text file."""
+
+    def __init__(self, systems, sigma=1.0, kappa=0.4, lambdaSigma1=3.0, ccelec=CCELEC, device=0):
+        L = _lib.load()
+        p = _lib.gse_params_t()
+        L.gse_params_default(ctypes.byref(p))
+        p.sigma, p.kappa = float(sigma), float(kappa)
+        p.lambda_sigma = p.lambda_sigma1 = float(lambdaSigma1)
+        p.ccelec = float(ccelec)
+        p.precision = _lib.PRECISION["mixed"]
+        p.device = int(device)
+        arr = (_lib.gse_system_t * len(systems))()
+        for k, s in enumerate(systems):
+            arr[k].size_x, arr[k].size_y, arr[k].size_z = (int(v) for v in s["size"])
+            arr[k].box_x, arr[k].box_y, arr[k].box_z = (float(v) for v in s["box"])
+            arr[k].n = int(s["n"])
+        h = ctypes.c_void_p()
+        check(L.gse_batch_create(ctypes.byref(p), len(systems), arr, ctypes.byref(h)))
+        self._L = L
+        self.h = h
+        self.systems = list(systems)
+        self.counts = [int(s["n"]) for s in systems]
+        self.first = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.n_total = int(self.first[-1])
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self._L.gse_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> "_lib.gse_batch_info_t":
+        i = _lib.gse_batch_info_t()
+        check(self._L.gse_batch_info(self.h, ctypes.byref(i)))
+        return i
+
+    def set_stream(self, stream_handle: int):
+        check(self._L.gse_batch_set_stream(self.h, stream_handle))
+
+    def forward(self, xyzq, energies=None, fx=None, fy=None, fz=None):
+        """xyzq: (n_total, 4) float32 host array or CUDA tensor.  Without
+        output arguments, returns (energies, forces) as numpy arrays."""
+        x = _xyzq_arg(xyzq, np.float32)
+        if energies is None and fx is None:
+            e = np.zeros(len(self.counts))
+            f = np.zeros((3, self.n_total))
+            check(self._L.gse_batch_forward(self.h, ptr(x), e.ctypes.data, f[0].ctypes.data,
+                                            f[1].ctypes.data, f[2].ctypes.data))
+            return e, f.T.copy()
+        check(self._L.gse_batch_forward(self.h, ptr(x), ptr(energies), ptr(fx), ptr(fy), ptr(fz)))
+        return None
+
+    def adjoint(self, xyzq, dLdE=None, gforces=None):
+        """Reverse pass of L(E, F).  dLdE: (S,) ; gforces: (n_total, 3) or None.
+        Returns (dL/dq[n], dL/dx[n, 3]) as numpy arrays."""
+        x = _xyzq_arg(xyzq, np.float32)
+        d = None if dLdE is None else np.ascontiguousarray(dLdE, dtype=np.float64)
+        g = None
+        if gforces is not None:
+            g = np.ascontiguousarray(np.asarray(gforces, dtype=np.float64).T)
+        out = np.zeros((4, self.n_total))
+        check(self._L.gse_batch_adjoint(
+            self.h, ptr(x), None if d is None else d.ctypes.data,
+            None if g is None else g[0].ctypes.data, None if g is None else g[1].ctypes.data,
+            None if g is None else g[2].ctypes.data, out[0].ctypes.data, out[1].ctypes.data,
+            out[2].ctypes.data, out[3].ctypes.data))
+        return out[0].copy(), out[1:].T.copy()
+
+    def capture(self, with_adjoint=False):
+        check(self._L.gse_batch_capture(self.h, 1 if with_adjoint else 0))
+
+    def launch(self):
+        check(self._L.gse_batch_launch(self.h))
+
+    def autotune(self, cache_path=None, use_cache=True):
+        check(self._L.gse_batch_autotune(
+            self.h, None if cache_path is None else str(cache_path).encode(), 1 if use_cache else 0))
+
+    def buffers(self):
+        """The batch's device buffers as CUDA torch tensors (views, no copy)."""
+        import torch
+        i = self.info()
+        dev = torch.device("cuda", torch.cuda.current_device())
+
+        def view(addr, n, dtype, shape):
+            return _torch_view(addr, n, dtype, dev).view(*shape)
+
+        n, s = self.n_total, len(self.counts)
+        return {
+            "xyzq": view(i.xyzq, 4 * n, torch.float32, (n, 4)),
+            "energies": view(i.energies, s, torch.float64, (s,)),
+            "forces": view(i.forces, 3 * n, torch.float64, (3, n)),
+            "dLdE": view(i.dLdE, s, torch.float64, (s,)),
+            "grad_forces": view(i.grad_forces, 3 * n, torch.float64, (3, n)),
+            "grad_out": view(i.grad_out, 4 * n, torch.float64, (4, n)),
+        }
+
+
+def _torch_view(addr, numel, dtype, device):
+    """A torch tensor over device memory the library owns (no copy, no ownership)."""
+    import torch
+    if numel == 0:
+        return torch.empty(0, dtype=dtype, device=device)
+
+    class _Iface:
+        pass
+
+    o = _Iface()
+    typestr = {torch.float32: "<f4", torch.float64: "<f8"}[dtype]
+    o.__cuda_array_interface__ = {"shape": (numel,), "typestr": typestr, "data": (addr, False),
+                                  "version": 2, "strides": None}
+    return torch.as_tensor(o, device=device)

@@ -251,6 +251,79 @@ gse_status_t gse_spread_mixed_noalloc(int size_x, int size_y, int size_z, double
                                       double rcut, int n, const float* xyzq, double box_x,
                                       double box_y, double box_z, float* rho_out, void* stream);
 
+/* ---- many independent systems in one pass ------------------------------ */
+
+/* No counterpart in the reference, which evaluates one system per object
+ * (CpuGSEk<AT,CT>::calc_energy_force, CpuGSEk.h).  A batch holds S systems
+ * that share sigma, kappa, lambda_sigma1 and ccelec (from the common
+ * gse_params_t) but each have their own grid, box and atom count.  The mixed
+ * form only (GSE_PRECISION_MIXED): positions are float {x,y,z,q}, results
+ * double.  Every system computes exactly what a mixed gse_forward on its own
+ * context computes, to float-rounding differences of the accumulation order
+ * (grid values are summed in 64-bit fixed point, so a batch's own results do
+ * not change from run to run). */
+typedef struct gse_system {
+  int size_x, size_y, size_z; /* grid points per side, each >= 10 */
+  double box_x, box_y, box_z; /* orthorhombic box lengths */
+  int n;                      /* atoms of this system (>= 0) */
+} gse_system_t;
+
+typedef struct gse_batch gse_batch_t;
+
+/* Sizes and device buffers of a batch.  Atoms are numbered system after
+ * system: system s owns atoms first_s .. first_s + n_s - 1, first_s the sum
+ * of the earlier systems' n.  The device buffers stay valid until
+ * gse_batch_destroy and are the ones a captured graph reads and writes. */
+typedef struct gse_batch_info {
+  int n_total, n_systems, n_size_classes;
+  long long grid_points;           /* real grid points over all systems */
+  int scatter_items, gather_items; /* (system, brick) work items */
+  int scatter_ctas, gather_ctas;   /* persistent CTAs (autotuned) */
+  int largest_first;               /* work items ordered by system size */
+  void* xyzq;                      /* float4 [n_total] positions and charges */
+  double* energies;                /* [n_systems] */
+  double* forces;                  /* [3][n_total]: fx, then fy, then fz */
+  double* dLdE;                    /* [n_systems] reverse-pass input */
+  double* grad_forces;             /* [3][n_total] reverse-pass input */
+  double* grad_out;                /* [4][n_total]: dL/dq, dL/dx, dL/dy, dL/dz */
+} gse_batch_info_t;
+
+/* Build a batch: bins, grids grouped by size for strided FFT plans, and the
+ * Green's-function table of every system (built in FP64). */
+gse_status_t gse_batch_create(const gse_params_t* common, int n_systems,
+                              const gse_system_t* systems, gse_batch_t** batch);
+gse_status_t gse_batch_destroy(gse_batch_t* batch);
+gse_status_t gse_batch_set_stream(gse_batch_t* batch, void* stream);
+gse_status_t gse_batch_info(gse_batch_t* batch, gse_batch_info_t* info);
+
+/* One evaluation of every system.  xyzq: n_total float4 records (host or
+ * device; NULL = use the batch's xyzq buffer as it is).  energies [n_systems],
+ * fx/fy/fz [n_total] may be host, device or NULL. */
+gse_status_t gse_batch_forward(gse_batch_t* batch, const void* xyzq, double* energies,
+                               double* fx, double* fy, double* fz);
+
+/* Forward pass, then the reverse pass of L(E, F): dLdE [n_systems] and the
+ * force cotangents gfx/gfy/gfz [n_total] (all three or none; NULL = zero) give
+ * dL/dq, dL/dx, dL/dy, dL/dz [n_total] (each may be NULL). */
+gse_status_t gse_batch_adjoint(gse_batch_t* batch, const void* xyzq, const double* dLdE,
+                               const double* gfx, const double* gfy, const double* gfz,
+                               double* dq, double* dx, double* dy, double* dz);
+
+/* Capture one forward pass (and, if with_adjoint, the reverse pass) on the
+ * batch's buffers into a CUDA graph; gse_batch_launch replays it on the
+ * batch's stream, asynchronously.  Write inputs into the gse_batch_info
+ * buffers and read results from them.  Changing the stream or re-tuning
+ * drops the graph. */
+gse_status_t gse_batch_capture(gse_batch_t* batch, int with_adjoint);
+gse_status_t gse_batch_launch(gse_batch_t* batch);
+
+/* Time the persistent-CTA counts of spread and gather and the order of the
+ * work items on the batch's current positions, keep the fastest.  With
+ * cache_path, the choice is appended to that text file under a key made of
+ * the system count, grid-size histogram, atom count and SM count; with
+ * use_cache != 0 a cached choice for the same key is taken without timing. */
+gse_status_t gse_batch_autotune(gse_batch_t* batch, const char* cache_path, int use_cache);
+
 #ifdef __cplusplus
 }
 #endif

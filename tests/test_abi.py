@@ -79,6 +79,34 @@ def test_create_without_gpu_reports_unsupported(lib):
 def test_null_context_is_an_error(lib):
     assert lib.gse_solve_poisson(None) == 1
     assert lib.gse_destroy(None) == 0
+    assert lib.gse_batch_forward(None, None, None, None, None, None) == 1
+    assert lib.gse_batch_launch(None) == 1
+    assert lib.gse_batch_destroy(None) == 0
+
+
+def test_batch_create_checks_arguments_before_touching_a_gpu(lib):
+    import torch
+    from gse_b200 import _lib
+    p = _lib.gse_params_t()
+    lib.gse_params_default(ctypes.byref(p))
+    p.sigma = 2.0
+    systems = (_lib.gse_system_t * 2)()
+    for s in systems:
+        s.size_x = s.size_y = s.size_z = 16
+        s.box_x = s.box_y = s.box_z = 16.0
+        s.n = 30
+    h = ctypes.c_void_p()
+    assert lib.gse_batch_create(ctypes.byref(p), 0, systems, ctypes.byref(h)) == 1
+    # the FP64 form has no batched path
+    assert lib.gse_batch_create(ctypes.byref(p), 2, systems, ctypes.byref(h)) == 7
+    assert "mixed" in lib.gse_last_error().decode()
+    p.precision = _lib.PRECISION["mixed"]
+    p.kappa = 0.6
+    assert lib.gse_batch_create(ctypes.byref(p), 2, systems, ctypes.byref(h)) == 1
+    p.kappa = 0.4
+    if not torch.cuda.is_available():
+        assert lib.gse_batch_create(ctypes.byref(p), 2, systems, ctypes.byref(h)) == 7
+    assert not h.value
 
 
 def test_python_mirror_has_reference_methods():

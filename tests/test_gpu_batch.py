@@ -1,0 +1,190 @@
+"""Batched systems (gse_batch_*, mixed form) through the C ABI.
+
+Every system of a batch must give what a mixed single-system context gives on
+its own: energies within 1e-6 relative, forces within 1e-5 relative RMS (the
+two paths round the grid differently: 64-bit fixed point with a global scale
+in the batch, per-brick scales in the single-system spread), and both within
+1e-5 of the FP64 form.  A batch's own results are bit-identical run to run,
+and a replayed CUDA graph gives what the eager call gives."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SIGMA = 2.0
+
+
+def rms(F, R):
+    d = np.asarray(F, np.float64) - np.asarray(R, np.float64)
+    return float(np.sqrt((d * d).sum() / max((np.asarray(R, np.float64) ** 2).sum(), 1e-300)))
+
+
+def mixed_systems():
+    """Uneven systems: cubic ones as the batching workload builds them, plus
+    odd, non-cubic, tiny (stencil wider than the grid) and empty systems."""
+    from gse_b200 import workloads as W
+    out = []
+    for s in W.config_batch(10, seed=3, n_min=501, n_max=4001):
+        out.append({"size": s.grid, "box": s.boxes, "xyzq": s.xyzq})
+    out.append({"size": (17, 18, 20), "box": (17.5, 18.2, 19.9),
+                "xyzq": W.triplets(900, 17.5, 5).astype(np.float32)
+                * np.array([1.0, 18.2 / 17.5, 19.9 / 17.5, 1.0], np.float32)})
+    out.append({"size": (10, 10, 10), "box": (10.0, 10.0, 10.0),
+                "xyzq": W.triplets(99, 10.0, 6).astype(np.float32)})
+    out.append({"size": (16, 16, 16), "box": (16.0, 16.0, 16.0),
+                "xyzq": np.zeros((0, 4), np.float32)})
+    return out
+
+
+def make_batch(systems):
+    from gse_b200.gse import Batch
+    desc = [{"size": s["size"], "box": s["box"], "n": s["xyzq"].shape[0]} for s in systems]
+    b = Batch(desc, sigma=SIGMA, kappa=0.4, lambdaSigma1=3.0)
+    xyzq = np.concatenate([s["xyzq"] for s in systems]).astype(np.float32)
+    return b, xyzq
+
+
+def single(s, precision):
+    from gse_b200.gse import Context
+    M, box = s["size"], s["box"]
+    ctx = Context(M[0], M[1], M[2], SIGMA, 0.4, 3.0, 3.0, box[0], box[1], box[2],
+                  precision=precision)
+    ct = np.float32 if precision == "mixed" else np.float64
+    x = s["xyzq"].astype(ct)
+    n = x.shape[0]
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    E = ctx.forward(n, x, fx, fy, fz) if n else 0.0
+    return ctx, E, np.stack([fx, fy, fz], 1)
+
+
+@pytest.fixture(scope="module")
+def batch_case():
+    systems = mixed_systems()
+    b, xyzq = make_batch(systems)
+    return systems, b, xyzq
+
+
+def test_batch_forward_matches_single_systems(batch_case):
+    systems, b, xyzq = batch_case
+    E, F = b.forward(xyzq)
+    assert E.shape == (len(systems),) and F.shape == (b.n_total, 3)
+    for k, s in enumerate(systems):
+        lo, hi = b.first[k], b.first[k + 1]
+        if hi == lo:
+            assert E[k] == 0.0
+            continue
+        _, Em, Fm = single(s, "mixed")
+        _, Ed, Fd = single(s, "fp64")
+        print(k, s["size"], hi - lo, "E rel", abs(E[k] - Em) / abs(Em), "F rms", rms(F[lo:hi], Fm),
+              "vs fp64", rms(F[lo:hi], Fd))
+        assert abs(E[k] - Em) <= 1e-6 * abs(Em)
+        assert rms(F[lo:hi], Fm) <= 1e-5
+        assert rms(F[lo:hi], Fd) <= 1e-5
+        assert abs(E[k] - Ed) <= 1e-5 * abs(Ed)
+
+
+def test_batch_is_deterministic(batch_case):
+    _, b, xyzq = batch_case
+    E1, F1 = b.forward(xyzq)
+    E2, F2 = b.forward(xyzq)
+    assert np.array_equal(F1, F2)
+    assert np.allclose(E1, E2, rtol=1e-13, atol=0.0)
+
+
+def test_graph_replay_matches_eager(batch_case):
+    import torch
+    _, b, xyzq = batch_case
+    E, F = b.forward(xyzq)
+    bufs = b.buffers()
+    b.capture(with_adjoint=False)
+    bufs["forces"].zero_()
+    bufs["energies"].zero_()
+    for _ in range(3):
+        b.launch()
+    torch.cuda.synchronize()
+    assert np.array_equal(bufs["forces"].cpu().numpy().T, F)
+    assert np.allclose(bufs["energies"].cpu().numpy(), E, rtol=1e-13, atol=0.0)
+    # new positions written into the batch's buffer are picked up by the graph
+    x2 = xyzq.copy()
+    x2[:, :3] += 0.37
+    bufs["xyzq"].copy_(torch.from_numpy(x2))
+    b.launch()
+    torch.cuda.synchronize()
+    E2, F2 = b.forward(x2)
+    assert np.array_equal(bufs["forces"].cpu().numpy().T, F2)
+
+
+def test_batch_adjoint_matches_single_systems(batch_case):
+    systems, b, xyzq = batch_case
+    rng = np.random.default_rng(4)
+    G = rng.standard_normal((b.n_total, 3))
+    dLdE = rng.uniform(0.5, 1.5, len(systems))
+    dq, dx = b.adjoint(xyzq, dLdE, G)
+    for k, s in enumerate(systems):
+        lo, hi = int(b.first[k]), int(b.first[k + 1])
+        n = hi - lo
+        if n == 0:
+            continue
+        ctx, _, _ = single(s, "mixed")
+        x = s["xyzq"].astype(np.float32)
+        q, gx, gy, gz = (np.zeros(n) for _ in range(4))
+        g = G[lo:hi]
+        ctx.adjoint(n, x, float(dLdE[k]), np.ascontiguousarray(g[:, 0]),
+                    np.ascontiguousarray(g[:, 1]), np.ascontiguousarray(g[:, 2]), q, gx, gy, gz)
+        print(k, "dq rms", rms(dq[lo:hi], q), "dx rms", rms(dx[lo:hi], np.stack([gx, gy, gz], 1)))
+        assert rms(dq[lo:hi], q) <= 1e-5
+        assert rms(dx[lo:hi], np.stack([gx, gy, gz], 1)) <= 1e-5
+
+
+def test_graph_with_adjoint_matches_eager(batch_case):
+    import torch
+    systems, b, xyzq = batch_case
+    rng = np.random.default_rng(8)
+    G = rng.standard_normal((b.n_total, 3))
+    dLdE = np.ones(len(systems))
+    dq, dx = b.adjoint(xyzq, dLdE, G)
+    bufs = b.buffers()
+    bufs["xyzq"].copy_(torch.from_numpy(xyzq))
+    bufs["dLdE"].copy_(torch.from_numpy(dLdE))
+    bufs["grad_forces"].copy_(torch.from_numpy(np.ascontiguousarray(G.T)))
+    b.capture(with_adjoint=True)
+    bufs["grad_out"].zero_()
+    b.launch()
+    torch.cuda.synchronize()
+    out = bufs["grad_out"].cpu().numpy()
+    # the reverse pass sums its source grid with FP32 atomics, whose order
+    # differs from run to run
+    assert rms(out[0], dq) <= 1e-6
+    assert rms(out[1:].T, dx) <= 1e-6
+
+
+def test_autotune_and_cache(batch_case, tmp_path):
+    _, b, xyzq = batch_case
+    E0, F0 = b.forward(xyzq)
+    cache = tmp_path / "tune.txt"
+    b.autotune(cache, use_cache=False)
+    i1 = b.info()
+    text = cache.read_text().split()
+    assert len(text) == 5 and text[0].startswith("batch-n")
+    E1, F1 = b.forward(xyzq)
+    assert rms(F1, F0) <= 1e-12 and np.allclose(E1, E0, rtol=1e-12)
+    b.autotune(cache, use_cache=True)  # taken from the file, no new line
+    i2 = b.info()
+    assert len(cache.read_text().splitlines()) == 1
+    assert (i1.scatter_ctas, i1.gather_ctas, i1.largest_first) == \
+        (i2.scatter_ctas, i2.gather_ctas, i2.largest_first)
+
+
+def test_batch_of_256_systems_runs():
+    """The batching workload's full size: 256 systems, N log-uniform in
+    [501, 8001].  Spot-check three systems against single contexts."""
+    from gse_b200 import workloads as W
+    syst = [{"size": s.grid, "box": s.boxes, "xyzq": s.xyzq} for s in W.config_batch(256)]
+    b, xyzq = make_batch(syst)
+    E, F = b.forward(xyzq)
+    assert np.isfinite(E).all() and np.isfinite(F).all()
+    for k in (0, 100, 255):
+        lo, hi = b.first[k], b.first[k + 1]
+        _, Em, Fm = single(syst[k], "mixed")
+        assert abs(E[k] - Em) <= 1e-6 * abs(Em)
+        assert rms(F[lo:hi], Fm) <= 1e-5
