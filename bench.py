@@ -183,6 +183,56 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_batch(steps: int, warmup: int, flush):
+    """The batching workload: 256 independent triplet systems, N log-uniform in
+    [501, 8001], forward + reverse pass replayed from one CUDA graph after the
+    autotuner has picked the persistent-CTA counts and the work order."""
+    import tempfile
+
+    import torch
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Batch
+    syst = W.config_batch(256)
+    desc = [{"size": y.grid, "box": y.boxes, "n": y.n} for y in syst]
+    b = Batch(desc, sigma=2.0, kappa=0.4, lambdaSigma1=3.0)
+    xyzq = np.concatenate([y.xyzq for y in syst]).astype(np.float32)
+    rng = np.random.default_rng(5)
+    G = rng.standard_normal((b.n_total, 3)).astype(np.float32).astype(np.float64)
+    b.forward(xyzq)
+    cache = os.path.join(tempfile.gettempdir(), "gse_batch_tune.txt")
+    b.autotune(cache, use_cache=False)
+    bufs = b.buffers()
+    bufs["xyzq"].copy_(torch.from_numpy(xyzq))
+    bufs["dLdE"].fill_(1.0)
+    bufs["grad_forces"].copy_(torch.from_numpy(np.ascontiguousarray(G.T)))
+    stream = torch.cuda.current_stream()
+    b.set_stream(stream.cuda_stream)
+    b.capture(with_adjoint=True)
+    for _ in range(warmup):
+        b.launch()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record(stream)
+        b.launch()
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(c) for a, c in zip(starts, ends)) / steps
+    i = b.info()
+    out = {"workload": "256 independent triplet systems, N log-uniform in [501, 8001], "
+                       "M = nearest multiple of 8 to L, sigma 2.0, mixed form",
+           "n_total": b.n_total, "size_classes": int(i.n_size_classes),
+           "grid_points": int(i.grid_points), "step": "forward + reverse pass, one CUDA graph",
+           "ms_per_step": ms, "systems_per_s": 256 / (ms / 1000.0),
+           "charges_per_s": b.n_total / (ms / 1000.0),
+           "autotuned": {"scatter_ctas": int(i.scatter_ctas), "gather_ctas": int(i.gather_ctas),
+                         "largest_first": bool(i.largest_first)}}
+    b.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -191,6 +241,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -343,13 +394,13 @@ def main():
         ab = algorithmic_bytes(dom, prec)
         achieved = ab / (dom_ms / 1000.0) / 1e9
         traffic = None
-        prof = os.path.join(ROOT, "profiles", f"{dom}_{prec}_traffic.json")
+        prof = os.path.join(ROOT, "profiles", "traffic_water262k.txt")
         if os.path.exists(prof):
-            try:
-                with open(prof) as fh:
-                    traffic = json.load(fh).get("dram_bytes_per_launch")
-            except Exception:
-                traffic = None
+            with open(prof) as fh:
+                for ln in fh:
+                    parts = ln.split()
+                    if len(parts) == 3 and parts[0] == dom and parts[1] == prec:
+                        traffic = int(parts[2])
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
@@ -365,6 +416,12 @@ def main():
             except Exception as exc:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                        "sample": f"failed: {exc}"}
+        batch = None
+        if not args.no_batch:
+            try:
+                batch = bench_batch(max(3, min(args.steps, 20)), args.warmup, flush)
+            except Exception as exc:  # noqa: BLE001
+                batch = {"failed": str(exc)}
         per_stage = {k: round(v[0] / max(v[1], 1), 4) for k, v in stage.items()}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -389,6 +446,7 @@ def main():
             "mixed_vs_fp64": {"force_rms": force_rms, "energy_rel": energy_rel},
             "vs_ewald": accuracy,
             "energy": E_main,
+            "batch": batch,
         }
         print(json.dumps(line), flush=True)
 

@@ -1,0 +1,88 @@
+// gse_dropin_check.cpp -- a caller written against the reference's class API
+// (the sequence cpu_gse.cpp runs for its GSE-k test, cpu_gse.cpp:424-455),
+// compiled against gse_dropin.h instead of the reference headers.
+//
+// usage: gse_dropin_check fp64|mixed Mx My Mz Lx Ly Lz sigma xyzq.txt
+//   xyzq.txt: one "x y z q" record per line.
+// Prints "E <energy>" and one "F fx fy fz" line per atom from CpuGSEk, then
+// "E_stages <energy>" and "F_stages ..." lines from the same computation
+// assembled out of CpuGaussCharge, CpuGreensFuncGSE and CpuFFTSolver.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "gse_dropin.h"
+
+using gse_b200::CpuFFTSolver;
+using gse_b200::CpuGaussCharge;
+using gse_b200::CpuGreensFuncGSE;
+using gse_b200::CpuGrid;
+using gse_b200::CpuGSEk;
+using gse_b200::xyzq_t;
+
+template <typename CT>
+int run(int M[3], double L[3], double sigma, const std::vector<double>& raw) {
+  const int n = (int)raw.size() / 4;
+  std::vector<xyzq_t<CT>> xyzq(n);
+  for (int i = 0; i < n; i++)
+    xyzq[i] = {(CT)raw[4 * i], (CT)raw[4 * i + 1], (CT)raw[4 * i + 2], (CT)raw[4 * i + 3]};
+  const double kappa = 0.4, lambdaSigma = 3.0, lambdaSigma1 = 3.0, ccelec = 332.0716;
+  std::vector<double> fx(n), fy(n), fz(n);
+
+  CpuGSEk<double, CT> gse(M[0], M[1], M[2], sigma, kappa, lambdaSigma, lambdaSigma1, L[0], L[1],
+                          L[2], ccelec);
+  gse.spreadCharge1(n, xyzq.data());
+  gse.solvePoisson();
+  const double E = gse.calculateEnergy();
+  gse.interpolateForce(n, xyzq.data(), fx.data(), fy.data(), fz.data());
+  printf("E %.17g\n", E);
+  for (int i = 0; i < n; i++) printf("F %.17g %.17g %.17g\n", fx[i], fy[i], fz[i]);
+
+  // the same evaluation from the stage classes
+  const double sigma1 = gse.getSigma1(), sigma2 = gse.getSigma2();
+  const double rcut = gse.getLambdaSigma1() * std::sqrt(2.0) * sigma1;
+  CpuGaussCharge<double, CT> gauss(M[0], M[1], M[2]);
+  CpuGreensFuncGSE<CT> green;
+  CpuFFTSolver<CT> solver(green, M[0], M[1], M[2]);
+  CpuGrid<CT> rho(M[0], M[1], M[2]), phi(M[0], M[1], M[2]);
+  gauss.spreadChargeToGrid(sigma1, rcut, n, xyzq.data(), L[0], L[1], L[2], rho);
+  solver.run(phi, rho, sigma2, L[0], L[1], L[2]);
+  double dot = 0.0;
+  for (int i = 0; i < rho.getSize(); i++)
+    dot += (double)rho.getDataPointer()[i] * (double)phi.getDataPointer()[i];
+  const double h3 = (L[0] / M[0]) * (L[1] / M[1]) * (L[2] / M[2]);
+  printf("E_stages %.17g\n", 0.5 * ccelec * h3 * dot);
+  gauss.interpolateForce(sigma1, rcut, n, xyzq.data(), L[0], L[1], L[2], phi, fx.data(),
+                         fy.data(), fz.data());
+  for (int i = 0; i < n; i++)
+    printf("F_stages %.17g %.17g %.17g\n", ccelec * fx[i], ccelec * fy[i], ccelec * fz[i]);
+  return 0;
+}
+
+int main(int argc, char** argv) {
+  if (argc != 10) {
+    fprintf(stderr, "usage: %s fp64|mixed Mx My Mz Lx Ly Lz sigma xyzq.txt\n", argv[0]);
+    return 2;
+  }
+  int M[3] = {atoi(argv[2]), atoi(argv[3]), atoi(argv[4])};
+  double L[3] = {atof(argv[5]), atof(argv[6]), atof(argv[7])};
+  const double sigma = atof(argv[8]);
+  FILE* f = fopen(argv[9], "r");
+  if (!f) {
+    fprintf(stderr, "cannot open %s\n", argv[9]);
+    return 2;
+  }
+  std::vector<double> raw;
+  double v;
+  while (fscanf(f, "%lf", &v) == 1) raw.push_back(v);
+  fclose(f);
+  try {
+    if (!strcmp(argv[1], "fp64")) return run<double>(M, L, sigma, raw);
+    if (!strcmp(argv[1], "mixed")) return run<float>(M, L, sigma, raw);
+    fprintf(stderr, "precision must be fp64 or mixed\n");
+    return 2;
+  } catch (const gse_b200::Error& e) {
+    fprintf(stderr, "error: %s\n", e.what());
+    return 1;
+  }
+}
