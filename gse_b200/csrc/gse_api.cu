@@ -110,12 +110,6 @@ struct gse_context {
   int* d_bstart = nullptr;
   int* d_btiles = nullptr;
   unsigned* d_qmax = nullptr;
-  // mixed-form scatter spread: halo tiles, per-tile scales, cover tables
-  int scat_w = 0;
-  int* d_halo = nullptr;
-  double* d_hscale = nullptr;
-  short2* d_cover = nullptr;
-  int cover_stride = 0;
   // Green's function table of the context's own solve (sigma2, box)
   void* d_gtab = nullptr;
   bool gtab_valid = false;
@@ -275,30 +269,6 @@ gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT
 }
 
 // Size the scatter buffers for stencil width W (once per width).
-gse_status_t ensure_scatter(gse_context_t* c, int W) {
-  if (c->scat_w == W) return GSE_OK;
-  std::vector<short2> cov;
-  int stride = 0;
-  if (!scatter_cover_table(c->bl, W, cov, &stride))
-    return fail(GSE_ERR_UNSUPPORTED, "grid too small for the scatter spread");
-  cudaFree(c->d_halo);
-  cudaFree(c->d_hscale);
-  cudaFree(c->d_cover);
-  cudaFree(c->d_gtab);
-  cudaFree(c->d_adj);
-  c->d_halo = nullptr;
-  c->d_hscale = nullptr;
-  c->d_cover = nullptr;
-  c->scat_w = 0;
-  CU(cudaMalloc(&c->d_halo, sizeof(int) * scatter_halo_words(c->bl, W)));
-  CU(cudaMalloc(&c->d_hscale, sizeof(double) * scatter_brick_count(c->bl)));
-  CU(cudaMalloc(&c->d_cover, sizeof(short2) * cov.size()));
-  CU(cudaMemcpy(c->d_cover, cov.data(), sizeof(short2) * cov.size(), cudaMemcpyHostToDevice));
-  c->cover_stride = stride;
-  c->scat_w = W;
-  return GSE_OK;
-}
-
 template <typename CT>
 bool tiled_ok(const gse_context_t* c, const Stencil<CT>& s) {
   return spread_tiled_supported<CT>(s) && c->p.size_x >= kMinTiledGrid &&
@@ -314,7 +284,6 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
   if (!normalize && tiled_ok<CT>(c, s)) {
     if (!presorted) TRY(bin_atoms<CT>(c, n, dx, s));
-    if (!c->fp64) TRY(ensure_scatter(c, 2 * s.nst[0] + 1));
     StageTimer tm(c, GSE_STAGE_SPREAD);
     if (c->fp64) {
       c->launches += 1;
@@ -322,8 +291,7 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
                                  (CT*)c->d_rho, c->stream));
     } else if constexpr (sizeof(CT) == 4) {
       c->launches += 2;
-      ScatterBuffers sb{c->d_halo, c->d_hscale, c->d_cover, c->cover_stride};
-      CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl, s, sb,
+      CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl, s, c->d_fixed,
                                (float*)c->d_rho, c->stream));
     }
   } else {
@@ -656,9 +624,6 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_bstart);
   cudaFree(c->d_btiles);
   cudaFree(c->d_qmax);
-  cudaFree(c->d_halo);
-  cudaFree(c->d_hscale);
-  cudaFree(c->d_cover);
   cudaFree(c->d_gtab);
   cudaFree(c->d_adj);
   cudaFree(c->d_partials);

@@ -427,16 +427,18 @@ __global__ void __launch_bounds__(kSpreadThreads)
 // ===========================================================================
 // A CTA owns the atoms of one kSB^3-cell brick and a shared tile of the brick
 // plus its n-cell halo, T = kSB + 2n points per axis, in int32 fixed point at
-// a scale 2^S chosen for this brick so that no partial sum can overflow
-// (|q| pref summed over the brick's atoms, times 2^S, stays below 2^30).
-// One warp per atom: lanes take (x, z) pairs of the (2n+1)^2 plane, form
-// t = round(q pref wx wz 2^(S+1)) and add round(t wy_int / 2^32) with
-// wy_int = round(wy (2^31 - 1)) for each of the 2n+1 y values -- one
-// mad.wide.s32 and one shared-memory integer reduction per cube point.
-// The z-plane pitch is congruent to 2n+1 mod 32, so the 32 lanes of an
+// a power-of-two scale 2^S chosen for this brick so that no partial sum can
+// overflow (|q| pref summed over the brick's atoms, times 2^S, stays below
+// 2^30, and every single contribution below 2^22).  One warp per atom: lanes
+// take (x, z) pairs of the (2n+1)^2 plane, form t = q pref wx wz 2^S and add
+// round(t wy) for each of the 2n+1 y values -- one fma (rounding by the
+// 1.5 * 2^23 magic constant) and one shared-memory integer reduction per cube
+// point.  The z-plane pitch is congruent to 2n+1 mod 32, so the 32 lanes of an
 // instruction (consecutive (x, z) pairs) hit 32 different banks.
-// The tile goes to its slot of a halo buffer; k_spread_fold sums the
-// overlapping tiles in a fixed order into the grid.
+// The finished tile is added into an int64 grid at the common scale
+// 2^kFlushBits (S <= kFlushBits, so the shift is exact) by integer
+// reductions; integer sums do not depend on their order, so the grid is the
+// same bit for bit on every run.
 template <int W>
 struct ScatterGeom {
   static constexpr int n = (W - 1) / 2;
@@ -446,22 +448,15 @@ struct ScatterGeom {
   static constexpr int words = T * PP;
 };
 
-// Where a finished brick tile goes: its slot of the halo buffer (summed later
-// by k_spread_fold), or straight into an int64 grid at 2^kFlushBits by
-// integer reductions (order-independent, so still deterministic).
-struct ScatterOut {
-  int* halo;            // halo mode: [bricks][T^3] slots, with
-  double* halo_scale;   //            2^-S per brick
-  int brick;
-  long long* grid64;    // flush mode: the system's int64 grid
-};
 constexpr int kFlushBits = 40;
+constexpr int kMinShift = 11;  // 2^30 * 2^(40-11) * 8 overlapping tiles < 2^63
 
 template <int W>
 __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
                                               const int* __restrict__ start, const BinLayout& b,
                                               const Stencil<float>& s, int bxi, int byi, int bzi,
-                                              int* __restrict__ tile, const ScatterOut& out) {
+                                              int* __restrict__ tile,
+                                              long long* __restrict__ grid64) {
   typedef ScatterGeom<W> G;
   constexpr int n = G::n, T = G::T;
   constexpr int NT = kScatterThreads, NW = NT / 32;
@@ -520,11 +515,10 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
     const double sum_b = (double)q * pref * 1.0001 + 1e-30;
     const double one_b = (double)m * pref * 1.0001 + 1e-30;
     int sh = kFlushBits;
-    while (sh > -60 && (sum_b * exp2((double)sh) >= 1073741824.0 ||
-                        one_b * exp2((double)sh) >= 4194304.0))
+    while (sh > kMinShift && (sum_b * exp2((double)sh) >= 1073741824.0 ||
+                              one_b * exp2((double)sh) >= 4194304.0))
       sh--;
     s_shift = sh;
-    if (out.halo_scale) out.halo_scale[out.brick] = exp2(-(double)sh);
   }
   __syncthreads();
   const float tscale = exp2f((float)s_shift);
@@ -586,15 +580,8 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
     }
     __syncthreads();
   }
-  if (out.halo) {
-    // tile -> halo slot [z][y][x], T^3 ints
-    int* dst = out.halo + (long long)out.brick * (T * T * T);
-    for (int i = tid; i < T * T * T; i += NT) {
-      const int zz = i / (T * T);
-      dst[i] = tile[zz * G::PP + (i - zz * T * T)];
-    }
-  } else {
-    // tile -> int64 grid at 2^kFlushBits (S <= kFlushBits, so the shift is exact)
+  {
+    // tile -> int64 grid at 2^kFlushBits
     const long long mul = 1LL << (kFlushBits - s_shift);
     for (int i = tid; i < T * T * T; i += NT) {
       const int zz = i / (T * T), r = i - zz * T * T, yy = r / T, xx = r - yy * T;
@@ -602,7 +589,7 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
       if (v != 0) {
         const int gx = wrap1(x0 - n + xx, b.M[0]), gy = wrap1(y0 - n + yy, b.M[1]),
                   gz = wrap1(z0 - n + zz, b.M[2]);
-        atomicAdd((unsigned long long*)(out.grid64 + gx +
+        atomicAdd((unsigned long long*)(grid64 + gx +
                                         ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
                   (unsigned long long)((long long)v * mul));
       }
@@ -613,72 +600,18 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
 template <int W>
 __global__ void __launch_bounds__(kScatterThreads)
     k_spread_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
-                     BinLayout b, Stencil<float> s, int* __restrict__ halo,
-                     double* __restrict__ halo_scale) {
+                     BinLayout b, Stencil<float> s, long long* __restrict__ grid64) {
   extern __shared__ int tile[];
-  const int brick = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  ScatterOut out{halo, halo_scale, brick, nullptr};
-  scatter_brick<W>(sorted, start, b, s, blockIdx.x, blockIdx.y, blockIdx.z, tile, out);
+  scatter_brick<W>(sorted, start, b, s, blockIdx.x, blockIdx.y, blockIdx.z, tile, grid64);
 }
 
-// rho(x, y, z) = sum over the brick tiles covering the point of
-// tile value * 2^-S(brick), in a fixed order (the cover lists).
-template <int W>
-__global__ void k_spread_fold(const int* __restrict__ halo, const double* __restrict__ halo_scale,
-                              BinLayout b, int nbx, int nby, const short2* __restrict__ cover,
-                              int cov_stride, float* __restrict__ rho) {
-  constexpr int T = ScatterGeom<W>::T;
-  constexpr int kFast = 2;  // covers per axis handled without a loop
-  constexpr int ZP = kFoldZ;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y, zb = blockIdx.z * ZP;
-  if (x >= b.M[0]) return;
-  const short2* cx = cover + (0 * cov_stride + x) * kMaxCover;
-  const short2* cy = cover + (1 * cov_stride + y) * kMaxCover;
-  const bool fast_xy = cx[kFast].x < 0 && cy[kFast].x < 0;
-  short2 ex[kFast], ey[kFast];
-#pragma unroll
-  for (int i = 0; i < kFast; i++) {
-    ex[i] = cx[i];
-    ey[i] = cy[i];
-  }
-#pragma unroll
-  for (int zi = 0; zi < ZP; zi++) {
-    const int z = min(zb + zi, b.M[2] - 1);  // planes past the end repeat the last one
-    const short2* cz = cover + (2 * cov_stride + z) * kMaxCover;
-    double acc = 0.0;
-    if (fast_xy && cz[kFast].x < 0) {
-      int v[kFast * kFast * kFast];
-      int br[kFast * kFast * kFast];
-#pragma unroll
-      for (int i = 0; i < kFast; i++) {
-        const short2 ez = cz[i];
-#pragma unroll
-        for (int j = 0; j < kFast; j++)
-#pragma unroll
-          for (int k = 0; k < kFast; k++) {
-            const int e = (i * kFast + j) * kFast + k;
-            const bool ok = ez.x >= 0 && ey[j].x >= 0 && ex[k].x >= 0;
-            br[e] = ok ? (ez.x * nby + ey[j].x) * nbx + ex[k].x : -1;
-            v[e] = ok ? halo[(long long)br[e] * (T * T * T) + (ez.y * T + ey[j].y) * T + ex[k].y]
-                      : 0;
-          }
-      }
-#pragma unroll
-      for (int e = 0; e < kFast * kFast * kFast; e++)
-        if (br[e] >= 0) acc += (double)v[e] * halo_scale[br[e]];
-    } else {
-      for (int i = 0; i < kMaxCover && cz[i].x >= 0; i++)
-        for (int j = 0; j < kMaxCover && cy[j].x >= 0; j++)
-          for (int k = 0; k < kMaxCover && cx[k].x >= 0; k++) {
-            const int brk = (cz[i].x * nby + cy[j].x) * nbx + cx[k].x;
-            acc += (double)halo[(long long)brk * (T * T * T) + (cz[i].y * T + cy[j].y) * T +
-                                cx[k].y] *
-                   halo_scale[brk];
-          }
-    }
-    rho[x + ((long long)y + (long long)z * b.M[1]) * b.M[0]] = (float)acc;
-  }
+// float grid from the int64 accumulation grid at 2^kFlushBits
+__global__ void k_grid64_to_real(const long long* __restrict__ g64, long long size,
+                                 float* __restrict__ out) {
+  const double unscale = exp2(-(double)kFlushBits);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)((double)g64[i] * unscale);
 }
 
 // ===========================================================================
@@ -779,16 +712,25 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   if (tid == 0) rng_p[NR] = natoms;
   if (natoms == 0) return;  // uniform: natoms is the same in every thread
 
-  // potential of the brick plus halo, one (y, z) row per warp iteration
+  // potential of the brick plus halo, one (y, z) row per warp iteration, as
+  // asynchronous element copies (cp.async) so that a warp keeps all of its
+  // rows in flight instead of waiting for each load
+  static_assert(TX <= 32, "one lane per tile column");
   const long long zs = (long long)b.M[0] * b.M[1];
+  const int gx = lane < TX ? wrap1(x0 - n + lane, b.M[0]) : 0;
   for (int r = warp; r < TY * TZ; r += NW) {
     const int ty = r % TY, tz = r / TY;
     const int gy = wrap1(y0 - n + ty, b.M[1]);
     const int gz = wrap1(z0 - n + tz, b.M[2]);
-    const CT* src = phi + (long long)gy * b.M[0] + gz * zs;
-    CT* dst = tile + tz * ZP + ty * TP;
-    for (int tx = lane; tx < TX; tx += 32) dst[tx] = src[wrap1(x0 - n + tx, b.M[0])];
+    const CT* src = phi + (long long)gy * b.M[0] + gz * zs + gx;
+    if (lane < TX) {
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tz * ZP + ty * TP + lane);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src),
+                   "n"(sizeof(CT))
+                   : "memory");
+    }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
   CT* tb = tabs + warp * 9 * kWPad;  // [axis][d, d^2, w][j]
@@ -1007,7 +949,7 @@ cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int
 
 template <int W>
 static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLayout& b,
-                             const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                             const Stencil<float>& s, long long* grid64, float* rho,
                              cudaStream_t st) {
   typedef ScatterGeom<W> G;
   const size_t smem = sizeof(int) * G::words;
@@ -1021,62 +963,25 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
     if (e != cudaSuccess) return e;
     attr[dev] = true;
   }
+  const long long size = (long long)b.M[0] * b.M[1] * b.M[2];
+  cudaError_t e = cudaMemsetAsync(grid64, 0, sizeof(long long) * size, st);
+  if (e != cudaSuccess) return e;
   const int nb[3] = {(b.M[0] + kSB - 1) / kSB, (b.M[1] + kSB - 1) / kSB,
                      (b.M[2] + kSB - 1) / kSB};
-  k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(
-      sorted, start, b, s, buf.halo, buf.scale);
-  dim3 fg((b.M[0] + 127) / 128, b.M[1], (b.M[2] + kFoldZ - 1) / kFoldZ);
-  k_spread_fold<W><<<fg, 128, 0, st>>>(buf.halo, buf.scale, b, nb[0], nb[1], buf.cover,
-                                        buf.cover_stride, rho);
+  k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(sorted, start, b,
+                                                                              s, grid64);
+  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, rho);
   return cudaGetLastError();
 }
 
-size_t scatter_halo_words(const BinLayout& b, int W) {
-  const int T = kSB + (W - 1);
-  const size_t nb = (size_t)((b.M[0] + kSB - 1) / kSB) * ((b.M[1] + kSB - 1) / kSB) *
-                    ((b.M[2] + kSB - 1) / kSB);
-  return nb * (size_t)T * T * T;
-}
-
-size_t scatter_brick_count(const BinLayout& b) {
-  return (size_t)((b.M[0] + kSB - 1) / kSB) * ((b.M[1] + kSB - 1) / kSB) *
-         ((b.M[2] + kSB - 1) / kSB);
-}
-
-bool scatter_cover_table(const BinLayout& b, int W, std::vector<short2>& out, int* stride) {
-  const int n = (W - 1) / 2, T = kSB + 2 * n;
-  int mx = 0;
-  for (int d = 0; d < 3; d++) mx = b.M[d] > mx ? b.M[d] : mx;
-  *stride = mx;
-  out.assign((size_t)3 * mx * kMaxCover, make_short2(-1, -1));
-  for (int d = 0; d < 3; d++) {
-    const int M = b.M[d], nb = (M + kSB - 1) / kSB;
-    for (int x = 0; x < M; x++) {
-      int cnt = 0;
-      for (int bb = 0; bb < nb; bb++) {
-        const int u0 = bb * kSB - n;  // unwrapped start of the tile
-        for (int k = -((T + M) / M) - 1; k <= (T + M) / M + 1; k++) {
-          const int o = x + k * M - u0;
-          if (o >= 0 && o < T) {
-            if (cnt >= kMaxCover) return false;
-            out[((size_t)d * mx + x) * kMaxCover + cnt] = make_short2((short)bb, (short)o);
-            cnt++;
-          }
-        }
-      }
-    }
-  }
-  return true;
-}
-
 cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
-                                  const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                                  const Stencil<float>& s, long long* grid64, float* rho,
                                   cudaStream_t st) {
   switch (2 * s.nst[0] + 1) {
-    case 9: return scatter_w<9>(sorted, start, b, s, buf, rho, st);
-    case 11: return scatter_w<11>(sorted, start, b, s, buf, rho, st);
-    case 13: return scatter_w<13>(sorted, start, b, s, buf, rho, st);
-    case 15: return scatter_w<15>(sorted, start, b, s, buf, rho, st);
+    case 9: return scatter_w<9>(sorted, start, b, s, grid64, rho, st);
+    case 11: return scatter_w<11>(sorted, start, b, s, grid64, rho, st);
+    case 13: return scatter_w<13>(sorted, start, b, s, grid64, rho, st);
+    case 15: return scatter_w<15>(sorted, start, b, s, grid64, rho, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -1122,7 +1027,7 @@ __global__ void __launch_bounds__(kScatterThreads)
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const BatchItem item = items[it];
     const BatchSys& S = sys[item.sys];
-    const ScatterOut out{nullptr, nullptr, 0, grid64 + S.grid_off};
+    long long* out = grid64 + S.grid_off;
     const int* st = start + S.bin_off;
     switch (S.W) {
       case 9: scatter_brick<9>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
@@ -1132,14 +1037,6 @@ __global__ void __launch_bounds__(kScatterThreads)
     }
     __syncthreads();
   }
-}
-
-__global__ void k_batch_fixed_to_real(const long long* __restrict__ g64, long long size,
-                                      float* __restrict__ out) {
-  const double unscale = exp2(-(double)kFlushBits);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = (float)((double)g64[i] * unscale);
 }
 
 // rhok *= G per bin; energy[s] += efac_s * sum_k G |rho(k)|^2 (full spectrum).
@@ -1253,7 +1150,7 @@ cudaError_t launch_batch_spread(const float4* sorted, const int* start, const Ba
   if (nitems > 0)
     k_batch_scatter<<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(sorted, start, sys, items,
                                                                          nitems, grid64);
-  k_batch_fixed_to_real<<<148 * 8, 256, 0, st>>>(grid64, gsize, rho);
+  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, gsize, rho);
   return cudaGetLastError();
 }
 

@@ -19,11 +19,9 @@ constexpr int kSpreadChunk = 64;    // atoms staged per round
 constexpr int kMaxSeg = 4;          // periodic images of one row segment
 constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX
 constexpr int kGatherThreads = 256;          // >= kGY * kGZ
-constexpr int kFoldZ = 8;                    // z planes per fold thread
 constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
 constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
 constexpr int kScatterThreads = 512;  // >= kSB * kSB
-constexpr int kMaxCover = 8;        // brick tiles covering one coordinate
 constexpr int kScatterList = 1024;  // atoms per scatter round (per brick)
 constexpr int kGatherList = 512;    // atoms per gather round (per brick)
 
@@ -103,19 +101,10 @@ cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int
                                 const float* phi, double outscale, double* fx, double* fy,
                                 double* fz, cudaStream_t st);
 
-// Buffers of the mixed-form scatter spread.
-struct ScatterBuffers {
-  int* halo;          // [bricks][T][T][T] int32 tiles
-  double* scale;      // [bricks] 2^-S of each tile
-  const short2* cover;  // [3][cover_stride][kMaxCover] (brick, tile offset), -1 = end
-  int cover_stride;
-};
-
-size_t scatter_halo_words(const BinLayout& b, int W);
-size_t scatter_brick_count(const BinLayout& b);
-bool scatter_cover_table(const BinLayout& b, int W, std::vector<short2>& out, int* stride);
+// Mixed-form spread: brick tiles added into the int64 grid `grid64` (cleared
+// here) at 2^40, then converted into the float grid `rho`.
 cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
-                                  const Stencil<float>& s, ScatterBuffers buf, float* rho,
+                                  const Stencil<float>& s, long long* grid64, float* rho,
                                   cudaStream_t st);
 
 template <typename CT>
