@@ -21,6 +21,7 @@
 #include "gse_adjoint.cuh"
 #include "gse_internal.cuh"
 #include "gse_tiled.cuh"
+#include "gse_tiled_dev.cuh"
 
 namespace gse {
 
@@ -191,6 +192,537 @@ __global__ void __launch_bounds__(256)
     adj_gather_atom<float>(xyzq[ii], perm[ii], S.sp, S.sg, c, dLdE[si] * c * S.h3,
                            psi + S.grid_off, phi + S.grid_off, gfx, gfy, gfz, dq, dx, dy, dz);
   }
+}
+
+// ===========================================================================
+// Tiled reverse pass (mixed form)
+// ===========================================================================
+// The same brick decomposition as the forward pass.  The adjoint source is
+// scattered like the charge spread (one warp per atom, lanes over (x, z)
+// pairs of the stencil plane, the y values in registers) into an int32 brick
+// tile that is added into an int64 grid, so lambda is bit-identical from run
+// to run.  The weight of a point is e (G . u) over the gather sphere:
+// separable in its y factor, e_x e_z (Gx u_x + Gz u_z) e_y + e_x e_z Gy (e_y u_y).
+// The sphere test here is u_y^2 < rcut^2 - (u_x^2 + u_z^2); it may differ
+// from the forward gather's association of the same sum only for points
+// whose distance equals the cut-off to rounding, whose weight is e^-9 of the
+// centre's.
+
+template <int W>
+__device__ __forceinline__ void adj_scatter_brick(
+    const float4* __restrict__ sorted, const int* __restrict__ perm, const int* __restrict__ start,
+    const BinLayout& b, const Stencil<float>& s, float cA, const double* __restrict__ gfx,
+    const double* __restrict__ gfy, const double* __restrict__ gfz, int bxi, int byi, int bzi,
+    int* __restrict__ tile, long long* __restrict__ grid64) {
+  typedef ScatterGeom<W> G;
+  constexpr int n = G::n;
+  constexpr int NT = kScatterThreads, NW = NT / 32;
+  constexpr int NPASS = (W * W + 31) / 32;
+  __shared__ int rng_a[kSB * kSB], rng_p[kSB * kSB];
+  __shared__ int alist[kScatterList];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = bxi * kSB, y0 = byi * kSB, z0 = bzi * kSB;
+  // |cA q e (G.u)| <= |cA q| |G| max_u |u| exp(-u^2/(2 s^2)) = |cA q| |G| s e^(-1/2)
+  const float acA = fabsf(cA) * sqrtf(0.5f / s.inv_2s2) * 0.60653066f * 1.0001f;
+  int total;
+  const int shift = brick_prologue<W, NT>(
+      start, b, x0, y0, z0, tile, rng_a, rng_p,
+      [&](int i) {
+        const int o = perm[i];
+        const float gx = (float)gfx[o], gy = (float)gfy[o], gz = (float)gfz[o];
+        return fabsf(sorted[i].w) * acA * sqrtf(gx * gx + gy * gy + gz * gz);
+      },
+      &total);
+  const float tscale = exp2f((float)shift);
+  int poff[NPASS], psx[NPASS], psz[NPASS];
+#pragma unroll
+  for (int pass = 0; pass < NPASS; pass++) {
+    const int p = pass * 32 + lane;
+    const int pz = p < W * W ? p / W : 0, px = p < W * W ? p - (p / W) * W : 0;
+    psx[pass] = px;
+    psz[pass] = pz;
+    poff[pass] = pz * G::PP + px;
+  }
+  for (int c0 = 0; c0 < total; c0 += kScatterList) {
+    brick_atom_list<NT, kSB * kSB>(rng_a, rng_p, total, c0, kScatterList, alist);
+    __syncthreads();
+    const int nc = min(kScatterList, total - c0);
+    for (int q = warp; q < nc; q += NW) {
+      const int ai = alist[q];
+      const float4 a = sorted[ai];
+      const int o = perm[ai];
+      const float Gx = (float)gfx[o], Gy = (float)gfy[o], Gz = (float)gfz[o];
+      const float pos3[3] = {a.x, a.y, a.z};
+      const int org[3] = {x0, y0, z0};
+      int loc[3];
+      float ul[3], u2l[3], el[3];  // lane j < W: u = x - r_j, u^2 and e along each axis
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int cc = centre_cell(pos3[d], s.inv_h[d]);
+        loc[d] = wrap1(cc, s.M[d]) - org[d];
+        const float u = sub_rn(pos3[d], mul_rn((float)(cc - n + lane), s.h[d]));
+        const float u2 = mul_rn(u, u);
+        ul[d] = u;
+        u2l[d] = u2;
+        el[d] = (lane < W) ? expf(mul_rn(-u2, s.inv_2s2)) : 0.f;
+      }
+      float ey[W], eyuy[W], uy2[W];
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        ey[k] = __shfl_sync(0xffffffffu, el[1], k);
+        eyuy[k] = ey[k] * __shfl_sync(0xffffffffu, ul[1], k);
+        uy2[k] = __shfl_sync(0xffffffffu, u2l[1], k);
+      }
+      const float amp = cA * a.w * tscale;
+      int* base = tile + loc[2] * G::PP + loc[1] * G::RP + loc[0];
+#pragma unroll
+      for (int pass = 0; pass < NPASS; pass++) {
+        const float ex = __shfl_sync(0xffffffffu, el[0], psx[pass]);
+        const float ux = __shfl_sync(0xffffffffu, ul[0], psx[pass]);
+        const float ux2 = __shfl_sync(0xffffffffu, u2l[0], psx[pass]);
+        const float ez = __shfl_sync(0xffffffffu, el[2], psz[pass]);
+        const float uz = __shfl_sync(0xffffffffu, ul[2], psz[pass]);
+        const float uz2 = __shfl_sync(0xffffffffu, u2l[2], psz[pass]);
+        if (pass * 32 + lane < W * W) {
+          const float w = amp * ex * ez;
+          const float t1 = w * (Gx * ux + Gz * uz), t2 = w * Gy;
+          const float rem = s.rcut2 - (ux2 + uz2);
+          int* cell = base + poff[pass];
+#pragma unroll
+          for (int k = 0; k < W; k++) {
+            if (uy2[k] < rem) {
+              // |t1 e_y + t2 e_y u_y| < 2^22: both roundings stay at unit spacing
+              const int v =
+                  __float_as_int(fmaf(t1, ey[k], fmaf(t2, eyuy[k], 12582912.0f))) - 0x4B400000;
+              atomicAdd(cell + k * G::RP, v);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  brick_flush<W, NT>(tile, b, x0, y0, z0, shift, grid64);
+}
+
+// Shared memory of the reverse-pass gather for stencil width W.
+template <int W>
+struct AdjGatherGeom {
+  static constexpr int n = (W - 1) / 2;
+  static constexpr int TX = kAX + 2 * n, TY = kAY + 2 * n, TZ = kAZ + 2 * n;
+  static constexpr int TP = TX | 1;
+  static constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
+  static constexpr int NW = kAdjThreads / 32;
+  static constexpr size_t bytes =
+      sizeof(float) * (2 * TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+};
+
+// Reverse-pass gather of the atoms of one kAX x kAY x kAZ brick: Psi = psi +
+// gE c h^3 phi and phi of the brick plus halo in shared memory; one warp per
+// atom: the cube rows of Psi (moments e, e u_x) and the sphere rows of phi
+// (moments e, e u_x, e u_x^2), combined into dL/dq and dL/dx.
+template <int W>
+__device__ __forceinline__ void adj_gather_brick(
+    const float4* __restrict__ sorted, const int* __restrict__ perm, const int* __restrict__ start,
+    const BinLayout& b, const Stencil<float>& sp, const Stencil<float>& sg, double c,
+    double gE_ch3, const float* __restrict__ psi, const float* __restrict__ phi,
+    const double* __restrict__ gfx, const double* __restrict__ gfy,
+    const double* __restrict__ gfz, double* __restrict__ dq, double* __restrict__ dx,
+    double* __restrict__ dy, double* __restrict__ dz, int bxi, int byi, int bzi,
+    unsigned char* smem) {
+  typedef AdjGatherGeom<W> AG;
+  constexpr int n = AG::n, TX = AG::TX, TY = AG::TY, TZ = AG::TZ, TP = AG::TP, ZP = AG::ZP;
+  constexpr int NW = AG::NW, NT = kAdjThreads;
+  constexpr int NR = kAY * kAZ;
+  constexpr int NG = (W * W + 31) / 32;
+  float* tpsi = (float*)smem;                     // [TZ][ZP]
+  float* tphi = tpsi + TZ * ZP;                   // [TZ][ZP]
+  float* tabs = tphi + TZ * ZP;                   // [NW][axis][u, u^2, e][kWPad]
+  int* rowl = (int*)(tabs + NW * 9 * kWPad);      // [NW][W*W]
+  __shared__ int rng_a[NR], rng_p[NR + 1];
+  __shared__ int alist[kGatherList];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = bxi * kAX, y0 = byi * kAY, z0 = bzi * kAZ;
+  const int ex = min(kAX, b.M[0] - x0), ey = min(kAY, b.M[1] - y0), ez = min(kAZ, b.M[2] - z0);
+  int cnt = 0;
+  if (tid < NR) {
+    const int yy = tid % kAY, zz = tid / kAY;
+    int a0 = 0, a1 = 0;
+    if (yy < ey && zz < ez) {
+      const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
+      a0 = start[rowkey + x0 / kBinX];
+      a1 = start[rowkey + (x0 + ex - 1) / kBinX + 1];
+    }
+    rng_a[tid] = a0;
+    cnt = a1 - a0;
+  }
+  int natoms;
+  const int pos = block_exclusive_scan(cnt, &natoms);
+  if (tid < NR) rng_p[tid] = pos;
+  if (tid == 0) rng_p[NR] = natoms;
+  if (natoms == 0) return;  // uniform
+  stage_tile_async<float, TX, TY, TZ, TP, ZP, NW>(psi, b, x0, y0, z0, n, tpsi);
+  stage_tile_async<float, TX, TY, TZ, TP, ZP, NW>(phi, b, x0, y0, z0, n, tphi);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  {
+    const float g = (float)gE_ch3;
+    for (int i = tid; i < TZ * ZP; i += NT) tpsi[i] = fmaf(g, tphi[i], tpsi[i]);
+  }
+  __syncthreads();
+
+  float* tb = tabs + warp * 9 * kWPad;
+  int* rl = rowl + warp * W * W;
+  int gjy[NG], gjz[NG];
+#pragma unroll
+  for (int g = 0; g < NG; g++) {
+    const int r = g * 32 + lane;
+    gjz[g] = r < W * W ? r / W : 0;
+    gjy[g] = r < W * W ? r - (r / W) * W : 0;
+  }
+  const double pref_sp = (double)sp.pref, inv_s2 = 2.0 * (double)sp.inv_2s2;
+  const double cA = c * (double)sg.pref;
+  for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
+    for (int r = tid; r < NR; r += NT) {
+      const int p0 = rng_p[r], p1 = rng_p[r + 1];
+      for (int p = max(p0, c0); p < min(p1, c0 + kGatherList); p++)
+        alist[p - c0] = rng_a[r] + (p - p0);
+    }
+    __syncthreads();
+    const int nc = min(kGatherList, natoms - c0);
+    for (int q = warp; q < nc; q += NW) {
+      const int ai = alist[q];
+      const float4 a = sorted[ai];
+      const float pos3[3] = {a.x, a.y, a.z};
+      const int org[3] = {x0, y0, z0};
+      int loc[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const int cc = centre_cell(pos3[d], sp.inv_h[d]);
+        loc[d] = wrap1(cc, sp.M[d]) - org[d];
+        if (lane < W) {
+          const float u = sub_rn(pos3[d], mul_rn((float)(cc - n + lane), sp.h[d]));
+          const float u2 = mul_rn(u, u);
+          tb[(d * 3 + 0) * kWPad + lane] = u;
+          tb[(d * 3 + 1) * kWPad + lane] = u2;
+          tb[(d * 3 + 2) * kWPad + lane] = expf(mul_rn(-u2, sp.inv_2s2));
+        }
+      }
+      __syncwarp();
+      unsigned long long w2[W];  // (e_x, e_x u_x) per x offset
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        const float e = tb[(0 * 3 + 2) * kWPad + k];
+        const float eu = e * tb[(0 * 3 + 0) * kWPad + k];
+        asm("mov.b64 %0, {%1, %2};" : "=l"(w2[k]) : "f"(e), "f"(eu));
+      }
+      // cube rows of Psi: P = sum e Psi, V = sum e Psi u
+      double P = 0.0, Vx = 0.0, Vy = 0.0, Vz = 0.0;
+#pragma unroll
+      for (int g = 0; g < NG; g++) {
+        if (g * 32 + lane < W * W) {
+          const int jy = gjy[g], jz = gjz[g];
+          const float* row = tpsi + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
+          unsigned long long acc = 0ull;
+#pragma unroll
+          for (int k = 0; k < W; k++) {
+            unsigned long long p2;
+            asm("mov.b64 %0, {%1, %1};" : "=l"(p2) : "f"(row[k]));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2[k]), "l"(p2));
+          }
+          float r0, r1;
+          asm("mov.b64 {%0, %1}, %2;" : "=f"(r0), "=f"(r1) : "l"(acc));
+          const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
+          const float a0 = w * r0;
+          P += (double)a0;
+          Vx += (double)(w * r1);
+          Vy += (double)(a0 * tb[(1 * 3 + 0) * kWPad + jy]);
+          Vz += (double)(a0 * tb[(2 * 3 + 0) * kWPad + jz]);
+        }
+      }
+      P = warp_sum(P);
+      Vx = warp_sum(Vx);
+      Vy = warp_sum(Vy);
+      Vz = warp_sum(Vz);
+      // sphere rows of phi
+      int nrow = 0;
+#pragma unroll
+      for (int g = 0; g < NG; g++) {
+        const int r = g * 32 + lane;
+        bool ne = false;
+        if (r < W * W)
+          ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) <
+               sg.rcut2;
+        const unsigned m = __ballot_sync(0xffffffffu, ne);
+        if (ne) rl[nrow + __popc(m & ((1u << lane) - 1u))] = (gjz[g] << 8) | gjy[g];
+        nrow += __popc(m);
+      }
+      __syncwarp();
+      float dx2[W], eu2[W];
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        dx2[k] = tb[(0 * 3 + 1) * kWPad + k];
+        eu2[k] = tb[(0 * 3 + 2) * kWPad + k] * dx2[k];
+      }
+      double T0 = 0, T1x = 0, T1y = 0, T1z = 0;
+      double Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
+      for (int i = lane; i < nrow; i += 32) {
+        const int r = rl[i];
+        const int jz = r >> 8, jy = r & 255;
+        const float uy2 = tb[(1 * 3 + 1) * kWPad + jy], uz2 = tb[(2 * 3 + 1) * kWPad + jz];
+        const float rem = sg.rcut2 - (uy2 + uz2);
+        const float* row = tphi + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
+        unsigned long long acc = 0ull;
+        float s2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+          const float ph = dx2[k] < rem ? row[k] : 0.f;
+          unsigned long long p2;
+          asm("mov.b64 %0, {%1, %1};" : "=l"(p2) : "f"(ph));
+          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2[k]), "l"(p2));
+          s2 = fmaf(eu2[k], ph, s2);
+        }
+        float s0, s1;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(acc));
+        const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
+        const float uy = tb[(1 * 3 + 0) * kWPad + jy], uz = tb[(2 * 3 + 0) * kWPad + jz];
+        const float a0 = w * s0, a1 = w * s1;
+        T0 += (double)a0;
+        T1x += (double)a1;
+        T1y += (double)(a0 * uy);
+        T1z += (double)(a0 * uz);
+        Mxx += (double)(w * s2);
+        Mxy += (double)(a1 * uy);
+        Mxz += (double)(a1 * uz);
+        Myy += (double)(a0 * uy2);
+        Myz += (double)(a0 * uy * uz);
+        Mzz += (double)(a0 * uz2);
+      }
+      T0 = warp_sum(T0);
+      T1x = warp_sum(T1x);
+      T1y = warp_sum(T1y);
+      T1z = warp_sum(T1z);
+      Mxx = warp_sum(Mxx);
+      Mxy = warp_sum(Mxy);
+      Mxz = warp_sum(Mxz);
+      Myy = warp_sum(Myy);
+      Myz = warp_sum(Myz);
+      Mzz = warp_sum(Mzz);
+      if (lane == 0) {
+        const int o = perm[ai];
+        const double q = (double)a.w;
+        const double Gx = gfx ? gfx[o] : 0.0, Gy = gfy ? gfy[o] : 0.0, Gz = gfz ? gfz[o] : 0.0;
+        const double T2x = Mxx * Gx + Mxy * Gy + Mxz * Gz;
+        const double T2y = Mxy * Gx + Myy * Gy + Myz * Gz;
+        const double T2z = Mxz * Gx + Myz * Gy + Mzz * Gz;
+        const double vs = -pref_sp * inv_s2;  // (r - x) = -u
+        dq[o] = pref_sp * P + cA * (Gx * T1x + Gy * T1y + Gz * T1z);
+        dx[o] = q * vs * Vx + cA * q * (Gx * T0 - T2x * inv_s2);
+        dy[o] = q * vs * Vy + cA * q * (Gy * T0 - T2y * inv_s2);
+        dz[o] = q * vs * Vz + cA * q * (Gz * T0 - T2z * inv_s2);
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(kScatterThreads)
+    k_adj_scatter(const float4* __restrict__ sorted, const int* __restrict__ perm,
+                  const int* __restrict__ start, BinLayout b, Stencil<float> s, float cA,
+                  const double* __restrict__ gfx, const double* __restrict__ gfy,
+                  const double* __restrict__ gfz, long long* __restrict__ grid64) {
+  extern __shared__ int atile[];
+  adj_scatter_brick<W>(sorted, perm, start, b, s, cA, gfx, gfy, gfz, blockIdx.x, blockIdx.y,
+                       blockIdx.z, atile, grid64);
+}
+
+template <int W>
+__global__ void __launch_bounds__(kAdjThreads, 2)
+    k_adj_gather_tiled(const float4* __restrict__ sorted, const int* __restrict__ perm,
+                       const int* __restrict__ start, BinLayout b, Stencil<float> sp,
+                       Stencil<float> sg, double c, double gE_ch3, const float* __restrict__ psi,
+                       const float* __restrict__ phi, const double* __restrict__ gfx,
+                       const double* __restrict__ gfy, const double* __restrict__ gfz,
+                       double* __restrict__ dq, double* __restrict__ dx, double* __restrict__ dy,
+                       double* __restrict__ dz) {
+  extern __shared__ __align__(16) unsigned char asm_[];
+  adj_gather_brick<W>(sorted, perm, start, b, sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx,
+                      dy, dz, blockIdx.x, blockIdx.y, blockIdx.z, asm_);
+}
+
+__global__ void __launch_bounds__(kScatterThreads)
+    k_batch_adj_scatter(const float4* __restrict__ sorted, const int* __restrict__ perm,
+                        const int* __restrict__ start, const BatchSys* __restrict__ sys,
+                        const BatchItem* __restrict__ items, int nitems, double c,
+                        const double* __restrict__ gfx, const double* __restrict__ gfy,
+                        const double* __restrict__ gfz, long long* __restrict__ grid64) {
+  extern __shared__ int atile[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const BatchItem item = items[it];
+    const BatchSys& S = sys[item.sys];
+    const float cA = (float)(c * (double)S.sg.pref);
+    const int* st = start + S.bin_off;
+    long long* out = grid64 + S.grid_off;
+    switch (S.W) {
+      case 9: adj_scatter_brick<9>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
+      case 11: adj_scatter_brick<11>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
+      case 13: adj_scatter_brick<13>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
+      case 15: adj_scatter_brick<15>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kAdjThreads, 2)
+    k_batch_adj_gather_tiled(const float4* __restrict__ sorted, const int* __restrict__ perm,
+                             const int* __restrict__ start, const BatchSys* __restrict__ sys,
+                             const BatchItem* __restrict__ items, int nitems, double c,
+                             const double* __restrict__ dLdE, const float* __restrict__ psi,
+                             const float* __restrict__ phi, const double* __restrict__ gfx,
+                             const double* __restrict__ gfy, const double* __restrict__ gfz,
+                             double* __restrict__ dq, double* __restrict__ dx,
+                             double* __restrict__ dy, double* __restrict__ dz) {
+  extern __shared__ __align__(16) unsigned char asm_[];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const BatchItem item = items[it];
+    const BatchSys& S = sys[item.sys];
+    const double gE_ch3 = dLdE[item.sys] * c * S.h3;
+    const int* st = start + S.bin_off;
+    const float* ps = psi + S.grid_off;
+    const float* ph = phi + S.grid_off;
+    switch (S.W) {
+      case 9: adj_gather_brick<9>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
+      case 11: adj_gather_brick<11>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
+      case 13: adj_gather_brick<13>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
+      case 15: adj_gather_brick<15>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
+    }
+    __syncthreads();
+  }
+}
+
+namespace {
+template <class K>
+cudaError_t set_smem_once(K kernel, size_t bytes, bool* done) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (done[dev]) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[dev] = true;
+  return e;
+}
+
+template <int W>
+cudaError_t adj_scatter_w(const float4* sorted, const int* perm, const int* start,
+                          const BinLayout& b, const Stencil<float>& s, double c, const double* gfx,
+                          const double* gfy, const double* gfz, long long* grid64, float* lambda,
+                          cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = sizeof(int) * ScatterGeom<W>::words;
+  cudaError_t e = set_smem_once(k_adj_scatter<W>, smem, done);
+  if (e != cudaSuccess) return e;
+  const long long size = (long long)b.M[0] * b.M[1] * b.M[2];
+  e = cudaMemsetAsync(grid64, 0, sizeof(long long) * size, st);
+  if (e != cudaSuccess) return e;
+  const dim3 grd((b.M[0] + kSB - 1) / kSB, (b.M[1] + kSB - 1) / kSB, (b.M[2] + kSB - 1) / kSB);
+  k_adj_scatter<W><<<grd, kScatterThreads, smem, st>>>(sorted, perm, start, b, s,
+                                                       (float)(c * (double)s.pref), gfx, gfy, gfz,
+                                                       grid64);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_grid64_to_real(grid64, size, lambda, st);
+}
+
+template <int W>
+cudaError_t adj_gather_w(const float4* sorted, const int* perm, const int* start,
+                         const BinLayout& b, const Stencil<float>& sp, const Stencil<float>& sg,
+                         double c, double gE_ch3, const float* psi, const float* phi,
+                         const double* gfx, const double* gfy, const double* gfz, double* dq,
+                         double* dx, double* dy, double* dz, cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = AdjGatherGeom<W>::bytes;
+  const cudaError_t e = set_smem_once(k_adj_gather_tiled<W>, smem, done);
+  if (e != cudaSuccess) return e;
+  const dim3 grd((b.M[0] + kAX - 1) / kAX, (b.M[1] + kAY - 1) / kAY, (b.M[2] + kAZ - 1) / kAZ);
+  k_adj_gather_tiled<W><<<grd, kAdjThreads, smem, st>>>(sorted, perm, start, b, sp, sg, c, gE_ch3,
+                                                        psi, phi, gfx, gfy, gfz, dq, dx, dy, dz);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_adj_scatter(const float4* sorted, const int* perm, const int* start,
+                               const BinLayout& b, const Stencil<float>& sg, double c,
+                               const double* gfx, const double* gfy, const double* gfz,
+                               long long* grid64, float* lambda, cudaStream_t st) {
+  switch (2 * sg.nst[0] + 1) {
+    case 9: return adj_scatter_w<9>(sorted, perm, start, b, sg, c, gfx, gfy, gfz, grid64, lambda, st);
+    case 11: return adj_scatter_w<11>(sorted, perm, start, b, sg, c, gfx, gfy, gfz, grid64, lambda, st);
+    case 13: return adj_scatter_w<13>(sorted, perm, start, b, sg, c, gfx, gfy, gfz, grid64, lambda, st);
+    case 15: return adj_scatter_w<15>(sorted, perm, start, b, sg, c, gfx, gfy, gfz, grid64, lambda, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
+                                    const BinLayout& b, const Stencil<float>& sp,
+                                    const Stencil<float>& sg, double c, double gE_ch3,
+                                    const float* psi, const float* phi, const double* gfx,
+                                    const double* gfy, const double* gfz, double* dq, double* dx,
+                                    double* dy, double* dz, cudaStream_t st) {
+  switch (2 * sp.nst[0] + 1) {
+    case 9: return adj_gather_w<9>(sorted, perm, start, b, sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz, st);
+    case 11: return adj_gather_w<11>(sorted, perm, start, b, sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz, st);
+    case 13: return adj_gather_w<13>(sorted, perm, start, b, sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz, st);
+    case 15: return adj_gather_w<15>(sorted, perm, start, b, sp, sg, c, gE_ch3, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+size_t adj_gather_smem(int W) {
+  switch (W) {
+    case 9: return AdjGatherGeom<9>::bytes;
+    case 11: return AdjGatherGeom<11>::bytes;
+    case 13: return AdjGatherGeom<13>::bytes;
+    default: return AdjGatherGeom<15>::bytes;
+  }
+}
+
+cudaError_t launch_batch_adj_scatter(const float4* sorted, const int* perm, const int* start,
+                                     const BatchSys* sys, const BatchItem* items, int nitems,
+                                     int ctas, double c, const double* gfx, const double* gfy,
+                                     const double* gfz, long long* grid64, long long gsize,
+                                     float* lambda, cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = sizeof(int) * ScatterGeom<15>::words;
+  cudaError_t e = set_smem_once(k_batch_adj_scatter, smem, done);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(grid64, 0, sizeof(long long) * gsize, st);
+  if (e != cudaSuccess) return e;
+  if (nitems > 0)
+    k_batch_adj_scatter<<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(
+        sorted, perm, start, sys, items, nitems, c, gfx, gfy, gfz, grid64);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_grid64_to_real(grid64, gsize, lambda, st);
+}
+
+cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
+                                          const BatchSys* sys, const BatchItem* items, int nitems,
+                                          int ctas, double c, const double* dLdE, const float* psi,
+                                          const float* phi, const double* gfx, const double* gfy,
+                                          const double* gfz, double* dq, double* dx, double* dy,
+                                          double* dz, int max_w, cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = adj_gather_smem(max_w);
+  const cudaError_t e = set_smem_once(k_batch_adj_gather_tiled, adj_gather_smem(15), done);
+  if (e != cudaSuccess) return e;
+  if (nitems > 0)
+    k_batch_adj_gather_tiled<<<std::min(ctas, nitems), kAdjThreads, smem, st>>>(
+        sorted, perm, start, sys, items, nitems, c, dLdE, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int ntot,

@@ -19,6 +19,33 @@ cudaError_t launch_batch_adj_gather(const float4* xyzq, const int* perm, int nto
                                     double* dq, double* dx, double* dy, double* dz,
                                     cudaStream_t st);
 
+// Tiled reverse pass of the mixed form (sorted atoms and bin starts as the
+// forward pass leaves them).  The source lambda is accumulated in `grid64`
+// (cleared here) and written as floats into `lambda`.
+cudaError_t launch_adj_scatter(const float4* sorted, const int* perm, const int* start,
+                               const BinLayout& b, const Stencil<float>& sg, double c,
+                               const double* gfx, const double* gfy, const double* gfz,
+                               long long* grid64, float* lambda, cudaStream_t st);
+cudaError_t launch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
+                                    const BinLayout& b, const Stencil<float>& sp,
+                                    const Stencil<float>& sg, double c, double gE_ch3,
+                                    const float* psi, const float* phi, const double* gfx,
+                                    const double* gfy, const double* gfz, double* dq, double* dx,
+                                    double* dy, double* dz, cudaStream_t st);
+cudaError_t launch_batch_adj_scatter(const float4* sorted, const int* perm, const int* start,
+                                     const BatchSys* sys, const BatchItem* items, int nitems,
+                                     int ctas, double c, const double* gfx, const double* gfy,
+                                     const double* gfz, long long* grid64, long long gsize,
+                                     float* lambda, cudaStream_t st);
+cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
+                                          const BatchSys* sys, const BatchItem* items, int nitems,
+                                          int ctas, double c, const double* dLdE, const float* psi,
+                                          const float* phi, const double* gfx, const double* gfy,
+                                          const double* gfz, double* dq, double* dx, double* dy,
+                                          double* dz, int max_w, cudaStream_t st);
+// Shared memory of the reverse-pass gather block for stencil width W.
+size_t adj_gather_smem(int W);
+
 template <typename CT>
 cudaError_t launch_adj_source(const typename Vec4<CT>::type* xyzq, const int* perm, int n,
                               const Stencil<CT>& s, double c, const double* gfx,

@@ -975,6 +975,15 @@ gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
   c->phi_valid = true;
   c->energy_valid = true;
   // adjoint source lambda into the rho buffer, then psi = K lambda in place
+  const bool tiled_mixed =
+      !c->fp64 && tiled_ok<float>(c, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, true, false));
+  if (tiled_mixed) {
+    const Stencil<float> sg = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, true, false);
+    c->launches += 2;
+    CU(launch_adj_scatter((const float4*)c->d_sorted, c->d_perm, c->d_bstart, c->bl, sg,
+                          c->p.ccelec, gd[0], gd[1], gd[2], c->d_fixed, (float*)c->d_rho,
+                          c->stream));
+  } else {
   CU(cudaMemsetAsync(c->d_rho, 0, c->size * c->ct, c->stream));
   c->launches += 3;
   if (c->fp64) {
@@ -986,6 +995,7 @@ gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
     CU(launch_adj_source<float>((const float4*)c->d_sorted, c->d_perm, n, sg, c->p.ccelec, gd[0],
                                 gd[1], gd[2], (float*)c->d_rho, c->stream));
   }
+  }
   TRY(do_solve(c, c->d_rho, c->d_rho, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, false));
   c->rho_valid = false;
   const bool dev_out = is_device_ptr(dq) && is_device_ptr(dx) && is_device_ptr(dy) &&
@@ -996,7 +1006,15 @@ gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
   } else {
     for (int k = 0; k < 4; k++) od[k] = o + k * cap;
   }
-  if (c->fp64) {
+  if (tiled_mixed) {
+    const Stencil<float> sp = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false);
+    const Stencil<float> sg = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, true, false);
+    c->launches += 1;
+    CU(launch_adj_gather_tiled((const float4*)c->d_sorted, c->d_perm, c->d_bstart, c->bl, sp, sg,
+                               c->p.ccelec, gE_ch3, (const float*)c->d_rho,
+                               (const float*)c->d_phi, gd[0], gd[1], gd[2], od[0], od[1], od[2],
+                               od[3], c->stream));
+  } else if (c->fp64) {
     const Stencil<double> sp = stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false);
     const Stencil<double> sg = stencil_of<double>(c, box.v, c->sigma1, c->rcut1, true, false);
     CU(launch_adj_gather<double>((const double4*)c->d_sorted, c->d_perm, n, sp, sg, c->p.ccelec,

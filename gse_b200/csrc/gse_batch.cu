@@ -51,7 +51,8 @@ struct gse_batch {
   std::vector<BatchSys> sys;
   std::vector<int> first;
   std::vector<SizeClass> cls;
-  std::vector<BatchItem> scat, gath;
+  std::vector<BatchItem> scat, gath, agath;  // spread, gather, reverse-pass gather bricks
+  int max_w = 0;
   int nbins = 0;
   long long gtot = 0, ktot = 0;
   // device
@@ -61,6 +62,7 @@ struct gse_batch {
   int* d_ksys = nullptr;
   BatchItem* d_scat = nullptr;
   BatchItem* d_gath = nullptr;
+  BatchItem* d_agath = nullptr;
   float4* d_xyzq = nullptr;
   float4* d_sorted = nullptr;
   int* d_perm = nullptr;
@@ -81,7 +83,7 @@ struct gse_batch {
   double* d_dLdE = nullptr;    // nsys
   double* d_gin = nullptr;     // 3 x ntot
   double* d_gout = nullptr;    // 4 x ntot
-  int scat_ctas = 0, gath_ctas = 0;
+  int scat_ctas = 0, gath_ctas = 0, agath_ctas = 0;
   bool largest_first = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -133,7 +135,7 @@ void order_items(gse_batch_t* b, bool largest_first) {
       return nx > ny;
     });
   };
-  std::vector<BatchItem> s, g;
+  std::vector<BatchItem> s, g, ag;
   for (int k = 0; k < b->nsys; k++) {
     const BatchSys& S = b->sys[k];
     const int ns[3] = {(S.b.M[0] + kSB - 1) / kSB, (S.b.M[1] + kSB - 1) / kSB,
@@ -146,13 +148,20 @@ void order_items(gse_batch_t* b, bool largest_first) {
     for (int z = 0; z < ng[2]; z++)
       for (int y = 0; y < ng[1]; y++)
         for (int x = 0; x < ng[0]; x++) g.push_back({k, x, y, z});
+    const int na[3] = {(S.b.M[0] + kAX - 1) / kAX, (S.b.M[1] + kAY - 1) / kAY,
+                       (S.b.M[2] + kAZ - 1) / kAZ};
+    for (int z = 0; z < na[2]; z++)
+      for (int y = 0; y < na[1]; y++)
+        for (int x = 0; x < na[0]; x++) ag.push_back({k, x, y, z});
   }
   if (largest_first) {
     by_work(s);
     by_work(g);
+    by_work(ag);
   }
   b->scat = s;
   b->gath = g;
+  b->agath = ag;
   b->largest_first = largest_first;
 }
 
@@ -160,6 +169,8 @@ gse_status_t upload_items(gse_batch_t* b) {
   BCU(cudaMemcpy(b->d_scat, b->scat.data(), sizeof(BatchItem) * b->scat.size(),
                  cudaMemcpyHostToDevice));
   BCU(cudaMemcpy(b->d_gath, b->gath.data(), sizeof(BatchItem) * b->gath.size(),
+                 cudaMemcpyHostToDevice));
+  BCU(cudaMemcpy(b->d_agath, b->agath.data(), sizeof(BatchItem) * b->agath.size(),
                  cudaMemcpyHostToDevice));
   return GSE_OK;
 }
@@ -189,20 +200,20 @@ gse_status_t run_forward(gse_batch_t* b) {
 gse_status_t run_adjoint(gse_batch_t* b) {
   cudaStream_t st = b->stream;
   const long long nt = b->ntot;
-  BCU(cudaMemsetAsync(b->d_lam, 0, sizeof(float) * b->gtot, st));
-  BCU(launch_batch_adj_source(b->d_sorted, b->d_perm, b->ntot, b->d_sys, b->d_first, b->nsys,
-                              b->p.ccelec, b->d_gin, b->d_gin + nt, b->d_gin + 2 * nt, b->d_lam,
-                              st));
+  BCU(launch_batch_adj_scatter(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_scat,
+                               (int)b->scat.size(), b->scat_ctas, b->p.ccelec, b->d_gin,
+                               b->d_gin + nt, b->d_gin + 2 * nt, b->d_g64, b->gtot, b->d_lam, st));
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecR2C(c.pf, (cufftReal*)(b->d_lam + c.goff), (cufftComplex*)(b->d_rhok + c.koff)));
   BCU(launch_batch_green(b->d_rhok, b->d_gtab, b->ktot, b->d_sys, b->d_kfirst, b->d_ksys, b->nsys,
                          nullptr, st));
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecC2R(c.pb, (cufftComplex*)(b->d_rhok + c.koff), (cufftReal*)(b->d_lam + c.goff)));
-  BCU(launch_batch_adj_gather(b->d_sorted, b->d_perm, b->ntot, b->d_sys, b->d_first, b->nsys,
-                              b->p.ccelec, b->d_dLdE, b->d_lam, b->d_phi, b->d_gin,
-                              b->d_gin + nt, b->d_gin + 2 * nt, b->d_gout, b->d_gout + nt,
-                              b->d_gout + 2 * nt, b->d_gout + 3 * nt, st));
+  BCU(launch_batch_adj_gather_tiled(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_agath,
+                                    (int)b->agath.size(), b->agath_ctas, b->p.ccelec, b->d_dLdE,
+                                    b->d_lam, b->d_phi, b->d_gin, b->d_gin + nt,
+                                    b->d_gin + 2 * nt, b->d_gout, b->d_gout + nt,
+                                    b->d_gout + 2 * nt, b->d_gout + 3 * nt, b->max_w, st));
   return GSE_OK;
 }
 
@@ -296,6 +307,7 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
       return set_error(GSE_ERR_UNSUPPORTED, "stencil width must be 9, 11, 13 or 15 on every axis");
     }
     S.W = 2 * S.sp.nst[0] + 1;
+    b->max_w = std::max(b->max_w, S.W);
     const double h3 = (box[0] / M[0]) * (box[1] / M[1]) * (box[2] / M[2]);
     S.h3 = h3;
     S.efac = 0.5 * common->ccelec * h3;
@@ -405,11 +417,13 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
   }
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
-  b->scat_ctas = sms;
+  b->scat_ctas = 2 * sms;
   b->gath_ctas = 2 * sms;
+  b->agath_ctas = 2 * sms;
   order_items(b, true);
   BCUC(cudaMalloc(&b->d_scat, sizeof(BatchItem) * std::max<size_t>(b->scat.size(), 1)));
   BCUC(cudaMalloc(&b->d_gath, sizeof(BatchItem) * std::max<size_t>(b->gath.size(), 1)));
+  BCUC(cudaMalloc(&b->d_agath, sizeof(BatchItem) * std::max<size_t>(b->agath.size(), 1)));
   if (upload_items(b) != GSE_OK) return bail(GSE_ERR_CUDA);
   BCUC(cudaDeviceSynchronize());
 #undef BCUC
@@ -426,7 +440,7 @@ gse_status_t gse_batch_destroy(gse_batch_t* b) {
     if (c.pf) cufftDestroy(c.pf);
     if (c.pb) cufftDestroy(c.pb);
   }
-  void* ptrs[] = {b->d_sys, b->d_first, b->d_kfirst, b->d_ksys, b->d_scat, b->d_gath,
+  void* ptrs[] = {b->d_sys, b->d_first, b->d_kfirst, b->d_ksys, b->d_scat, b->d_gath, b->d_agath,
                   b->d_xyzq, b->d_sorted, b->d_perm, b->d_key, b->d_tmp, b->d_counts,
                   b->d_start, b->d_tiles, b->d_qmax, b->d_g64, b->d_rho, b->d_phi, b->d_lam,
                   b->d_rhok, b->d_gtab, b->d_energy, b->d_dLdE, b->d_forces, b->d_gin,

@@ -17,17 +17,13 @@
 //            atom, lanes over the non-empty (y, z) rows of its sphere.
 #include "gse_internal.cuh"
 #include "gse_tiled.cuh"
+#include "gse_tiled_dev.cuh"
 
 namespace gse {
 
 // ===========================================================================
 // Binning
 // ===========================================================================
-template <typename CT>
-__device__ __forceinline__ int centre_cell(CT v, CT inv_h) {
-  return round_to_int(mul_rn(v, inv_h));
-}
-
 template <typename CT>
 __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, int n, BinLayout b,
                             CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
@@ -53,34 +49,6 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
 constexpr int kScanPer = 4;
 constexpr int kScanThreads = 1024;
 constexpr int kScanTile = kScanPer * kScanThreads;
-
-__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
-  __shared__ int ws[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) ws[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    const int nw = blockDim.x >> 5;
-    int s = (lane < nw) ? ws[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    ws[lane] = s;
-  }
-  __syncthreads();
-  const int before = (w > 0 ? ws[w - 1] : 0) + x - v;
-  if (total) *total = ws[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return before;
-}
 
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_tiles(const int* __restrict__ counts, int nb, int* __restrict__ start,
@@ -440,88 +408,26 @@ __global__ void __launch_bounds__(kSpreadThreads)
 // reductions; integer sums do not depend on their order, so the grid is the
 // same bit for bit on every run.
 template <int W>
-struct ScatterGeom {
-  static constexpr int n = (W - 1) / 2;
-  static constexpr int T = kSB + 2 * n;
-  static constexpr int RP = T;                              // y pitch
-  static constexpr int PP = ((T * T + 31) / 32) * 32 + W;   // z pitch, = W (mod 32)
-  static constexpr int words = T * PP;
-};
-
-constexpr int kFlushBits = 40;
-constexpr int kMinShift = 11;  // 2^30 * 2^(40-11) * 8 overlapping tiles < 2^63
-
-template <int W>
 __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
                                               const int* __restrict__ start, const BinLayout& b,
                                               const Stencil<float>& s, int bxi, int byi, int bzi,
                                               int* __restrict__ tile,
                                               long long* __restrict__ grid64) {
   typedef ScatterGeom<W> G;
-  constexpr int n = G::n, T = G::T;
+  constexpr int n = G::n;
   constexpr int NT = kScatterThreads, NW = NT / 32;
   constexpr int NPASS = (W * W + 31) / 32;
   __shared__ int rng_a[kSB * kSB], rng_p[kSB * kSB];
   __shared__ int alist[kScatterList];
-  __shared__ float qsum_w[NW], qmax_w[NW];
-  __shared__ int s_shift;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int x0 = bxi * kSB, y0 = byi * kSB, z0 = bzi * kSB;
-  const int ex = min(kSB, b.M[0] - x0), ey = min(kSB, b.M[1] - y0), ez = min(kSB, b.M[2] - z0);
-
-  // the brick's atoms: one range per (y, z) cell row
-  int cnt = 0, a0 = 0;
-  if (tid < kSB * kSB) {
-    const int yy = tid % kSB, zz = tid / kSB;
-    if (yy < ey && zz < ez) {
-      const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
-      a0 = start[rowkey + x0 / kBinX];
-      cnt = start[rowkey + (x0 + ex - 1) / kBinX + 1] - a0;
-    }
-  }
+  const float apref = fabsf(s.pref);
   int total;
-  const int pos = block_exclusive_scan(cnt, &total);
-  if (tid < kSB * kSB) {
-    rng_a[tid] = a0;
-    rng_p[tid] = pos;
-  }
-  for (int i = tid; i < G::words / 4; i += NT)
-    reinterpret_cast<int4*>(tile)[i] = make_int4(0, 0, 0, 0);
-  for (int i = (G::words / 4) * 4 + tid; i < G::words; i += NT) tile[i] = 0;
-  // fixed-point scale of this brick: every contribution below 2^22 and every
-  // partial sum below 2^30
-  float qs = 0.f, qm = 0.f;
-  for (int j = 0; j < cnt; j++) {
-    const float q = fabsf(sorted[a0 + j].w);
-    qs += q;
-    qm = fmaxf(qm, q);
-  }
-  qs = warp_sum(qs);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
-  if (lane == 0) {
-    qsum_w[warp] = qs;
-    qmax_w[warp] = qm;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    float q = 0.f, m = 0.f;
-    for (int w = 0; w < NW; w++) {
-      q += qsum_w[w];
-      m = fmaxf(m, qmax_w[w]);
-    }
-    const double pref = fabs((double)s.pref);
-    const double sum_b = (double)q * pref * 1.0001 + 1e-30;
-    const double one_b = (double)m * pref * 1.0001 + 1e-30;
-    int sh = kFlushBits;
-    while (sh > kMinShift && (sum_b * exp2((double)sh) >= 1073741824.0 ||
-                              one_b * exp2((double)sh) >= 4194304.0))
-      sh--;
-    s_shift = sh;
-  }
-  __syncthreads();
-  const float tscale = exp2f((float)s_shift);
+  const int shift = brick_prologue<W, NT>(
+      start, b, x0, y0, z0, tile, rng_a, rng_p,
+      [&](int i) { return fabsf(sorted[i].w) * apref; }, &total);
+  const float tscale = exp2f((float)shift);
 
   // per-lane (x, z) pair of each pass and its tile offset: the same for all atoms
   int poff[NPASS], psx[NPASS], psz[NPASS];
@@ -535,13 +441,7 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
   }
 
   for (int c0 = 0; c0 < total; c0 += kScatterList) {
-    // flat list of this chunk's atoms
-    for (int r = tid; r < kSB * kSB; r += NT) {
-      const int p0 = rng_p[r];
-      const int p1 = (r + 1 < kSB * kSB) ? rng_p[r + 1] : total;
-      for (int p = max(p0, c0); p < min(p1, c0 + kScatterList); p++)
-        alist[p - c0] = rng_a[r] + (p - p0);
-    }
+    brick_atom_list<NT, kSB * kSB>(rng_a, rng_p, total, c0, kScatterList, alist);
     __syncthreads();
     const int nc = min(kScatterList, total - c0);
     for (int q = warp; q < nc; q += NW) {
@@ -580,21 +480,7 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
     }
     __syncthreads();
   }
-  {
-    // tile -> int64 grid at 2^kFlushBits
-    const long long mul = 1LL << (kFlushBits - s_shift);
-    for (int i = tid; i < T * T * T; i += NT) {
-      const int zz = i / (T * T), r = i - zz * T * T, yy = r / T, xx = r - yy * T;
-      const int v = tile[zz * G::PP + r];
-      if (v != 0) {
-        const int gx = wrap1(x0 - n + xx, b.M[0]), gy = wrap1(y0 - n + yy, b.M[1]),
-                  gz = wrap1(z0 - n + zz, b.M[2]);
-        atomicAdd((unsigned long long*)(grid64 + gx +
-                                        ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
-                  (unsigned long long)((long long)v * mul));
-      }
-    }
-  }
+  brick_flush<W, NT>(tile, b, x0, y0, z0, shift, grid64);
 }
 
 template <int W>
@@ -712,24 +598,9 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   if (tid == 0) rng_p[NR] = natoms;
   if (natoms == 0) return;  // uniform: natoms is the same in every thread
 
-  // potential of the brick plus halo, one (y, z) row per warp iteration, as
-  // asynchronous element copies (cp.async) so that a warp keeps all of its
-  // rows in flight instead of waiting for each load
-  static_assert(TX <= 32, "one lane per tile column");
-  const long long zs = (long long)b.M[0] * b.M[1];
-  const int gx = lane < TX ? wrap1(x0 - n + lane, b.M[0]) : 0;
-  for (int r = warp; r < TY * TZ; r += NW) {
-    const int ty = r % TY, tz = r / TY;
-    const int gy = wrap1(y0 - n + ty, b.M[1]);
-    const int gz = wrap1(z0 - n + tz, b.M[2]);
-    const CT* src = phi + (long long)gy * b.M[0] + gz * zs + gx;
-    if (lane < TX) {
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tz * ZP + ty * TP + lane);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src),
-                   "n"(sizeof(CT))
-                   : "memory");
-    }
-  }
+  // potential of the brick plus halo, staged by asynchronous element copies
+  // so that a warp keeps all of its rows in flight
+  stage_tile_async<CT, TX, TY, TZ, TP, ZP, NW>(phi, b, x0, y0, z0, n, tile);
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
@@ -945,6 +816,12 @@ cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int
     case 15: return gather_w<CT, 15>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float* out,
+                                  cudaStream_t st) {
+  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, out);
+  return cudaGetLastError();
 }
 
 template <int W>

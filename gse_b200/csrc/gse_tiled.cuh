@@ -24,6 +24,8 @@ constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
 constexpr int kScatterThreads = 512;  // >= kSB * kSB
 constexpr int kScatterList = 1024;  // atoms per scatter round (per brick)
 constexpr int kGatherList = 512;    // atoms per gather round (per brick)
+constexpr int kAX = 16, kAY = 8, kAZ = 8;  // reverse-pass gather brick (two staged grids)
+constexpr int kAdjThreads = 256;           // >= kAY * kAZ
 
 // Atoms sorted by key (z cell, y cell, x bin); start[k] .. start[k+1] is bin k.
 struct BinLayout {
@@ -100,6 +102,10 @@ cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int
                                 const BatchSys* sys, const BatchItem* items, int nitems, int ctas,
                                 const float* phi, double outscale, double* fx, double* fy,
                                 double* fz, cudaStream_t st);
+
+// float grid = int64 accumulation grid at 2^40 (the scatter kernels' output)
+cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float* out,
+                                  cudaStream_t st);
 
 // Mixed-form spread: brick tiles added into the int64 grid `grid64` (cleared
 // here) at 2^40, then converted into the float grid `rho`.

@@ -1,0 +1,192 @@
+// gse_tiled_dev.cuh -- device helpers shared by the tiled forward kernels
+// (gse_tiled.cu) and the tiled reverse-pass kernels (gse_adjoint.cu).
+#pragma once
+
+#include "gse_internal.cuh"
+#include "gse_tiled.cuh"
+
+namespace gse {
+
+// Grid cell nearest to a coordinate (the stencil centre), not yet wrapped.
+template <typename CT>
+__device__ __forceinline__ int centre_cell(CT v, CT inv_h) {
+  return round_to_int(mul_rn(v, inv_h));
+}
+
+// Exclusive prefix sum of one int per thread over the whole block; *total
+// receives the block's sum.  All threads of the block must call it.
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int ws[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    int s = (lane < nw) ? ws[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    ws[lane] = s;
+  }
+  __syncthreads();
+  const int before = (w > 0 ? ws[w - 1] : 0) + x - v;
+  if (total) *total = ws[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return before;
+}
+
+// ---------------------------------------------------------------------------
+// Brick tiles of the scatter kernels (forward spread and adjoint source).
+// ---------------------------------------------------------------------------
+// Shared int32 tile of one kSB^3 brick plus its n-point halo, T points per
+// axis; the z-plane pitch is congruent to 2n+1 mod 32 so that the 32 lanes of
+// one instruction (consecutive (x, z) pairs of a stencil plane) hit 32
+// different banks.
+template <int W>
+struct ScatterGeom {
+  static constexpr int n = (W - 1) / 2;
+  static constexpr int T = kSB + 2 * n;
+  static constexpr int RP = T;                              // y pitch
+  static constexpr int PP = ((T * T + 31) / 32) * 32 + W;   // z pitch, = W (mod 32)
+  static constexpr int words = T * PP;
+};
+
+constexpr int kFlushBits = 40;  // scale of the int64 accumulation grids
+constexpr int kMinShift = 11;   // 2^30 * 2^(40-11) * 8 overlapping tiles < 2^63
+
+// Block prologue of a scatter brick: the brick's atoms (one contiguous range
+// per (y, z) cell row, start offsets in rng_a, exclusive prefix in rng_p),
+// the cleared tile, and the brick's power-of-two scale 2^S such that the sum
+// of bound(i) over its atoms times 2^S stays below 2^30 and every single
+// bound(i) times 2^S below 2^22.  bound(i) is an upper bound of |contribution|
+// of sorted atom i to any one grid point.  Returns S; *total gets the atom
+// count.  All threads of the block must call it.
+template <int W, int NT, class Bound>
+__device__ __forceinline__ int brick_prologue(const int* __restrict__ start, const BinLayout& b,
+                                              int x0, int y0, int z0, int* __restrict__ tile,
+                                              int* rng_a, int* rng_p, Bound bound, int* total) {
+  typedef ScatterGeom<W> G;
+  constexpr int NW = NT / 32;
+  __shared__ float qsum_w[NW], qmax_w[NW];
+  __shared__ int s_shift;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ex = min(kSB, b.M[0] - x0), ey = min(kSB, b.M[1] - y0), ez = min(kSB, b.M[2] - z0);
+  int cnt = 0, a0 = 0;
+  if (tid < kSB * kSB) {
+    const int yy = tid % kSB, zz = tid / kSB;
+    if (yy < ey && zz < ez) {
+      const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
+      a0 = start[rowkey + x0 / kBinX];
+      cnt = start[rowkey + (x0 + ex - 1) / kBinX + 1] - a0;
+    }
+  }
+  const int pos = block_exclusive_scan(cnt, total);
+  if (tid < kSB * kSB) {
+    rng_a[tid] = a0;
+    rng_p[tid] = pos;
+  }
+  for (int i = tid; i < G::words / 4; i += NT)
+    reinterpret_cast<int4*>(tile)[i] = make_int4(0, 0, 0, 0);
+  for (int i = (G::words / 4) * 4 + tid; i < G::words; i += NT) tile[i] = 0;
+  float qs = 0.f, qm = 0.f;
+  for (int j = 0; j < cnt; j++) {
+    const float q = bound(a0 + j);
+    qs += q;
+    qm = fmaxf(qm, q);
+  }
+  qs = warp_sum(qs);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
+  if (lane == 0) {
+    qsum_w[warp] = qs;
+    qmax_w[warp] = qm;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double q = 0.0;
+    float m = 0.f;
+    for (int w = 0; w < NW; w++) {
+      q += (double)qsum_w[w];
+      m = fmaxf(m, qmax_w[w]);
+    }
+    const double sum_b = q * 1.0001 + 1e-30;
+    const double one_b = (double)m * 1.0001 + 1e-30;
+    int sh = kFlushBits;
+    while (sh > kMinShift && (sum_b * exp2((double)sh) >= 1073741824.0 ||
+                              one_b * exp2((double)sh) >= 4194304.0))
+      sh--;
+    s_shift = sh;
+  }
+  __syncthreads();
+  return s_shift;
+}
+
+// Flat list alist[0 .. min(chunk, total - c0)) of the brick's atoms c0, c0+1,
+// ... (block-wide; the caller synchronises before reading it).
+template <int NT, int NROWS>
+__device__ __forceinline__ void brick_atom_list(const int* rng_a, const int* rng_p, int total,
+                                                int c0, int chunk, int* alist) {
+  for (int r = threadIdx.x; r < NROWS; r += NT) {
+    const int p0 = rng_p[r];
+    const int p1 = (r + 1 < NROWS) ? rng_p[r + 1] : total;
+    for (int p = max(p0, c0); p < min(p1, c0 + chunk); p++) alist[p - c0] = rng_a[r] + (p - p0);
+  }
+}
+
+// Finished tile (values at 2^shift) -> int64 grid at 2^kFlushBits (shift <=
+// kFlushBits, so the scaling is exact) by integer reductions, which do not
+// depend on their order.
+template <int W, int NT>
+__device__ __forceinline__ void brick_flush(const int* __restrict__ tile, const BinLayout& b,
+                                            int x0, int y0, int z0, int shift,
+                                            long long* __restrict__ grid64) {
+  typedef ScatterGeom<W> G;
+  constexpr int n = G::n, T = G::T;
+  const long long mul = 1LL << (kFlushBits - shift);
+  for (int i = threadIdx.x; i < T * T * T; i += NT) {
+    const int zz = i / (T * T), r = i - zz * T * T, yy = r / T, xx = r - yy * T;
+    const int v = tile[zz * G::PP + r];
+    if (v != 0) {
+      const int gx = wrap1(x0 - n + xx, b.M[0]), gy = wrap1(y0 - n + yy, b.M[1]),
+                gz = wrap1(z0 - n + zz, b.M[2]);
+      atomicAdd((unsigned long long*)(grid64 + gx +
+                                      ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
+                (unsigned long long)((long long)v * mul));
+    }
+  }
+}
+
+// Stage the potential-like grid `src` for a brick at (x0, y0, z0) with an
+// n-point halo into the shared tile [TZ][ZP] (rows of pitch TP) by
+// asynchronous element copies; the caller waits (cp.async.wait_all) and
+// synchronises.
+template <typename CT, int TX, int TY, int TZ, int TP, int ZP, int NW>
+__device__ __forceinline__ void stage_tile_async(const CT* __restrict__ src, const BinLayout& b,
+                                                 int x0, int y0, int z0, int n, CT* tile) {
+  static_assert(TX <= 32, "one lane per tile column");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long zs = (long long)b.M[0] * b.M[1];
+  const int gx = lane < TX ? wrap1(x0 - n + lane, b.M[0]) : 0;
+  for (int r = warp; r < TY * TZ; r += NW) {
+    const int ty = r % TY, tz = r / TY;
+    const int gy = wrap1(y0 - n + ty, b.M[1]);
+    const int gz = wrap1(z0 - n + tz, b.M[2]);
+    const CT* s = src + (long long)gy * b.M[0] + gz * zs + gx;
+    if (lane < TX) {
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tz * ZP + ty * TP + lane);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(s),
+                   "n"(sizeof(CT))
+                   : "memory");
+    }
+  }
+}
+
+}  // namespace gse

@@ -152,10 +152,10 @@ def test_graph_with_adjoint_matches_eager(batch_case):
     b.launch()
     torch.cuda.synchronize()
     out = bufs["grad_out"].cpu().numpy()
-    # the reverse pass sums its source grid with FP32 atomics, whose order
-    # differs from run to run
-    assert rms(out[0], dq) <= 1e-6
-    assert rms(out[1:].T, dx) <= 1e-6
+    # the reverse pass accumulates its source grid in 64-bit fixed point, so
+    # it is as reproducible as the forward pass
+    assert np.array_equal(out[0], dq)
+    assert np.array_equal(out[1:].T, dx)
 
 
 def test_autotune_and_cache(batch_case, tmp_path):
