@@ -39,10 +39,19 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
     key[i] = k;
     atomicAdd(&counts[k], 1);
   }
+  if (!qmax_bits) return;  // uniform
+  // block maximum first: one atomic per block, not per warp, on the single
+  // address (same-address atomics serialise)
+  __shared__ float wmax[32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
-  // non-negative floats order like their bit patterns (NaN compares largest)
-  if ((threadIdx.x & 31) == 0) atomicMax(qmax_bits, __float_as_uint(qm));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = qm;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) qm = fmaxf(qm, wmax[w]);
+    // non-negative floats order like their bit patterns (NaN compares largest)
+    atomicMax(qmax_bits, __float_as_uint(qm));
+  }
 }
 
 // Three-phase exclusive scan of counts[0..nb) into start[0..nb].
@@ -103,6 +112,22 @@ __global__ void k_bin_place_any(int n, const int* __restrict__ key, const int* _
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int k = key[i];
     tmp[start[k] + atomicAdd(&fill[k], 1)] = i;
+  }
+}
+
+// Placement in any order within a bin (the mixed form's kernels do not
+// depend on the order of the atoms of a bin): counts[] counts down to zero.
+template <typename CT>
+__global__ void k_bin_place_direct(const typename Vec4<CT>::type* __restrict__ xyzq, int n,
+                                   const int* __restrict__ key, const int* __restrict__ start,
+                                   int* __restrict__ counts,
+                                   typename Vec4<CT>::type* __restrict__ sorted,
+                                   int* __restrict__ perm) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k = key[i];
+    const int slot = start[k] + atomicSub(&counts[k], 1) - 1;
+    sorted[slot] = xyzq[i];
+    perm[slot] = i;
   }
 }
 
@@ -715,16 +740,22 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
   if (ntiles > kScanTile) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(w.qmax_bits, 0, sizeof(unsigned), st);
-  if (e != cudaSuccess) return e;
+  // the largest |q| feeds the FP64 spread's range check only
+  unsigned* qmax = sizeof(CT) == 8 ? w.qmax_bits : nullptr;
+  if (qmax) {
+    e = cudaMemsetAsync(qmax, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+  }
   const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
-                                        w.qmax_bits);
+                                        qmax);
   return launch_bin_scan_place<CT>(xyzq, n, nb, w, sorted, perm, st);
 }
 
-// counts (filled) -> start offsets -> stable placement of the atoms.
+// counts (filled) -> start offsets -> placement of the atoms: stable (in
+// the original order within a bin) for the FP64 form, whose output-stationary
+// spread sums atoms in bin order; any order for the mixed form.
 template <typename CT>
 cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, int nb,
                                   BinScratch w, typename Vec4<CT>::type* sorted, int* perm,
@@ -737,10 +768,14 @@ cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, in
   k_scan_sums<<<1, kScanThreads, 0, st>>>(w.tile_sums, ntiles, w.start, nb);
   k_scan_add<<<(nb + 255) / 256, 256, 0, st>>>(w.start, nb, w.tile_sums);
   if (n > 0) {
-    e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
-    if (e != cudaSuccess) return e;
-    k_bin_place_any<<<gb, 256, 0, st>>>(n, w.key, w.start, w.counts, w.tmp);
-    k_bin_place_stable<CT><<<gb, 256, 0, st>>>(xyzq, n, w.key, w.start, w.tmp, sorted, perm);
+    if (sizeof(CT) == 4) {
+      k_bin_place_direct<CT><<<gb, 256, 0, st>>>(xyzq, n, w.key, w.start, w.counts, sorted, perm);
+    } else {
+      e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
+      if (e != cudaSuccess) return e;
+      k_bin_place_any<<<gb, 256, 0, st>>>(n, w.key, w.start, w.counts, w.tmp);
+      k_bin_place_stable<CT><<<gb, 256, 0, st>>>(xyzq, n, w.key, w.start, w.tmp, sorted, perm);
+    }
   }
   return cudaGetLastError();
 }
@@ -877,12 +912,9 @@ __device__ __forceinline__ int batch_sys_of(const int* __restrict__ first, int n
 
 __global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
                                   const BatchSys* __restrict__ sys, const int* __restrict__ first,
-                                  int nsys, int* __restrict__ key, int* __restrict__ counts,
-                                  unsigned* __restrict__ qmax_bits) {
-  float qm = 0.f;
+                                  int nsys, int* __restrict__ key, int* __restrict__ counts) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntot; i += gridDim.x * blockDim.x) {
     const float4 a = xyzq[i];
-    qm = fmaxf(qm, fabsf(a.w));
     const BatchSys& S = sys[batch_sys_of(first, nsys, i)];
     const int cx = wrap1(centre_cell(a.x, S.sp.inv_h[0]), S.b.M[0]);
     const int cy = wrap1(centre_cell(a.y, S.sp.inv_h[1]), S.b.M[1]);
@@ -891,9 +923,6 @@ __global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
     key[i] = k;
     atomicAdd(&counts[k], 1);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(0xffffffffu, qm, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(qmax_bits, __float_as_uint(qm));
 }
 
 __global__ void __launch_bounds__(kScatterThreads)
@@ -997,14 +1026,11 @@ size_t batch_gather_smem() {
 cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
                              int nsys, int nbins, BinScratch w, float4* sorted, int* perm,
                              cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nbins, st);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(w.qmax_bits, 0, sizeof(unsigned), st);
+  const cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nbins, st);
   if (e != cudaSuccess) return e;
   const int gb = (int)std::min<long long>(148 * 8, (ntot + 255) / 256 > 0 ? (ntot + 255) / 256 : 1);
   if (ntot > 0)
-    k_batch_bin_count<<<gb, 256, 0, st>>>(xyzq, ntot, sys, first, nsys, w.key, w.counts,
-                                          w.qmax_bits);
+    k_batch_bin_count<<<gb, 256, 0, st>>>(xyzq, ntot, sys, first, nsys, w.key, w.counts);
   return launch_bin_scan_place<float>(xyzq, ntot, nbins, w, sorted, perm, st);
 }
 

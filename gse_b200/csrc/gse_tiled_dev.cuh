@@ -75,7 +75,8 @@ __device__ __forceinline__ int brick_prologue(const int* __restrict__ start, con
                                               int* rng_a, int* rng_p, Bound bound, int* total) {
   typedef ScatterGeom<W> G;
   constexpr int NW = NT / 32;
-  __shared__ float qsum_w[NW], qmax_w[NW];
+  __shared__ double qsum_w[NW];
+  __shared__ float qmax_w[NW];
   __shared__ int s_shift;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ex = min(kSB, b.M[0] - x0), ey = min(kSB, b.M[1] - y0), ez = min(kSB, b.M[2] - z0);
@@ -96,10 +97,13 @@ __device__ __forceinline__ int brick_prologue(const int* __restrict__ start, con
   for (int i = tid; i < G::words / 4; i += NT)
     reinterpret_cast<int4*>(tile)[i] = make_int4(0, 0, 0, 0);
   for (int i = (G::words / 4) * 4 + tid; i < G::words; i += NT) tile[i] = 0;
-  float qs = 0.f, qm = 0.f;
+  // double sums of the float bounds: exact for any realistic spread of
+  // magnitudes, so the scale does not depend on the order of a bin's atoms
+  double qs = 0.0;
+  float qm = 0.f;
   for (int j = 0; j < cnt; j++) {
     const float q = bound(a0 + j);
-    qs += q;
+    qs += (double)q;
     qm = fmaxf(qm, q);
   }
   qs = warp_sum(qs);
@@ -114,7 +118,7 @@ __device__ __forceinline__ int brick_prologue(const int* __restrict__ start, con
     double q = 0.0;
     float m = 0.f;
     for (int w = 0; w < NW; w++) {
-      q += (double)qsum_w[w];
+      q += qsum_w[w];
       m = fmaxf(m, qmax_w[w]);
     }
     const double sum_b = q * 1.0001 + 1e-30;
