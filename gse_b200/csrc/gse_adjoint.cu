@@ -552,6 +552,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
                       dy, dz, blockIdx.x, blockIdx.y, blockIdx.z, asm_);
 }
 
+template <int W>
 __global__ void __launch_bounds__(kScatterThreads)
     k_batch_adj_scatter(const float4* __restrict__ sorted, const int* __restrict__ perm,
                         const int* __restrict__ start, const BatchSys* __restrict__ sys,
@@ -563,18 +564,13 @@ __global__ void __launch_bounds__(kScatterThreads)
     const BatchItem item = items[it];
     const BatchSys& S = sys[item.sys];
     const float cA = (float)(c * (double)S.sg.pref);
-    const int* st = start + S.bin_off;
-    long long* out = grid64 + S.grid_off;
-    switch (S.W) {
-      case 9: adj_scatter_brick<9>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
-      case 11: adj_scatter_brick<11>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
-      case 13: adj_scatter_brick<13>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
-      case 15: adj_scatter_brick<15>(sorted, perm, st, S.b, S.sg, cA, gfx, gfy, gfz, item.bx, item.by, item.bz, atile, out); break;
-    }
+    adj_scatter_brick<W>(sorted, perm, start + S.bin_off, S.b, S.sg, cA, gfx, gfy, gfz, item.bx,
+                         item.by, item.bz, atile, grid64 + S.grid_off);
     __syncthreads();
   }
 }
 
+template <int W>
 __global__ void __launch_bounds__(kAdjThreads, 2)
     k_batch_adj_gather_tiled(const float4* __restrict__ sorted, const int* __restrict__ perm,
                              const int* __restrict__ start, const BatchSys* __restrict__ sys,
@@ -589,15 +585,9 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     const BatchItem item = items[it];
     const BatchSys& S = sys[item.sys];
     const double gE_ch3 = dLdE[item.sys] * c * S.h3;
-    const int* st = start + S.bin_off;
-    const float* ps = psi + S.grid_off;
-    const float* ph = phi + S.grid_off;
-    switch (S.W) {
-      case 9: adj_gather_brick<9>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
-      case 11: adj_gather_brick<11>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
-      case 13: adj_gather_brick<13>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
-      case 15: adj_gather_brick<15>(sorted, perm, st, S.b, S.sp, S.sg, c, gE_ch3, ps, ph, gfx, gfy, gfz, dq, dx, dy, dz, item.bx, item.by, item.bz, asm_); break;
-    }
+    adj_gather_brick<W>(sorted, perm, start + S.bin_off, S.b, S.sp, S.sg, c, gE_ch3,
+                        psi + S.grid_off, phi + S.grid_off, gfx, gfy, gfz, dq, dx, dy, dz, item.bx,
+                        item.by, item.bz, asm_);
     __syncthreads();
   }
 }
@@ -681,48 +671,79 @@ cudaError_t launch_adj_gather_tiled(const float4* sorted, const int* perm, const
   return cudaErrorInvalidValue;
 }
 
-size_t adj_gather_smem(int W) {
-  switch (W) {
-    case 9: return AdjGatherGeom<9>::bytes;
-    case 11: return AdjGatherGeom<11>::bytes;
-    case 13: return AdjGatherGeom<13>::bytes;
-    default: return AdjGatherGeom<15>::bytes;
-  }
-}
-
 cudaError_t launch_batch_adj_scatter(const float4* sorted, const int* perm, const int* start,
-                                     const BatchSys* sys, const BatchItem* items, int nitems,
-                                     int ctas, double c, const double* gfx, const double* gfy,
-                                     const double* gfz, long long* grid64, long long gsize,
-                                     float* lambda, cudaStream_t st) {
-  static bool done[64] = {};
-  const size_t smem = sizeof(int) * ScatterGeom<15>::words;
-  cudaError_t e = set_smem_once(k_batch_adj_scatter, smem, done);
+                                     const BatchSys* sys, const BatchItem* items,
+                                     const BatchSeg* segs, int nseg, int ctas, double c,
+                                     const double* gfx, const double* gfy, const double* gfz,
+                                     long long* grid64, long long gsize, float* lambda,
+                                     cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(grid64, 0, sizeof(long long) * gsize, st);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(grid64, 0, sizeof(long long) * gsize, st);
-  if (e != cudaSuccess) return e;
-  if (nitems > 0)
-    k_batch_adj_scatter<<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(
-        sorted, perm, start, sys, items, nitems, c, gfx, gfy, gfz, grid64);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  for (int k = 0; k < nseg; k++) {
+    const BatchItem* it = items + segs[k].first;
+    const int cnt = std::min(ctas, segs[k].count), ni = segs[k].count;
+    if (ni <= 0) continue;
+#define GSE_BAS(WW)                                                                          \
+  case WW: {                                                                                 \
+    static bool done[64] = {};                                                               \
+    const size_t smem = sizeof(int) * ScatterGeom<WW>::words;                                \
+    e = set_smem_once(k_batch_adj_scatter<WW>, smem, done);                                  \
+    if (e == cudaSuccess)                                                                    \
+      k_batch_adj_scatter<WW><<<cnt, kScatterThreads, smem, st>>>(sorted, perm, start, sys,  \
+                                                                  it, ni, c, gfx, gfy, gfz,  \
+                                                                  grid64);                   \
+    break;                                                                                   \
+  }
+    switch (segs[k].W) {
+      GSE_BAS(9)
+      GSE_BAS(11)
+      GSE_BAS(13)
+      GSE_BAS(15)
+      default: e = cudaErrorInvalidValue;
+    }
+#undef GSE_BAS
+    if (e != cudaSuccess) return e;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   return launch_grid64_to_real(grid64, gsize, lambda, st);
 }
 
 cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
-                                          const BatchSys* sys, const BatchItem* items, int nitems,
-                                          int ctas, double c, const double* dLdE, const float* psi,
-                                          const float* phi, const double* gfx, const double* gfy,
-                                          const double* gfz, double* dq, double* dx, double* dy,
-                                          double* dz, int max_w, cudaStream_t st) {
-  static bool done[64] = {};
-  const size_t smem = adj_gather_smem(max_w);
-  const cudaError_t e = set_smem_once(k_batch_adj_gather_tiled, adj_gather_smem(15), done);
-  if (e != cudaSuccess) return e;
-  if (nitems > 0)
-    k_batch_adj_gather_tiled<<<std::min(ctas, nitems), kAdjThreads, smem, st>>>(
-        sorted, perm, start, sys, items, nitems, c, dLdE, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz);
-  return cudaGetLastError();
+                                          const BatchSys* sys, const BatchItem* items,
+                                          const BatchSeg* segs, int nseg, int ctas, double c,
+                                          const double* dLdE, const float* psi, const float* phi,
+                                          const double* gfx, const double* gfy, const double* gfz,
+                                          double* dq, double* dx, double* dy, double* dz,
+                                          cudaStream_t st) {
+  for (int k = 0; k < nseg; k++) {
+    const BatchItem* it = items + segs[k].first;
+    const int cnt = std::min(ctas, segs[k].count), ni = segs[k].count;
+    if (ni <= 0) continue;
+    cudaError_t e;
+#define GSE_BAG(WW)                                                                          \
+  case WW: {                                                                                 \
+    static bool done[64] = {};                                                               \
+    const size_t smem = AdjGatherGeom<WW>::bytes;                                            \
+    e = set_smem_once(k_batch_adj_gather_tiled<WW>, smem, done);                             \
+    if (e == cudaSuccess)                                                                    \
+      k_batch_adj_gather_tiled<WW><<<cnt, kAdjThreads, smem, st>>>(                          \
+          sorted, perm, start, sys, it, ni, c, dLdE, psi, phi, gfx, gfy, gfz, dq, dx, dy, dz);   \
+    break;                                                                                   \
+  }
+    switch (segs[k].W) {
+      GSE_BAG(9)
+      GSE_BAG(11)
+      GSE_BAG(13)
+      GSE_BAG(15)
+      default: e = cudaErrorInvalidValue;
+    }
+#undef GSE_BAG
+    if (e != cudaSuccess) return e;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int ntot,

@@ -33,18 +33,18 @@ cudaError_t launch_adj_gather_tiled(const float4* sorted, const int* perm, const
                                     const double* gfy, const double* gfz, double* dq, double* dx,
                                     double* dy, double* dz, cudaStream_t st);
 cudaError_t launch_batch_adj_scatter(const float4* sorted, const int* perm, const int* start,
-                                     const BatchSys* sys, const BatchItem* items, int nitems,
-                                     int ctas, double c, const double* gfx, const double* gfy,
-                                     const double* gfz, long long* grid64, long long gsize,
-                                     float* lambda, cudaStream_t st);
+                                     const BatchSys* sys, const BatchItem* items,
+                                     const BatchSeg* segs, int nseg, int ctas, double c,
+                                     const double* gfx, const double* gfy, const double* gfz,
+                                     long long* grid64, long long gsize, float* lambda,
+                                     cudaStream_t st);
 cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm, const int* start,
-                                          const BatchSys* sys, const BatchItem* items, int nitems,
-                                          int ctas, double c, const double* dLdE, const float* psi,
-                                          const float* phi, const double* gfx, const double* gfy,
-                                          const double* gfz, double* dq, double* dx, double* dy,
-                                          double* dz, int max_w, cudaStream_t st);
-// Shared memory of the reverse-pass gather block for stencil width W.
-size_t adj_gather_smem(int W);
+                                          const BatchSys* sys, const BatchItem* items,
+                                          const BatchSeg* segs, int nseg, int ctas, double c,
+                                          const double* dLdE, const float* psi, const float* phi,
+                                          const double* gfx, const double* gfy, const double* gfz,
+                                          double* dq, double* dx, double* dy, double* dz,
+                                          cudaStream_t st);
 
 template <typename CT>
 cudaError_t launch_adj_source(const typename Vec4<CT>::type* xyzq, const int* perm, int n,

@@ -52,7 +52,7 @@ struct gse_batch {
   std::vector<int> first;
   std::vector<SizeClass> cls;
   std::vector<BatchItem> scat, gath, agath;  // spread, gather, reverse-pass gather bricks
-  int max_w = 0;
+  std::vector<BatchSeg> scat_seg, gath_seg, agath_seg;  // runs of one stencil width
   int nbins = 0;
   long long gtot = 0, ktot = 0;
   // device
@@ -159,6 +159,21 @@ void order_items(gse_batch_t* b, bool largest_first) {
     by_work(g);
     by_work(ag);
   }
+  // group by stencil width (stable, so the order above holds within a width)
+  auto by_width = [&](std::vector<BatchItem>& v, std::vector<BatchSeg>& seg) {
+    std::stable_sort(v.begin(), v.end(), [&](const BatchItem& x, const BatchItem& y) {
+      return b->sys[x.sys].W < b->sys[y.sys].W;
+    });
+    seg.clear();
+    for (int i = 0; i < (int)v.size(); i++) {
+      const int w = b->sys[v[i].sys].W;
+      if (seg.empty() || seg.back().W != w) seg.push_back({w, i, 0});
+      seg.back().count++;
+    }
+  };
+  by_width(s, b->scat_seg);
+  by_width(g, b->gath_seg);
+  by_width(ag, b->agath_seg);
   b->scat = s;
   b->gath = g;
   b->agath = ag;
@@ -181,8 +196,8 @@ gse_status_t run_forward(gse_batch_t* b) {
   BinScratch w{b->d_key, b->d_counts, b->d_start, b->d_tiles, b->d_tmp, b->d_qmax};
   BCU(launch_batch_bin(b->d_xyzq, b->ntot, b->d_sys, b->d_first, b->nsys, b->nbins, w,
                        b->d_sorted, b->d_perm, st));
-  BCU(launch_batch_spread(b->d_sorted, b->d_start, b->d_sys, b->d_scat, (int)b->scat.size(),
-                          b->scat_ctas, b->d_g64, b->gtot, b->d_rho, st));
+  BCU(launch_batch_spread(b->d_sorted, b->d_start, b->d_sys, b->d_scat, b->scat_seg.data(),
+                          (int)b->scat_seg.size(), b->scat_ctas, b->d_g64, b->gtot, b->d_rho, st));
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecR2C(c.pf, (cufftReal*)(b->d_rho + c.goff), (cufftComplex*)(b->d_rhok + c.koff)));
   BCU(cudaMemsetAsync(b->d_energy, 0, sizeof(double) * b->nsys, st));
@@ -191,7 +206,8 @@ gse_status_t run_forward(gse_batch_t* b) {
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecC2R(c.pb, (cufftComplex*)(b->d_rhok + c.koff), (cufftReal*)(b->d_phi + c.goff)));
   BCU(launch_batch_gather(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_gath,
-                          (int)b->gath.size(), b->gath_ctas, b->d_phi, b->p.ccelec, b->d_forces,
+                          b->gath_seg.data(), (int)b->gath_seg.size(), b->gath_ctas, b->d_phi,
+                          b->p.ccelec, b->d_forces,
                           b->d_forces + b->ntot, b->d_forces + 2 * (long long)b->ntot, st));
   return GSE_OK;
 }
@@ -201,7 +217,8 @@ gse_status_t run_adjoint(gse_batch_t* b) {
   cudaStream_t st = b->stream;
   const long long nt = b->ntot;
   BCU(launch_batch_adj_scatter(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_scat,
-                               (int)b->scat.size(), b->scat_ctas, b->p.ccelec, b->d_gin,
+                               b->scat_seg.data(), (int)b->scat_seg.size(), b->scat_ctas,
+                               b->p.ccelec, b->d_gin,
                                b->d_gin + nt, b->d_gin + 2 * nt, b->d_g64, b->gtot, b->d_lam, st));
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecR2C(c.pf, (cufftReal*)(b->d_lam + c.goff), (cufftComplex*)(b->d_rhok + c.koff)));
@@ -210,10 +227,10 @@ gse_status_t run_adjoint(gse_batch_t* b) {
   for (const SizeClass& c : b->cls)
     BFFT(cufftExecC2R(c.pb, (cufftComplex*)(b->d_rhok + c.koff), (cufftReal*)(b->d_lam + c.goff)));
   BCU(launch_batch_adj_gather_tiled(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_agath,
-                                    (int)b->agath.size(), b->agath_ctas, b->p.ccelec, b->d_dLdE,
-                                    b->d_lam, b->d_phi, b->d_gin, b->d_gin + nt,
-                                    b->d_gin + 2 * nt, b->d_gout, b->d_gout + nt,
-                                    b->d_gout + 2 * nt, b->d_gout + 3 * nt, b->max_w, st));
+                                    b->agath_seg.data(), (int)b->agath_seg.size(),
+                                    b->agath_ctas, b->p.ccelec, b->d_dLdE, b->d_lam, b->d_phi,
+                                    b->d_gin, b->d_gin + nt, b->d_gin + 2 * nt, b->d_gout,
+                                    b->d_gout + nt, b->d_gout + 2 * nt, b->d_gout + 3 * nt, st));
   return GSE_OK;
 }
 
@@ -307,7 +324,6 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
       return set_error(GSE_ERR_UNSUPPORTED, "stencil width must be 9, 11, 13 or 15 on every axis");
     }
     S.W = 2 * S.sp.nst[0] + 1;
-    b->max_w = std::max(b->max_w, S.W);
     const double h3 = (box[0] / M[0]) * (box[1] / M[1]) * (box[2] / M[2]);
     S.h3 = h3;
     S.efac = 0.5 * common->ccelec * h3;

@@ -577,6 +577,27 @@ __device__ __forceinline__ void row_sums<float, 13>(const float* row, const floa
   asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(acc));
 }
 
+// Shared memory of the gather for calculation type CT and stencil width W:
+// the potential tile [TZ][ZP] (rows of pitch TP), per-atom weight tables and
+// per-atom row lists.
+template <typename CT, int W>
+struct GatherGeom {
+  static constexpr int n = (W - 1) / 2;
+  static constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
+  static constexpr int TP = TX | 1;  // odd row pitch
+  // plane pitch = W*TP (mod 32): row (jy, jz) starts in bank TP*(jy + W*jz)
+  // mod 32, distinct for 32 consecutive (jy, jz)
+  static constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
+  static constexpr int NW = kGatherThreads / 32;
+  static constexpr int APW = 32 / kGatherLanes;  // atoms per warp at a time
+  static constexpr size_t bytes =
+      sizeof(CT) * (TZ * ZP + NW * APW * 9 * kWPad) + sizeof(int) * NW * APW * W * W;
+};
+
+// The gather of the atoms of one brick.  kGatherLanes lanes share one atom
+// (two atoms per warp at 16): each group builds its atom's weight tables,
+// compacts the (y, z) rows that meet the sphere and sums them, one row per
+// lane and iteration, in the order of the row list.
 template <typename CT, int W>
 __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __restrict__ sorted,
                                              const int* __restrict__ perm,
@@ -585,22 +606,20 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
                                              double outscale, double* __restrict__ fx,
                                              double* __restrict__ fy, double* __restrict__ fz,
                                              int bxi, int byi, int bzi, unsigned char* gsm) {
-  constexpr int n = (W - 1) / 2;
-  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
-  constexpr int TP = TX | 1;  // odd row pitch
-  // plane pitch = W*TP (mod 32): row (jy, jz) starts in bank TP*(jy + W*jz) mod 32,
-  // distinct for 32 consecutive (jy, jz)
-  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
-  constexpr int NW = kGatherThreads / 32;
+  typedef GatherGeom<CT, W> GG;
+  constexpr int n = GG::n, TX = GG::TX, TY = GG::TY, TZ = GG::TZ, TP = GG::TP, ZP = GG::ZP;
+  constexpr int NW = GG::NW, APW = GG::APW, GL = kGatherLanes;
   constexpr int NR = kGY * kGZ;  // cell rows of the brick
+  constexpr int NG = (W * W + GL - 1) / GL;
   typedef typename Vec4<CT>::type V;
   CT* tile = (CT*)gsm;                                   // [TZ][ZP]
-  CT* tabs = tile + TZ * ZP;                             // [NW][3][3][kWPad]
-  int* rowl = (int*)(tabs + NW * 3 * 3 * kWPad);         // [NW][W*W]
+  CT* tabs = tile + TZ * ZP;                             // [NW][APW][axis][d, d^2, w][kWPad]
+  int* rowl = (int*)(tabs + NW * APW * 9 * kWPad);       // [NW][APW][W*W]
   __shared__ int rng_a[NR], rng_p[NR + 1];
   __shared__ int alist[kGatherList];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = lane / GL, gl = lane % GL;
   const int x0 = bxi * kGX, y0 = byi * kGY, z0 = bzi * kGZ;
   const int ex = min(kGX, b.M[0] - x0), ey = min(kGY, b.M[1] - y0), ez = min(kGZ, b.M[2] - z0);
 
@@ -629,91 +648,94 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
-  CT* tb = tabs + warp * 9 * kWPad;  // [axis][d, d^2, w][j]
-  int* rl = rowl + warp * W * W;
+  CT* tb = tabs + (warp * APW + grp) * 9 * kWPad;  // [axis][d, d^2, w][j]
+  int* rl = rowl + (warp * APW + grp) * W * W;
   // (jy, jz) of the rows each lane tests, the same for every atom
-  constexpr int NG = (W * W + 31) / 32;
   int gjy[NG], gjz[NG];
 #pragma unroll
   for (int g = 0; g < NG; g++) {
-    const int r = g * 32 + lane;
+    const int r = g * GL + gl;
     gjz[g] = r < W * W ? r / W : 0;
     gjy[g] = r < W * W ? r - (r / W) * W : 0;
   }
+  const unsigned gmask = GL == 32 ? 0xffffffffu : ((1u << GL) - 1u);
   for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
-  for (int r = tid; r < NR; r += kGatherThreads) {
-    const int p0 = rng_p[r], p1 = rng_p[r + 1];
-    for (int p = max(p0, c0); p < min(p1, c0 + kGatherList); p++) alist[p - c0] = rng_a[r] + (p - p0);
-  }
-  __syncthreads();
-  const int nc = min(kGatherList, natoms - c0);
-  for (int q = warp; q < nc; q += NW) {
-    const int ai = alist[q];
-    const V a = sorted[ai];
-    const CT pos3[3] = {a.x, a.y, a.z};
-    const int org[3] = {x0, y0, z0};
-    int loc[3];
+    brick_atom_list<kGatherThreads, NR>(rng_a, rng_p, natoms, c0, kGatherList, alist);
+    __syncthreads();
+    const int nc = min(kGatherList, natoms - c0);
+    for (int q0 = APW * warp; q0 < nc; q0 += APW * NW) {
+      const int q = q0 + grp;
+      const bool valid = q < nc;  // the last group of a chunk may have no atom
+      const int ai = alist[valid ? q : q0];
+      const V a = sorted[ai];
+      const CT pos3[3] = {a.x, a.y, a.z};
+      const int org[3] = {x0, y0, z0};
+      int loc[3];
 #pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const int c = centre_cell(pos3[d], s.inv_h[d]);
-      loc[d] = wrap1(c, s.M[d]) - org[d];  // first stencil cell in tile coordinates
-      if (lane < W) {
-        const CT dd = sub_rn(pos3[d], mul_rn((CT)(c - n + lane), s.h[d]));
-        const CT d2 = mul_rn(dd, dd);
-        tb[(d * 3 + 0) * kWPad + lane] = dd;
-        tb[(d * 3 + 1) * kWPad + lane] = d2;
-        tb[(d * 3 + 2) * kWPad + lane] = gexp(mul_rn(-d2, s.inv_2s2));
+      for (int d = 0; d < 3; d++) {
+        const int c = centre_cell(pos3[d], s.inv_h[d]);
+        loc[d] = wrap1(c, s.M[d]) - org[d];  // first stencil cell in tile coordinates
+        for (int j = gl; j < W; j += GL) {
+          const CT dd = sub_rn(pos3[d], mul_rn((CT)(c - n + j), s.h[d]));
+          const CT d2 = mul_rn(dd, dd);
+          tb[(d * 3 + 0) * kWPad + j] = dd;
+          tb[(d * 3 + 1) * kWPad + j] = d2;
+          tb[(d * 3 + 2) * kWPad + j] = gexp(mul_rn(-d2, s.inv_2s2));
+        }
       }
-    }
-    __syncwarp();
-    // non-empty rows (the whole row is outside the sphere when dy^2+dz^2 >= rcut^2)
-    int nrow = 0;
+      __syncwarp();
+      // non-empty rows (the whole row is outside the sphere when dy^2+dz^2 >= rcut^2)
+      int nrow = 0;
 #pragma unroll
-    for (int g = 0; g < NG; g++) {
-      const int r = g * 32 + lane;
-      bool ne = false;
-      if (r < W * W)
-        ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) < s.rcut2;
-      const unsigned m = __ballot_sync(0xffffffffu, ne);
-      if (ne) rl[nrow + __popc(m & ((1u << lane) - 1u))] = (gjz[g] << 8) | gjy[g];
-      nrow += __popc(m);
-    }
-    __syncwarp();
-    CT dx2[W], wx[W], wdx[W];
+      for (int g = 0; g < NG; g++) {
+        const int r = g * GL + gl;
+        bool ne = false;
+        if (r < W * W)
+          ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) <
+               s.rcut2;
+        const unsigned m = (__ballot_sync(0xffffffffu, ne) >> (GL * grp)) & gmask;
+        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = (gjz[g] << 8) | gjy[g];
+        nrow += __popc(m);
+      }
+      __syncwarp();
+      CT dx2[W], wx[W], wdx[W];
 #pragma unroll
-    for (int k = 0; k < W; k++) {
-      dx2[k] = tb[(0 * 3 + 1) * kWPad + k];
-      wx[k] = tb[(0 * 3 + 2) * kWPad + k];
-      wdx[k] = wx[k] * tb[(0 * 3 + 0) * kWPad + k];
+      for (int k = 0; k < W; k++) {
+        dx2[k] = tb[(0 * 3 + 1) * kWPad + k];
+        wx[k] = tb[(0 * 3 + 2) * kWPad + k];
+        wdx[k] = wx[k] * tb[(0 * 3 + 0) * kWPad + k];
+      }
+      // rows accumulate in double (the reference's AT), each row's 2n+1 terms in CT
+      double ax = 0, ay = 0, az = 0;
+      for (int i = gl; i < nrow; i += GL) {
+        const int r = rl[i];
+        const int jz = r >> 8, jy = r & 255;
+        const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
+        const CT rem = s.rcut2 - (dy2 + dz2);
+        const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
+        CT s0, s1;
+        row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
+        const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
+        ax += (double)(wyz * s1);
+        ay += (double)(wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0);
+        az += (double)(wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0);
+      }
+#pragma unroll
+      for (int o = GL / 2; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+      }
+      if (gl == 0 && valid) {
+        const int o = perm[ai];
+        const double f = outscale * (double)(a.w * s.pref);
+        fx[o] = f * ax;
+        fy[o] = f * ay;
+        fz[o] = f * az;
+      }
+      __syncwarp();
     }
-    // rows accumulate in double (the reference's AT), each row's 2n+1 terms in CT
-    double ax = 0, ay = 0, az = 0;
-    for (int i = lane; i < nrow; i += 32) {
-      const int r = rl[i];
-      const int jz = r >> 8, jy = r & 255;
-      const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
-      const CT rem = s.rcut2 - (dy2 + dz2);
-      const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
-      CT s0, s1;
-      row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
-      const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
-      ax += (double)(wyz * s1);
-      ay += (double)(wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0);
-      az += (double)(wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0);
-    }
-    ax = warp_sum(ax);
-    ay = warp_sum(ay);
-    az = warp_sum(az);
-    if (lane == 0) {
-      const int o = perm[ai];
-      const double f = outscale * (double)(a.w * s.pref);
-      fx[o] = f * ax;
-      fy[o] = f * ay;
-      fz[o] = f * az;
-    }
-    __syncwarp();
-  }
-  __syncthreads();
+    __syncthreads();
   }
 }
 
@@ -818,11 +840,7 @@ static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* pe
                             const int* start, const BinLayout& b, const Stencil<CT>& s,
                             const CT* phi, double outscale, double* fx, double* fy, double* fz,
                             cudaStream_t st) {
-  constexpr int n = (W - 1) / 2;
-  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
-  constexpr int TP = TX | 1, NW = kGatherThreads / 32;
-  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
-  const size_t smem = sizeof(CT) * (TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+  const size_t smem = GatherGeom<CT, W>::bytes;
   static bool attr[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -925,6 +943,7 @@ __global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
   }
 }
 
+template <int W>
 __global__ void __launch_bounds__(kScatterThreads)
     k_batch_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
                     const BatchSys* __restrict__ sys, const BatchItem* __restrict__ items,
@@ -933,14 +952,8 @@ __global__ void __launch_bounds__(kScatterThreads)
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const BatchItem item = items[it];
     const BatchSys& S = sys[item.sys];
-    long long* out = grid64 + S.grid_off;
-    const int* st = start + S.bin_off;
-    switch (S.W) {
-      case 9: scatter_brick<9>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
-      case 11: scatter_brick<11>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
-      case 13: scatter_brick<13>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
-      case 15: scatter_brick<15>(sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, out); break;
-    }
+    scatter_brick<W>(sorted, start + S.bin_off, S.b, S.sp, item.bx, item.by, item.bz, tile,
+                     grid64 + S.grid_off);
     __syncthreads();
   }
 }
@@ -991,6 +1004,7 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+template <int W>
 __global__ void __launch_bounds__(kGatherThreads, 2)
     k_batch_gather(const float4* __restrict__ sorted, const int* __restrict__ perm,
                    const int* __restrict__ start, const BatchSys* __restrict__ sys,
@@ -1001,26 +1015,49 @@ __global__ void __launch_bounds__(kGatherThreads, 2)
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const BatchItem item = items[it];
     const BatchSys& S = sys[item.sys];
-    const int* st = start + S.bin_off;
-    const float* ph = phi + S.grid_off;
-    switch (S.W) {
-      case 9: gather_brick<float, 9>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
-      case 11: gather_brick<float, 11>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
-      case 13: gather_brick<float, 13>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
-      case 15: gather_brick<float, 15>(sorted, perm, st, S.b, S.sg, ph, outscale, fx, fy, fz, item.bx, item.by, item.bz, gsm); break;
-    }
+    gather_brick<float, W>(sorted, perm, start + S.bin_off, S.b, S.sg, phi + S.grid_off, outscale,
+                           fx, fy, fz, item.bx, item.by, item.bz, gsm);
     __syncthreads();
   }
 }
 
-size_t batch_scatter_smem() { return sizeof(int) * ScatterGeom<15>::words; }
+template <class K>
+static cudaError_t set_max_smem(K kernel, size_t bytes, bool* done) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (done[dev]) return cudaSuccess;
+  const cudaError_t e =
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done[dev] = true;
+  return e;
+}
 
-size_t batch_gather_smem() {
-  constexpr int W = 15, n = 7;
-  constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
-  constexpr int TP = TX | 1, NW = kGatherThreads / 32;
-  constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
-  return sizeof(float) * (TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+template <int W>
+static cudaError_t batch_scatter_w(const float4* sorted, const int* start, const BatchSys* sys,
+                                   const BatchItem* items, int nitems, int ctas,
+                                   long long* grid64, cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = sizeof(int) * ScatterGeom<W>::words;
+  const cudaError_t e = set_max_smem(k_batch_scatter<W>, smem, done);
+  if (e != cudaSuccess) return e;
+  k_batch_scatter<W><<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(sorted, start, sys,
+                                                                           items, nitems, grid64);
+  return cudaGetLastError();
+}
+
+template <int W>
+static cudaError_t batch_gather_w(const float4* sorted, const int* perm, const int* start,
+                                  const BatchSys* sys, const BatchItem* items, int nitems,
+                                  int ctas, const float* phi, double outscale, double* fx,
+                                  double* fy, double* fz, cudaStream_t st) {
+  static bool done[64] = {};
+  const size_t smem = GatherGeom<float, W>::bytes;
+  const cudaError_t e = set_max_smem(k_batch_gather<W>, smem, done);
+  if (e != cudaSuccess) return e;
+  k_batch_gather<W><<<std::min(ctas, nitems), kGatherThreads, smem, st>>>(
+      sorted, perm, start, sys, items, nitems, phi, outscale, fx, fy, fz);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
@@ -1035,24 +1072,23 @@ cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, 
 }
 
 cudaError_t launch_batch_spread(const float4* sorted, const int* start, const BatchSys* sys,
-                                const BatchItem* items, int nitems, int ctas, long long* grid64,
-                                long long gsize, float* rho, cudaStream_t st) {
-  const size_t smem = batch_scatter_smem();
-  static bool attr[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!attr[dev]) {
-    const cudaError_t e = cudaFuncSetAttribute(k_batch_scatter,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr[dev] = true;
-  }
+                                const BatchItem* items, const BatchSeg* segs, int nseg, int ctas,
+                                long long* grid64, long long gsize, float* rho, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(grid64, 0, sizeof(long long) * gsize, st);
   if (e != cudaSuccess) return e;
-  if (nitems > 0)
-    k_batch_scatter<<<std::min(ctas, nitems), kScatterThreads, smem, st>>>(sorted, start, sys, items,
-                                                                         nitems, grid64);
+  for (int k = 0; k < nseg; k++) {
+    const BatchItem* it = items + segs[k].first;
+    const int cnt = segs[k].count;
+    if (cnt <= 0) continue;
+    switch (segs[k].W) {
+      case 9: e = batch_scatter_w<9>(sorted, start, sys, it, cnt, ctas, grid64, st); break;
+      case 11: e = batch_scatter_w<11>(sorted, start, sys, it, cnt, ctas, grid64, st); break;
+      case 13: e = batch_scatter_w<13>(sorted, start, sys, it, cnt, ctas, grid64, st); break;
+      case 15: e = batch_scatter_w<15>(sorted, start, sys, it, cnt, ctas, grid64, st); break;
+      default: e = cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+  }
   k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, gsize, rho);
   return cudaGetLastError();
 }
@@ -1065,24 +1101,24 @@ cudaError_t launch_batch_green(float2* rhok, const float* tab, long long ktot, c
 }
 
 cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int* start,
-                                const BatchSys* sys, const BatchItem* items, int nitems, int ctas,
-                                const float* phi, double outscale, double* fx, double* fy,
-                                double* fz, cudaStream_t st) {
-  const size_t smem = batch_gather_smem();
-  static bool attr[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!attr[dev]) {
-    const cudaError_t e = cudaFuncSetAttribute(k_batch_gather,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                const BatchSys* sys, const BatchItem* items, const BatchSeg* segs,
+                                int nseg, int ctas, const float* phi, double outscale, double* fx,
+                                double* fy, double* fz, cudaStream_t st) {
+  for (int k = 0; k < nseg; k++) {
+    const BatchItem* it = items + segs[k].first;
+    const int cnt = segs[k].count;
+    if (cnt <= 0) continue;
+    cudaError_t e;
+    switch (segs[k].W) {
+      case 9: e = batch_gather_w<9>(sorted, perm, start, sys, it, cnt, ctas, phi, outscale, fx, fy, fz, st); break;
+      case 11: e = batch_gather_w<11>(sorted, perm, start, sys, it, cnt, ctas, phi, outscale, fx, fy, fz, st); break;
+      case 13: e = batch_gather_w<13>(sorted, perm, start, sys, it, cnt, ctas, phi, outscale, fx, fy, fz, st); break;
+      case 15: e = batch_gather_w<15>(sorted, perm, start, sys, it, cnt, ctas, phi, outscale, fx, fy, fz, st); break;
+      default: e = cudaErrorInvalidValue;
+    }
     if (e != cudaSuccess) return e;
-    attr[dev] = true;
   }
-  if (nitems > 0)
-    k_batch_gather<<<std::min(ctas, nitems), kGatherThreads, smem, st>>>(
-        sorted, perm, start, sys, items, nitems, phi, outscale, fx, fy, fz);
-  return cudaGetLastError();
+  return cudaSuccess;
 }
 
 #define GSE_TILED_INST(CT)                                                                      \

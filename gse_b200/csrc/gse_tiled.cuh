@@ -19,6 +19,7 @@ constexpr int kSpreadChunk = 64;    // atoms staged per round
 constexpr int kMaxSeg = 4;          // periodic images of one row segment
 constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX
 constexpr int kGatherThreads = 256;          // >= kGY * kGZ
+constexpr int kGatherLanes = 16;             // lanes sharing one atom in the gather
 constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
 constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
 constexpr int kScatterThreads = 512;  // >= kSB * kSB
@@ -87,21 +88,25 @@ struct BatchItem {
   int sys, bx, by, bz;  // brick of one system
 };
 
-size_t batch_scatter_smem();
-size_t batch_gather_smem();
+// A run of work items whose systems share one stencil width W (the batched
+// kernels are instantiated per width; one launch per run).
+struct BatchSeg {
+  int W, first, count;
+};
+
 cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
                              int nsys, int nbins, BinScratch w, float4* sorted, int* perm,
                              cudaStream_t st);
 cudaError_t launch_batch_spread(const float4* sorted, const int* start, const BatchSys* sys,
-                                const BatchItem* items, int nitems, int ctas, long long* grid64,
-                                long long gsize, float* rho, cudaStream_t st);
+                                const BatchItem* items, const BatchSeg* segs, int nseg, int ctas,
+                                long long* grid64, long long gsize, float* rho, cudaStream_t st);
 cudaError_t launch_batch_green(float2* rhok, const float* tab, long long ktot, const BatchSys* sys,
                                const long long* kfirst, const int* ksys, int nsys, double* energy,
                                cudaStream_t st);
 cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int* start,
-                                const BatchSys* sys, const BatchItem* items, int nitems, int ctas,
-                                const float* phi, double outscale, double* fx, double* fy,
-                                double* fz, cudaStream_t st);
+                                const BatchSys* sys, const BatchItem* items, const BatchSeg* segs,
+                                int nseg, int ctas, const float* phi, double outscale, double* fx,
+                                double* fy, double* fz, cudaStream_t st);
 
 // float grid = int64 accumulation grid at 2^40 (the scatter kernels' output)
 cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float* out,
