@@ -18,6 +18,7 @@ replicas only, no collective on the data path.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -68,19 +69,24 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "timestamp")
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
         self.file = None
+        self.window = None  # host wall-clock interval of the timed region
+
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
 
     def start(self):
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -101,6 +107,10 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             try:
+                if self.window is not None:
+                    ts = datetime.datetime.strptime(r[9].strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    if not (self.window[0] <= ts <= self.window[1]):
+                        continue
                 sm.append(float(r[1]))
                 mx = max(mx, float(r[2]))
                 for k, name in enumerate(names):
@@ -236,7 +246,7 @@ def bench_batch(steps: int, warmup: int, flush):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -287,38 +297,55 @@ def main():
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def timed_loop(ctx, x, f, e, steps, with_timing):
+    def timed_loop(ctx, x, f, e, steps, with_timing, clocks=None):
+        """Warm-up, then `steps` evaluations each bracketed by CUDA events on the
+        launching stream with an L2 flush before each (outside the interval).
+        Without stage timing, repeated calls on the same device buffers replay
+        the context's captured CUDA graph."""
         for _ in range(args.warmup):
             ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
         torch.cuda.synchronize()
         ctx.get_timing(reset=True)
-        launches0 = ctx.launch_count()
         ctx.set_timing(with_timing)
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         barrier()
         torch.cuda.synchronize()
+        if clocks is not None:
+            # the sampler needs a moment to start: keep the GPU busy meanwhile
+            clocks.start()
+            t_end = time.time() + 0.5
+            while time.time() < t_end:
+                ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
+                torch.cuda.synchronize()
+        launches0 = ctx.launch_count()
+        t0 = time.time()
         for k in range(steps):
             flush.zero_()  # L2 flush, outside the timed interval
             starts[k].record(stream)
             ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
             ends[k].record(stream)
         torch.cuda.synchronize()
+        t1 = time.time()
+        launches = ctx.launch_count() - launches0
+        clock_info = None
+        if clocks is not None:
+            clocks.mark(t0, t1)
+            clock_info = clocks.stop()
         barrier()
         ctx.set_timing(False)
         stage = ctx.get_timing(reset=True)
-        launches = ctx.launch_count() - launches0
         ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-        return ms, stage, launches
+        return ms, stage, launches, clock_info
 
     # ---- main arm: requested precision, device-resident inputs ----------
     prec = args.precision
     ctx = make_ctx(prec)
     x, f, e = device_inputs(prec)
-    clocks = ClockSampler(local)
-    clocks.start()
-    ms_local, stage, launches = timed_loop(ctx, x, f, e, args.steps, True)
-    clock_info = clocks.stop()
+    ms_local, _, launches, clock_info = timed_loop(ctx, x, f, e, args.steps, False,
+                                                   ClockSampler(local))
+    # per-stage device times from a separate, shorter run with stage events
+    _, stage, _, _ = timed_loop(ctx, x, f, e, max(3, min(args.steps, 20)), True)
     t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -358,8 +385,8 @@ def main():
     other = "fp64" if prec == "mixed" else "mixed"
     ctx2 = make_ctx(other)
     x2, f2, e2 = device_inputs(other)
-    ms2, stage2, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 20)), False)
-    value2 = world * max(3, min(args.steps, 20)) / (ms2 / 1000.0)
+    ms2, _, _, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 50)), False)
+    value2 = world * max(3, min(args.steps, 50)) / (ms2 / 1000.0)
     F64 = (f2 if other == "fp64" else F_main).double().cpu().numpy().T
     Fmx = (F_main if other == "fp64" else f2).double().cpu().numpy().T
     E64 = float(e2.item()) if other == "fp64" else E_main

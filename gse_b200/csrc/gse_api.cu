@@ -124,6 +124,23 @@ struct gse_context {
   cufftHandle plan_f = 0, plan_b = 0;
   bool plans = false;
   bool rho_valid = false, phi_valid = false, energy_valid = false;
+  // replay of repeated gse_forward calls with device inputs and outputs: the
+  // second identical call is captured into a CUDA graph, later ones launch it
+  struct FwdKey {
+    int n = -1;
+    const void* x = nullptr;
+    double *e = nullptr, *fx = nullptr, *fy = nullptr, *fz = nullptr;
+    double box[3] = {0, 0, 0};
+    cudaStream_t stream = nullptr;
+    bool operator==(const FwdKey& o) const {
+      return n == o.n && x == o.x && e == o.e && fx == o.fx && fy == o.fy && fz == o.fz &&
+             box[0] == o.box[0] && box[1] == o.box[1] && box[2] == o.box[2] &&
+             stream == o.stream;
+    }
+  } fwd_key;
+  cudaGraphExec_t fwd_exec = nullptr;
+  long long fwd_launches = 0;
+  bool fwd_graphs = true;
   // optional per-stage device timing (gse_set_timing)
   bool timing = false;
   cudaEvent_t ev[GSE_NUM_STAGES][2] = {};
@@ -205,8 +222,16 @@ gse_status_t check_stencil(const gse_context_t* c, const double box[3], double s
   return GSE_OK;
 }
 
+// Forget the captured forward graph (its buffers or parameters change).
+void drop_fwd_graph(gse_context_t* c) {
+  if (c->fwd_exec) cudaGraphExecDestroy(c->fwd_exec);
+  c->fwd_exec = nullptr;
+  c->fwd_key = gse_context_t::FwdKey();
+}
+
 gse_status_t ensure_atoms(gse_context_t* c, int n) {
   if ((size_t)n <= c->atom_cap) return GSE_OK;
+  drop_fwd_graph(c);
   size_t cap = c->atom_cap ? c->atom_cap : 1024;
   while (cap < (size_t)n) cap *= 2;
   cudaFree(c->d_xyzq);
@@ -602,6 +627,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   if (!c) return GSE_OK;
   cudaSetDevice(c->p.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_fwd_graph(c);
   if (c->plans) {
     cufftDestroy(c->plan_f);
     cufftDestroy(c->plan_b);
@@ -639,6 +665,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
 
 gse_status_t gse_set_stream(gse_context_t* c, void* stream) {
   TRY(check_ctx(c));
+  drop_fwd_graph(c);
   c->stream = (cudaStream_t)stream;
   CUFFT(cufftSetStream(c->plan_f, c->stream));
   CUFFT(cufftSetStream(c->plan_b, c->stream));
@@ -726,12 +753,11 @@ gse_status_t gse_interpolate_force(gse_context_t* c, int n, const void* xyzq, do
   return finish(c, host);
 }
 
-gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
-                         double* fy, double* fz) {
-  TRY(check_ctx(c));
-  const void* dx;
+// The four forward calls in one pass (sorting once for spread and gather).
+gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
+                          double* fy, double* fz, bool* host) {
+  const void* dx = nullptr;
   TRY(stage_atoms(c, n, xyzq, &dx));
-  bool host = false;
   const Box3 box = ctx_box(c);
   // one stable sort serves the spread and the gather
   if (c->fp64)
@@ -748,12 +774,82 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
   if (fx || fy || fz) {
     if (c->fp64)
       TRY(gather_to<double>(c, n, dx, box.v, c->sigma1, c->rcut1, (const double*)c->d_phi,
-                            c->p.ccelec, fx, fy, fz, &host, true));
+                            c->p.ccelec, fx, fy, fz, host, true));
     else
       TRY(gather_to<float>(c, n, dx, box.v, c->sigma1, c->rcut1, (const float*)c->d_phi,
-                           c->p.ccelec, fx, fy, fz, &host, true));
+                           c->p.ccelec, fx, fy, fz, host, true));
   }
-  TRY(energy_out(c, energy, &host));
+  return energy_out(c, energy, host);
+}
+
+gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
+                         double* fy, double* fz) {
+  TRY(check_ctx(c));
+  // Graph replay applies to calls whose inputs and outputs are all device
+  // memory, on a stream that can be captured, without stage timing; the key
+  // (pointers, count, box, stream) must repeat exactly.
+  const bool outs_dev = (!energy || is_device_ptr(energy)) &&
+                        ((!fx && !fy && !fz) || (fx && fy && fz && is_device_ptr(fx) &&
+                                                 is_device_ptr(fy) && is_device_ptr(fz)));
+  const bool graphable = c->fwd_graphs && !c->timing && c->stream != nullptr && n > 0 &&
+                         is_device_ptr(xyzq) && outs_dev && c->gtab_valid;
+  gse_context_t::FwdKey key;
+  key.n = n;
+  key.x = xyzq;
+  key.e = energy;
+  key.fx = fx;
+  key.fy = fy;
+  key.fz = fz;
+  key.box[0] = c->p.box_x;
+  key.box[1] = c->p.box_y;
+  key.box[2] = c->p.box_z;
+  key.stream = c->stream;
+  bool host = false;
+  if (!graphable) {
+    drop_fwd_graph(c);
+    TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
+    return finish(c, host);
+  }
+  if (c->fwd_exec && key == c->fwd_key) {
+    CU(cudaGraphLaunch(c->fwd_exec, c->stream));
+    c->launches += c->fwd_launches;
+    c->rho_valid = c->phi_valid = c->energy_valid = true;
+    return finish(c, false);
+  }
+  if (!(key == c->fwd_key)) {
+    // first call with this key: run it directly and remember the key
+    drop_fwd_graph(c);
+    TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
+    c->fwd_key = key;
+    return finish(c, host);
+  }
+  // second identical call: capture, instantiate, launch
+  const long long l0 = c->launches;
+  CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const gse_status_t st = forward_body(c, n, xyzq, energy, fx, fy, fz, &host);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+  gse_status_t result = st;
+  if (st == GSE_OK && ec == cudaSuccess && !host) {
+    const cudaError_t ei = cudaGraphInstantiate(&c->fwd_exec, g, 0);
+    if (ei == cudaSuccess) {
+      c->fwd_launches = c->launches - l0;
+      const cudaError_t el = cudaGraphLaunch(c->fwd_exec, c->stream);
+      if (el != cudaSuccess) result = fail(GSE_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(el));
+    } else {
+      c->fwd_exec = nullptr;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  if (!c->fwd_exec || result != GSE_OK) {
+    // capture failed: this pass ran nothing, so run it directly and stop trying
+    cudaGetLastError();
+    c->fwd_graphs = false;
+    drop_fwd_graph(c);
+    c->launches = l0;
+    host = false;
+    TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
+  }
   return finish(c, host);
 }
 

@@ -187,3 +187,39 @@ def test_errors_are_statuses():
     with pytest.raises(GseError) as ei:
         gs.setBoxSize(-1.0, 16.0, 16.0)
     assert ei.value.name == "GSE_ERR_INVALID_ARG"
+
+
+def test_repeated_device_forward_replays_a_graph():
+    """Repeated gse_forward calls with the same device buffers are captured
+    into a CUDA graph on the second call and replayed afterwards; replays see
+    new positions written into the same buffer and give what a fresh context
+    computes."""
+    import torch
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
+    s = W.config_water_23k()
+    M, L = s.M, s.box
+    st = torch.cuda.Stream()
+    outs = []
+    ctx = Context(M, M, M, s.sigma, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    ctx.set_stream(st.cuda_stream)
+    x = torch.from_numpy(s.xyzq).cuda()
+    f = torch.zeros(3, s.n, dtype=torch.float64, device="cuda")
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for k in range(5):
+        if k == 3:
+            with torch.cuda.stream(st):
+                x[:, :3] += 0.25
+        ctx.forward(s.n, x, f[0], f[1], f[2], energy_out=e)
+        st.synchronize()
+        outs.append((float(e.item()), f.clone()))
+    # calls 0..2 agree (eager, eager, capture+launch); 3 and 4 are replays on moved atoms
+    assert outs[0][0] == outs[1][0] == outs[2][0]
+    assert torch.equal(outs[0][1], outs[2][1])
+    assert torch.equal(outs[3][1], outs[4][1])
+    fresh = Context(M, M, M, s.sigma, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    f2 = torch.zeros_like(f)
+    E2 = fresh.forward(s.n, x.clone(), f2[0], f2[1], f2[2])
+    torch.cuda.synchronize()
+    assert torch.equal(f2, outs[4][1]) and E2 == outs[4][0]
+    assert ctx.launch_count() > 0
