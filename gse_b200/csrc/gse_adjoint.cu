@@ -313,14 +313,15 @@ struct AdjGatherGeom {
   static constexpr int TP = TX | 1;
   static constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
   static constexpr int NW = kAdjThreads / 32;
+  static constexpr int APW = 32 / kAdjLanes;  // atoms per warp at a time
   static constexpr size_t bytes =
-      sizeof(float) * (2 * TZ * ZP + NW * 9 * kWPad) + sizeof(int) * NW * W * W;
+      sizeof(float) * (2 * TZ * ZP + NW * APW * 9 * kWPad) + sizeof(int) * NW * APW * W * W;
 };
 
 // Reverse-pass gather of the atoms of one kAX x kAY x kAZ brick: Psi = psi +
-// gE c h^3 phi and phi of the brick plus halo in shared memory; one warp per
-// atom: the cube rows of Psi (moments e, e u_x) and the sphere rows of phi
-// (moments e, e u_x, e u_x^2), combined into dL/dq and dL/dx.
+// gE c h^3 phi and phi of the brick plus halo in shared memory; kAdjLanes
+// lanes per atom: the cube rows of Psi (moments e, e u_x) and the sphere rows
+// of phi (moments e, e u_x, e u_x^2), combined into dL/dq and dL/dx.
 template <int W>
 __device__ __forceinline__ void adj_gather_brick(
     const float4* __restrict__ sorted, const int* __restrict__ perm, const int* __restrict__ start,
@@ -332,16 +333,17 @@ __device__ __forceinline__ void adj_gather_brick(
     unsigned char* smem) {
   typedef AdjGatherGeom<W> AG;
   constexpr int n = AG::n, TX = AG::TX, TY = AG::TY, TZ = AG::TZ, TP = AG::TP, ZP = AG::ZP;
-  constexpr int NW = AG::NW, NT = kAdjThreads;
+  constexpr int NW = AG::NW, APW = AG::APW, NT = kAdjThreads, GL = kAdjLanes;
   constexpr int NR = kAY * kAZ;
-  constexpr int NG = (W * W + 31) / 32;
-  float* tpsi = (float*)smem;                     // [TZ][ZP]
-  float* tphi = tpsi + TZ * ZP;                   // [TZ][ZP]
-  float* tabs = tphi + TZ * ZP;                   // [NW][axis][u, u^2, e][kWPad]
-  int* rowl = (int*)(tabs + NW * 9 * kWPad);      // [NW][W*W]
+  constexpr int NG = (W * W + GL - 1) / GL;
+  float* tpsi = (float*)smem;                        // [TZ][ZP]
+  float* tphi = tpsi + TZ * ZP;                      // [TZ][ZP]
+  float* tabs = tphi + TZ * ZP;                      // [NW][APW][axis][u, u^2, e][kWPad]
+  int* rowl = (int*)(tabs + NW * APW * 9 * kWPad);   // [NW][APW][W*W]
   __shared__ int rng_a[NR], rng_p[NR + 1];
   __shared__ int alist[kGatherList];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = lane / GL, gl = lane % GL;
   const int x0 = bxi * kAX, y0 = byi * kAY, z0 = bzi * kAZ;
   const int ex = min(kAX, b.M[0] - x0), ey = min(kAY, b.M[1] - y0), ez = min(kAZ, b.M[2] - z0);
   int cnt = 0;
@@ -371,27 +373,26 @@ __device__ __forceinline__ void adj_gather_brick(
   }
   __syncthreads();
 
-  float* tb = tabs + warp * 9 * kWPad;
-  int* rl = rowl + warp * W * W;
+  float* tb = tabs + (warp * APW + grp) * 9 * kWPad;
+  int* rl = rowl + (warp * APW + grp) * W * W;
   int gjy[NG], gjz[NG];
 #pragma unroll
   for (int g = 0; g < NG; g++) {
-    const int r = g * 32 + lane;
+    const int r = g * GL + gl;
     gjz[g] = r < W * W ? r / W : 0;
     gjy[g] = r < W * W ? r - (r / W) * W : 0;
   }
+  const unsigned gmask = GL == 32 ? 0xffffffffu : ((1u << GL) - 1u);
   const double pref_sp = (double)sp.pref, inv_s2 = 2.0 * (double)sp.inv_2s2;
   const double cA = c * (double)sg.pref;
   for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
-    for (int r = tid; r < NR; r += NT) {
-      const int p0 = rng_p[r], p1 = rng_p[r + 1];
-      for (int p = max(p0, c0); p < min(p1, c0 + kGatherList); p++)
-        alist[p - c0] = rng_a[r] + (p - p0);
-    }
+    brick_atom_list<NT, NR>(rng_a, rng_p, natoms, c0, kGatherList, alist);
     __syncthreads();
     const int nc = min(kGatherList, natoms - c0);
-    for (int q = warp; q < nc; q += NW) {
-      const int ai = alist[q];
+    for (int q0 = APW * warp; q0 < nc; q0 += APW * NW) {
+      const int q = q0 + grp;
+      const bool valid = q < nc;
+      const int ai = alist[valid ? q : q0];
       const float4 a = sorted[ai];
       const float pos3[3] = {a.x, a.y, a.z};
       const int org[3] = {x0, y0, z0};
@@ -400,12 +401,12 @@ __device__ __forceinline__ void adj_gather_brick(
       for (int d = 0; d < 3; d++) {
         const int cc = centre_cell(pos3[d], sp.inv_h[d]);
         loc[d] = wrap1(cc, sp.M[d]) - org[d];
-        if (lane < W) {
-          const float u = sub_rn(pos3[d], mul_rn((float)(cc - n + lane), sp.h[d]));
+        for (int j = gl; j < W; j += GL) {
+          const float u = sub_rn(pos3[d], mul_rn((float)(cc - n + j), sp.h[d]));
           const float u2 = mul_rn(u, u);
-          tb[(d * 3 + 0) * kWPad + lane] = u;
-          tb[(d * 3 + 1) * kWPad + lane] = u2;
-          tb[(d * 3 + 2) * kWPad + lane] = expf(mul_rn(-u2, sp.inv_2s2));
+          tb[(d * 3 + 0) * kWPad + j] = u;
+          tb[(d * 3 + 1) * kWPad + j] = u2;
+          tb[(d * 3 + 2) * kWPad + j] = expf(mul_rn(-u2, sp.inv_2s2));
         }
       }
       __syncwarp();
@@ -420,7 +421,7 @@ __device__ __forceinline__ void adj_gather_brick(
       double P = 0.0, Vx = 0.0, Vy = 0.0, Vz = 0.0;
 #pragma unroll
       for (int g = 0; g < NG; g++) {
-        if (g * 32 + lane < W * W) {
+        if (g * GL + gl < W * W) {
           const int jy = gjy[g], jz = gjz[g];
           const float* row = tpsi + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
           unsigned long long acc = 0ull;
@@ -440,21 +441,17 @@ __device__ __forceinline__ void adj_gather_brick(
           Vz += (double)(a0 * tb[(2 * 3 + 0) * kWPad + jz]);
         }
       }
-      P = warp_sum(P);
-      Vx = warp_sum(Vx);
-      Vy = warp_sum(Vy);
-      Vz = warp_sum(Vz);
       // sphere rows of phi
       int nrow = 0;
 #pragma unroll
       for (int g = 0; g < NG; g++) {
-        const int r = g * 32 + lane;
+        const int r = g * GL + gl;
         bool ne = false;
         if (r < W * W)
           ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) <
                sg.rcut2;
-        const unsigned m = __ballot_sync(0xffffffffu, ne);
-        if (ne) rl[nrow + __popc(m & ((1u << lane) - 1u))] = (gjz[g] << 8) | gjy[g];
+        const unsigned m = (__ballot_sync(0xffffffffu, ne) >> (GL * grp)) & gmask;
+        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = (gjz[g] << 8) | gjy[g];
         nrow += __popc(m);
       }
       __syncwarp();
@@ -466,7 +463,7 @@ __device__ __forceinline__ void adj_gather_brick(
       }
       double T0 = 0, T1x = 0, T1y = 0, T1z = 0;
       double Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
-      for (int i = lane; i < nrow; i += 32) {
+      for (int i = gl; i < nrow; i += GL) {
         const int r = rl[i];
         const int jz = r >> 8, jy = r & 255;
         const float uy2 = tb[(1 * 3 + 1) * kWPad + jy], uz2 = tb[(2 * 3 + 1) * kWPad + jz];
@@ -498,28 +495,23 @@ __device__ __forceinline__ void adj_gather_brick(
         Myz += (double)(a0 * uy * uz);
         Mzz += (double)(a0 * uz2);
       }
-      T0 = warp_sum(T0);
-      T1x = warp_sum(T1x);
-      T1y = warp_sum(T1y);
-      T1z = warp_sum(T1z);
-      Mxx = warp_sum(Mxx);
-      Mxy = warp_sum(Mxy);
-      Mxz = warp_sum(Mxz);
-      Myy = warp_sum(Myy);
-      Myz = warp_sum(Myz);
-      Mzz = warp_sum(Mzz);
-      if (lane == 0) {
+      double acc14[14] = {P, Vx, Vy, Vz, T0, T1x, T1y, T1z, Mxx, Mxy, Mxz, Myy, Myz, Mzz};
+#pragma unroll
+      for (int o = GL / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int v = 0; v < 14; v++) acc14[v] += __shfl_xor_sync(0xffffffffu, acc14[v], o);
+      if (gl == 0 && valid) {
         const int o = perm[ai];
         const double q = (double)a.w;
         const double Gx = gfx ? gfx[o] : 0.0, Gy = gfy ? gfy[o] : 0.0, Gz = gfz ? gfz[o] : 0.0;
-        const double T2x = Mxx * Gx + Mxy * Gy + Mxz * Gz;
-        const double T2y = Mxy * Gx + Myy * Gy + Myz * Gz;
-        const double T2z = Mxz * Gx + Myz * Gy + Mzz * Gz;
+        const double T2x = acc14[8] * Gx + acc14[9] * Gy + acc14[10] * Gz;
+        const double T2y = acc14[9] * Gx + acc14[11] * Gy + acc14[12] * Gz;
+        const double T2z = acc14[10] * Gx + acc14[12] * Gy + acc14[13] * Gz;
         const double vs = -pref_sp * inv_s2;  // (r - x) = -u
-        dq[o] = pref_sp * P + cA * (Gx * T1x + Gy * T1y + Gz * T1z);
-        dx[o] = q * vs * Vx + cA * q * (Gx * T0 - T2x * inv_s2);
-        dy[o] = q * vs * Vy + cA * q * (Gy * T0 - T2y * inv_s2);
-        dz[o] = q * vs * Vz + cA * q * (Gz * T0 - T2z * inv_s2);
+        dq[o] = pref_sp * acc14[0] + cA * (Gx * acc14[5] + Gy * acc14[6] + Gz * acc14[7]);
+        dx[o] = q * vs * acc14[1] + cA * q * (Gx * acc14[4] - T2x * inv_s2);
+        dy[o] = q * vs * acc14[2] + cA * q * (Gy * acc14[4] - T2y * inv_s2);
+        dz[o] = q * vs * acc14[3] + cA * q * (Gz * acc14[4] - T2z * inv_s2);
       }
       __syncwarp();
     }

@@ -27,6 +27,9 @@ constexpr int kScatterList = 1024;  // atoms per scatter round (per brick)
 constexpr int kGatherList = 512;    // atoms per gather round (per brick)
 constexpr int kAX = 16, kAY = 8, kAZ = 8;  // reverse-pass gather brick (two staged grids)
 constexpr int kAdjThreads = 256;           // >= kAY * kAZ
+// lanes per atom in the reverse-pass gather: a whole warp (two atoms per warp
+// would need more shared memory than two blocks per SM leave for its tables)
+constexpr int kAdjLanes = 32;
 
 // Atoms sorted by key (z cell, y cell, x bin); start[k] .. start[k+1] is bin k.
 struct BinLayout {
