@@ -154,13 +154,17 @@ __device__ __forceinline__ void brick_flush(const int* __restrict__ tile, const 
                                             long long* __restrict__ grid64) {
   typedef ScatterGeom<W> G;
   constexpr int n = G::n, T = G::T;
+  static_assert(T <= 32, "one lane per tile column");
   const long long mul = 1LL << (kFlushBits - shift);
-  for (int i = threadIdx.x; i < T * T * T; i += NT) {
-    const int zz = i / (T * T), r = i - zz * T * T, yy = r / T, xx = r - yy * T;
-    const int v = tile[zz * G::PP + r];
+  // one (y, z) row of the tile per warp iteration, one lane per x; the
+  // wrapped x of a lane is the same for every row
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gx = lane < T ? wrap1(x0 - n + lane, b.M[0]) : 0;
+  for (int r = warp; r < T * T; r += NT / 32) {
+    const int zz = r / T, yy = r - zz * T;
+    const int v = lane < T ? tile[zz * G::PP + yy * T + lane] : 0;
     if (v != 0) {
-      const int gx = wrap1(x0 - n + xx, b.M[0]), gy = wrap1(y0 - n + yy, b.M[1]),
-                gz = wrap1(z0 - n + zz, b.M[2]);
+      const int gy = wrap1(y0 - n + yy, b.M[1]), gz = wrap1(z0 - n + zz, b.M[2]);
       atomicAdd((unsigned long long*)(grid64 + gx +
                                       ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
                 (unsigned long long)((long long)v * mul));
