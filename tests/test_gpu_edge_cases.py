@@ -1,0 +1,101 @@
+"""Edge cases of the CUDA path against the oracle (the C restatement of the
+reference, itself pinned to the compiled reference in test_oracle.py).
+
+FP64 within 1e-12 relative (forces RMS, energy), mixed within 1e-5 of the FP64
+oracle.  Cases: positions outside the box (negative and beyond L, several box
+lengths away), a single charge, zero atoms, all charges in one cell, zero
+charges, a large non-cubic grid, the smallest tiled grid, and stencils of
+every supported width on the tiled path."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_TOL = 1e-5
+
+
+def run(M, box, sigma, xyzq, precision):
+    from gse_b200.gse import CpuGSEk
+    ct = np.float64 if precision == "fp64" else np.float32
+    x = np.ascontiguousarray(xyzq, dtype=ct).reshape(-1, 4)
+    n = x.shape[0]
+    g = CpuGSEk(M[0], M[1], M[2], sigma, 0.4, 3.0, 3.0, box[0], box[1], box[2],
+                precision=precision)
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    E = g.forward(n, x, fx, fy, fz)
+    return E, np.stack([fx, fy, fz], 1)
+
+
+def check(M, box, sigma, xyzq, tol64=FP64_TOL, tolm=MIXED_TOL):
+    import oracle
+    E0, F0 = oracle.gsek_forward(M, box, sigma, np.asarray(xyzq, np.float64))
+    for precision, tol in (("fp64", tol64), ("mixed", tolm)):
+        E, F = run(M, box, sigma, xyzq, precision)
+        if np.abs(F0).sum() > 0:
+            assert oracle.force_rms(F, F0) <= tol, (precision, oracle.force_rms(F, F0))
+        else:
+            assert np.abs(F).max() == 0.0
+        if E0 != 0.0:
+            assert abs(E - E0) <= tol * abs(E0), (precision, E, E0)
+        else:
+            assert abs(E) <= 1e-30
+
+
+def waters(n, L, seed):
+    from gse_b200 import workloads as W
+    return W.triplets(n, L, seed).astype(np.float64)
+
+
+def test_positions_outside_the_box():
+    """The reference wraps grid indices, not positions: atoms anywhere in space
+    spread and gather with their periodic images' grid points."""
+    L, M = 18.0, 18
+    x = waters(300, L, 11)
+    rng = np.random.default_rng(3)
+    shift = rng.integers(-3, 4, size=(300, 3)) * L
+    x[:, :3] += shift
+    x[:5, :3] -= 0.5 * L  # a few straddling the faces
+    check((M, M, M), (L, L, L), 2.0, x)
+
+
+def test_single_charge_and_empty_system():
+    # the mesh force of an isolated charge on itself is a lattice residue that
+    # cancels to ~1e-3 of a pair force, so summation order shows at ~1e-11 of it
+    check((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.array([[3.3, 7.1, 12.9, 1.0]]),
+          tol64=1e-9)
+    E, F = run((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.zeros((0, 4)), "fp64")
+    assert E == 0.0 and F.shape == (0, 3)
+    E, F = run((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.zeros((0, 4)), "mixed")
+    assert E == 0.0 and F.shape == (0, 3)
+
+
+def test_all_charges_in_one_cell_and_zero_charges():
+    rng = np.random.default_rng(5)
+    x = np.zeros((200, 4))
+    x[:, :3] = 8.0 + rng.uniform(-0.2, 0.2, (200, 3))
+    x[:, 3] = rng.choice([-1.0, 1.0], 200)
+    check((16, 16, 16), (16.0, 16.0, 16.0), 2.0, x, tolm=2e-5)
+    x[:, 3] = 0.0
+    check((16, 16, 16), (16.0, 16.0, 16.0), 2.0, x)
+
+
+@pytest.mark.parametrize("M,box", [((10, 11, 12), (10.0, 11.0, 12.0)),
+                                   ((96, 80, 112), (93.0, 77.0, 108.0))])
+def test_small_and_large_noncubic_grids(M, box):
+    rng = np.random.default_rng(8)
+    n = 600 if M[0] < 20 else 30000
+    x = waters(n, box[0], 9)
+    x[:, :3] *= np.array(box) / box[0]
+    x[:, :3] += rng.uniform(0, 1e-3, (n, 3))
+    check(M, box, 2.0, x)
+
+
+@pytest.mark.parametrize("h", [1.45, 1.2, 1.0, 0.86])
+def test_every_tiled_stencil_width(h):
+    """rcut1 = 5.367 for sigma 2: h sets n = ceil(rcut/h) to 4, 5, 6, 7 --
+    stencil widths 9, 11, 13 and 15 on the tiled path."""
+    M = 24
+    L = M * h
+    x = waters(900, L, 12)
+    check((M, M, M), (L, L, L), 2.0, x)
