@@ -60,10 +60,20 @@ def test_positions_outside_the_box():
 
 
 def test_single_charge_and_empty_system():
-    # the mesh force of an isolated charge on itself is a lattice residue that
-    # cancels to ~1e-3 of a pair force, so summation order shows at ~1e-11 of it
-    check((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.array([[3.3, 7.1, 12.9, 1.0]]),
-          tol64=1e-9)
+    """The mesh force of an isolated charge on itself is a lattice residue that
+    cancels to ~1e-3 of the force between two unit charges 1 A apart, so it is
+    compared against that pair force: FP64 within 1e-12, mixed within 1e-5."""
+    import oracle
+    M, box = (16, 16, 16), (16.0, 16.0, 16.0)
+    one = np.array([[3.3, 7.1, 12.9, 1.0]])
+    pair = np.array([[3.3, 7.1, 12.9, 1.0], [4.3, 7.1, 12.9, -1.0]])
+    _, Fp = oracle.gsek_forward(M, box, 2.0, pair)
+    scale = float(np.abs(Fp).max())
+    E0, F0 = oracle.gsek_forward(M, box, 2.0, one)
+    for precision, tol in (("fp64", FP64_TOL), ("mixed", MIXED_TOL)):
+        E, F = run(M, box, 2.0, one, precision)
+        assert np.abs(F - F0).max() <= tol * scale, (precision, np.abs(F - F0).max() / scale)
+        assert abs(E - E0) <= tol * abs(E0)
     E, F = run((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.zeros((0, 4)), "fp64")
     assert E == 0.0 and F.shape == (0, 3)
     E, F = run((16, 16, 16), (16.0, 16.0, 16.0), 2.0, np.zeros((0, 4)), "mixed")
