@@ -234,15 +234,17 @@ __device__ __forceinline__ void adj_scatter_brick(
       },
       &total);
   const float tscale = exp2f((float)shift);
-  int poff[NPASS], psx[NPASS], psz[NPASS];
+  // (x, z) pairs of the stencil plane each lane tests, the same for every atom
+  int psx[NPASS], psz[NPASS];
 #pragma unroll
   for (int pass = 0; pass < NPASS; pass++) {
     const int p = pass * 32 + lane;
-    const int pz = p < W * W ? p / W : 0, px = p < W * W ? p - (p / W) * W : 0;
-    psx[pass] = px;
-    psz[pass] = pz;
-    poff[pass] = pz * G::PP + px;
+    psz[pass] = p < W * W ? p / W : 0;
+    psx[pass] = p < W * W ? p - (p / W) * W : 0;
   }
+  // per warp: the pairs whose column meets the sphere, packed x | z << 4
+  __shared__ unsigned char plist_all[NW][W * W];
+  unsigned char* plist = plist_all[warp];
   for (int c0 = 0; c0 < total; c0 += kScatterList) {
     brick_atom_list<NT, kSB * kSB>(rng_a, rng_p, total, c0, kScatterList, alist);
     __syncthreads();
@@ -273,21 +275,37 @@ __device__ __forceinline__ void adj_scatter_brick(
         eyuy[k] = ey[k] * __shfl_sync(0xffffffffu, ul[1], k);
         uy2[k] = __shfl_sync(0xffffffffu, u2l[1], k);
       }
-      const float amp = cA * a.w * tscale;
-      int* base = tile + loc[2] * G::PP + loc[1] * G::RP + loc[0];
+      // compact the (x, z) pairs with u_x^2 + u_z^2 < rcut^2: every point of
+      // the other columns lies outside the sphere
+      int npair = 0;
 #pragma unroll
       for (int pass = 0; pass < NPASS; pass++) {
-        const float ex = __shfl_sync(0xffffffffu, el[0], psx[pass]);
-        const float ux = __shfl_sync(0xffffffffu, ul[0], psx[pass]);
         const float ux2 = __shfl_sync(0xffffffffu, u2l[0], psx[pass]);
-        const float ez = __shfl_sync(0xffffffffu, el[2], psz[pass]);
-        const float uz = __shfl_sync(0xffffffffu, ul[2], psz[pass]);
         const float uz2 = __shfl_sync(0xffffffffu, u2l[2], psz[pass]);
-        if (pass * 32 + lane < W * W) {
+        const bool ne = pass * 32 + lane < W * W && ux2 + uz2 < s.rcut2;
+        const unsigned m = __ballot_sync(0xffffffffu, ne);
+        if (ne) plist[npair + __popc(m & ((1u << lane) - 1u))] =
+            (unsigned char)(psx[pass] | (psz[pass] << 4));
+        npair += __popc(m);
+      }
+      __syncwarp();
+      const float amp = cA * a.w * tscale;
+      int* base = tile + loc[2] * G::PP + loc[1] * G::RP + loc[0];
+      for (int i0 = 0; i0 < npair; i0 += 32) {
+        const bool live = i0 + lane < npair;
+        const int pp = live ? plist[i0 + lane] : 0;
+        const int px = pp & 15, pz = pp >> 4;
+        const float ex = __shfl_sync(0xffffffffu, el[0], px);
+        const float ux = __shfl_sync(0xffffffffu, ul[0], px);
+        const float ux2 = __shfl_sync(0xffffffffu, u2l[0], px);
+        const float ez = __shfl_sync(0xffffffffu, el[2], pz);
+        const float uz = __shfl_sync(0xffffffffu, ul[2], pz);
+        const float uz2 = __shfl_sync(0xffffffffu, u2l[2], pz);
+        if (live) {
           const float w = amp * ex * ez;
           const float t1 = w * (Gx * ux + Gz * uz), t2 = w * Gy;
           const float rem = s.rcut2 - (ux2 + uz2);
-          int* cell = base + poff[pass];
+          int* cell = base + pz * G::PP + px;
 #pragma unroll
           for (int k = 0; k < W; k++) {
             if (uy2[k] < rem) {
@@ -299,6 +317,7 @@ __device__ __forceinline__ void adj_scatter_brick(
           }
         }
       }
+      __syncwarp();
     }
     __syncthreads();
   }
