@@ -371,8 +371,8 @@ __device__ __forceinline__ void adj_gather_brick(
     int a0 = 0, a1 = 0;
     if (yy < ey && zz < ez) {
       const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
-      a0 = start[rowkey + x0 / kBinX];
-      a1 = start[rowkey + (x0 + ex - 1) / kBinX + 1];
+      a0 = start[rowkey + (x0 >> b.bxs)];
+      a1 = start[rowkey + ((x0 + ex - 1) >> b.bxs) + 1];
     }
     rng_a[tid] = a0;
     cnt = a1 - a0;

@@ -598,7 +598,7 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_rhok, c->ksize * 2 * c->ct));
   if (!c->fp64) CUC(cudaMalloc(&c->d_fixed, c->size * sizeof(long long)));
   CUC(cudaMalloc(&c->d_counts, sizeof(int) * c->nbins));
-  c->bl = make_bin_layout(M);
+  c->bl = make_bin_layout(M, c->fp64 ? kBinX64 : kBinX32);
   c->nbins2 = bin_count(c->bl);
   CUC(cudaMalloc(&c->d_bcounts, sizeof(int) * c->nbins2));
   CUC(cudaMalloc(&c->d_bstart, sizeof(int) * (c->nbins2 + 1)));

@@ -307,7 +307,7 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
     BatchSys& S = b->sys[k];
     const int M[3] = {y.size_x, y.size_y, y.size_z};
     const double box[3] = {y.box_x, y.box_y, y.box_z};
-    S.b = make_bin_layout(M);
+    S.b = make_bin_layout(M, kBinX32);
     S.bin_off = bin_off;
     if ((long long)bin_off + bin_count(S.b) > 4096LL * 4096LL) {
       delete b;

@@ -1,20 +1,23 @@
 // gse_tiled.cu -- the tiled spread and gather kernels of the GSE-k path.
 //
-//  binning   atoms are counting-sorted by (z cell, y cell, x-bin of kBinX cells)
-//            of their stencil centre round(x/h) mod M, stable in the original
-//            index, so every later sum runs in a fixed order.
-//  spread    CpuGaussCharge::spreadChargeToGrid (CpuGaussCharge.cpp:235-384):
-//            output-stationary.  A CTA owns a kTX x kTY x TZ block of the grid;
-//            each thread owns one (x, y) column of it with TZ accumulators in
-//            registers.  The atoms whose (2n+1)^3 cube reaches the block
-//            stream through shared memory in chunks; each warp keeps the ones
-//            that touch its 8 x 4 column patch and adds their 2n+1 z weights
-//            into its registers.  No atomics; every grid point is written
-//            once.
+//  binning   atoms are counting-sorted by (z cell, y cell, x-bin of 4 or 16 cells)
+//            of their stencil centre round(x/h) mod M; the FP64 form keeps the
+//            original order within a bin so that its sums run in a fixed
+//            order, the mixed form's integer sums need no order.
+//  spread    CpuGaussCharge::spreadChargeToGrid (CpuGaussCharge.cpp:235-384).
+//            FP64 form: output-stationary.  A CTA owns a kTX x kTY x TZ block
+//            of the grid; each thread owns one (x, y) column of it with TZ
+//            accumulators in registers.  The atoms whose (2n+1)^3 cube reaches
+//            the block stream through shared memory in chunks; each warp keeps
+//            the ones that touch its 8 x 4 column patch and adds their 2n+1 z
+//            weights into its registers.  No atomics; every grid point is
+//            written once.  Mixed form: atom-stationary scatter into an int32
+//            shared brick tile, added into an int64 grid (scatter_brick).
 //  gather    CpuGaussCharge::interpolateLoop (CpuGaussCharge.cpp:105-172): a
-//            CTA owns the atoms of a kBG^3-cell brick and stages the potential
-//            of the brick plus its n-cell halo in shared memory; one warp per
-//            atom, lanes over the non-empty (y, z) rows of its sphere.
+//            CTA owns the atoms of a kGX x kGY x kGZ-cell brick and stages the
+//            potential of the brick plus its n-cell halo in shared memory;
+//            kGatherLanes lanes per atom, over the non-empty (y, z) rows of
+//            its sphere.
 #include "gse_internal.cuh"
 #include "gse_tiled.cuh"
 #include "gse_tiled_dev.cuh"
@@ -35,7 +38,7 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
     const int cx = wrap1(centre_cell(a.x, inv_hx), b.M[0]);
     const int cy = wrap1(centre_cell(a.y, inv_hy), b.M[1]);
     const int cz = wrap1(centre_cell(a.z, inv_hz), b.M[2]);
-    const int k = (cz * b.M[1] + cy) * b.nbx + cx / kBinX;
+    const int k = (cz * b.M[1] + cy) * b.nbx + (cx >> b.bxs);
     key[i] = k;
     atomicAdd(&counts[k], 1);
   }
@@ -309,8 +312,8 @@ __global__ void __launch_bounds__(kSpreadThreads)
         const int cu = pmod(u, b.M[0]);
         const int seg_end = min(ux_hi, u + (b.M[0] - cu));  // end of this period
         const int c1 = cu + (seg_end - u);                  // exclusive cell end
-        const int a0 = start[rowkey + cu / kBinX];
-        const int a1 = start[rowkey + (c1 - 1) / kBinX + 1];
+        const int a0 = start[rowkey + (cu >> b.bxs)];
+        const int a1 = start[rowkey + ((c1 - 1) >> b.bxs) + 1];
         seg_a[nseg] = a0;
         seg_e[nseg] = a1;
         seg_sh[nseg] = u - cu;
@@ -630,8 +633,8 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
     int a0 = 0, a1 = 0;
     if (yy < ey && zz < ez) {
       const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
-      a0 = start[rowkey + x0 / kBinX];
-      a1 = start[rowkey + (x0 + ex - 1) / kBinX + 1];
+      a0 = start[rowkey + (x0 >> b.bxs)];
+      a1 = start[rowkey + ((x0 + ex - 1) >> b.bxs) + 1];
     }
     rng_a[tid] = a0;
     cnt = a1 - a0;
@@ -937,7 +940,7 @@ __global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
     const int cx = wrap1(centre_cell(a.x, S.sp.inv_h[0]), S.b.M[0]);
     const int cy = wrap1(centre_cell(a.y, S.sp.inv_h[1]), S.b.M[1]);
     const int cz = wrap1(centre_cell(a.z, S.sp.inv_h[2]), S.b.M[2]);
-    const int k = S.bin_off + (cz * S.b.M[1] + cy) * S.b.nbx + cx / kBinX;
+    const int k = S.bin_off + (cz * S.b.M[1] + cy) * S.b.nbx + (cx >> S.b.bxs);
     key[i] = k;
     atomicAdd(&counts[k], 1);
   }

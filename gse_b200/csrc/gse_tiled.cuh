@@ -9,7 +9,10 @@
 
 namespace gse {
 
-constexpr int kBinX = 4;            // x cells per bin (y and z bins are single cells)
+// x cells per bin (y and z bins are single cells): the FP64 spread reads atom
+// ranges at 4-cell granularity; every mixed-form kernel reads whole 16-cell
+// brick rows, so the mixed form bins 16 cells at a time (4x fewer bins to scan)
+constexpr int kBinX64 = 4, kBinX32 = 16;
 constexpr int kWPad = 16;           // padded stencil width (2n+1 <= 15 on the tiled path)
 constexpr int kTX = 16, kTY = 8;    // spread block columns (x, y)
 constexpr int kTZ32 = 32;           // spread block depth, mixed form (int64 accumulators)
@@ -17,7 +20,7 @@ constexpr int kTZ64 = 24;           // spread block depth, FP64 accumulators
 constexpr int kSpreadThreads = 128; // 4 warps, each an 8 x 4 column patch
 constexpr int kSpreadChunk = 64;    // atoms staged per round
 constexpr int kMaxSeg = 4;          // periodic images of one row segment
-constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX
+constexpr int kGX = 16, kGY = 16, kGZ = 8;  // gather brick (cells); kGX multiple of kBinX32
 constexpr int kGatherThreads = 256;          // >= kGY * kGZ
 constexpr int kGatherLanes = 16;             // lanes sharing one atom in the gather
 constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
@@ -34,7 +37,8 @@ constexpr int kAdjLanes = 32;
 // Atoms sorted by key (z cell, y cell, x bin); start[k] .. start[k+1] is bin k.
 struct BinLayout {
   int M[3];
-  int nbx;  // ceil(Mx / kBinX)
+  int nbx;    // ceil(Mx / bin width)
+  int bxs;    // log2 of the bin width in x cells
 };
 
 struct BinScratch {
@@ -63,12 +67,15 @@ inline Decay<CT> make_decay(const Stencil<CT>& s) {
   return d;
 }
 
-inline BinLayout make_bin_layout(const int M[3]) {
+inline BinLayout make_bin_layout(const int M[3], int bin_width) {
   BinLayout b;
   for (int d = 0; d < 3; d++) b.M[d] = M[d];
-  b.nbx = (M[0] + kBinX - 1) / kBinX;
+  b.bxs = bin_width == 16 ? 4 : 2;
+  b.nbx = (M[0] + (1 << b.bxs) - 1) >> b.bxs;
   return b;
 }
+static_assert(kGX % kBinX32 == 0 && kSB % kBinX32 == 0 && kAX % kBinX32 == 0,
+              "mixed-form bricks start on bin boundaries");
 
 inline int bin_count(const BinLayout& b) { return b.M[1] * b.M[2] * b.nbx; }
 

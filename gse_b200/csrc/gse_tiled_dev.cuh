@@ -85,8 +85,8 @@ __device__ __forceinline__ int brick_prologue(const int* __restrict__ start, con
     const int yy = tid % kSB, zz = tid / kSB;
     if (yy < ey && zz < ez) {
       const int rowkey = ((z0 + zz) * b.M[1] + (y0 + yy)) * b.nbx;
-      a0 = start[rowkey + x0 / kBinX];
-      cnt = start[rowkey + (x0 + ex - 1) / kBinX + 1] - a0;
+      a0 = start[rowkey + (x0 >> b.bxs)];
+      cnt = start[rowkey + ((x0 + ex - 1) >> b.bxs) + 1] - a0;
     }
   }
   const int pos = block_exclusive_scan(cnt, total);
