@@ -60,7 +60,7 @@ gse_status_t fail(gse_status_t s, const char* fmt, ...) {
     if (_s != GSE_OK) return _s;                                                            \
   } while (0)
 
-constexpr int kEnergyPartials = 148 * 4;
+constexpr int kEnergyPartials = 148 * 16;  // blocks of the energy reductions (+1 counter slot)
 constexpr int kBrick = 4;
 
 bool is_device_ptr(const void* p) {
@@ -433,7 +433,7 @@ gse_status_t do_solve_ctx(gse_context_t* c) {
   }
   {
     StageTimer tm(c, GSE_STAGE_GREEN);
-    c->launches += 2;
+    c->launches += 1;
     if (c->fp64)
       CU(launch_green_apply<double>((double2*)c->d_rhok, (const double*)c->d_gtab, g,
                                     c->d_partials, kEnergyPartials, energy_factor(c),
@@ -605,7 +605,8 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_btiles, sizeof(int) * (c->nbins2 / 4096 + 2)));
   CUC(cudaMalloc(&c->d_qmax, sizeof(unsigned)));
   CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
-  CUC(cudaMalloc(&c->d_partials, sizeof(double) * kEnergyPartials));
+  CUC(cudaMalloc(&c->d_partials, sizeof(double) * (kEnergyPartials + 1)));
+  CUC(cudaMemset(c->d_partials, 0, sizeof(double) * (kEnergyPartials + 1)));
   CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 4));
   CUC(cudaMalloc(&c->d_bad, sizeof(int)));
   CUC(cudaMemset(c->d_bad, 0, sizeof(int)));

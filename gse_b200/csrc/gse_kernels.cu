@@ -252,10 +252,15 @@ __global__ void k_green_table(GreenGeom g, CT* __restrict__ tab) {
 
 // rhok *= G (table) with the energy sum_k G |rho(k)|^2 over the full
 // spectrum: every bin counts twice except kx = 0 and the kx Nyquist bin.
+// Each block leaves its partial sum in partials[blockIdx.x]; the block that
+// finishes last (a counter in partials[gridDim.x], zero between launches)
+// adds the partials in index order, so the energy does not depend on which
+// block ran when, and writes factor * sum to energy_out.
 template <typename CT>
 __global__ void __launch_bounds__(256)
     k_green_apply(typename Cplx<CT>::type* __restrict__ rhok, const CT* __restrict__ tab,
-                  GreenGeom g, double* __restrict__ partials) {
+                  GreenGeom g, double* __restrict__ partials, double factor,
+                  double* __restrict__ energy_out) {
   const unsigned total = (unsigned)g.sizeX * g.nfft[1] * g.nfft[2];
   const unsigned sx = (unsigned)g.sizeX;
   const unsigned nyq = g.nx_even ? (unsigned)(g.nfft[0] / 2) : 0xffffffffu;
@@ -273,6 +278,31 @@ __global__ void __launch_bounds__(256)
     rhok[idx] = v;
   }
   block_sum_to(e, partials);
+  __shared__ bool last;
+  unsigned* done = reinterpret_cast<unsigned*>(partials + gridDim.x);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;  // uniform in the block
+  __threadfence();
+  __shared__ double red[32];
+  double t = 0.0;
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+    t += ((volatile double*)partials)[i];
+  t = warp_sum(t);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = t;
+  __syncthreads();
+  if (w == 0) {
+    double u = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    u = warp_sum(u);
+    if (lane == 0) {
+      energy_out[0] = u * factor;
+      *done = 0u;
+    }
+  }
 }
 
 // sum_i (double)(a[i]*b[i]) per block (the product in CT, as CpuGSE.cpp:97)
@@ -447,8 +477,7 @@ template <typename CT>
 cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
                                double* partials, int np, double factor, double* energy_out,
                                cudaStream_t st) {
-  k_green_apply<CT><<<np, 256, 0, st>>>(rhok, tab, g, partials);
-  k_energy_finalize<<<1, 1024, 0, st>>>(partials, np, factor, energy_out);
+  k_green_apply<CT><<<np, 256, 0, st>>>(rhok, tab, g, partials, factor, energy_out);
   return cudaGetLastError();
 }
 
