@@ -547,37 +547,23 @@ __device__ __forceinline__ bool in_sphere<float>(float dx2, float, float, float 
 }
 
 // s0 = sum_k m_k wx[k] row[k], s1 = sum_k m_k wx[k] dx[k] row[k] over the
-// 2n+1 points of one stencil row, m_k the sphere test.
+// 2n+1 points of one stencil row, m_k the sphere test.  The test guards the
+// two fmas (predicated, no select); a skipped point adds exactly nothing.
 template <typename CT, int W>
 __device__ __forceinline__ void row_sums(const CT* row, const CT (&dx2)[W], const CT (&wx)[W],
                                          const CT (&wdx)[W], CT dy2, CT dz2, CT rem, CT rcut2,
                                          CT& s0, CT& s1) {
-  s0 = (CT)0;
-  s1 = (CT)0;
+  CT a = (CT)0, c = (CT)0;
 #pragma unroll
   for (int k = 0; k < W; k++) {
-    const CT ph = in_sphere<CT>(dx2[k], dy2, dz2, rem, rcut2) ? row[k] : (CT)0;
-    s0 = fma(wx[k], ph, s0);
-    s1 = fma(wdx[k], ph, s1);
+    const CT ph = row[k];
+    if (in_sphere<CT>(dx2[k], dy2, dz2, rem, rcut2)) {
+      a = fma(wx[k], ph, a);
+      c = fma(wdx[k], ph, c);
+    }
   }
-}
-
-// FP32: both sums in one packed fma.rn.f32x2 per point (sm_100).
-template <>
-__device__ __forceinline__ void row_sums<float, 13>(const float* row, const float (&dx2)[13],
-                                                    const float (&wx)[13], const float (&wdx)[13],
-                                                    float, float, float rem, float, float& s0,
-                                                    float& s1) {
-  unsigned long long acc = 0ull;  // (s0, s1) packed, both +0.0f
-#pragma unroll
-  for (int k = 0; k < 13; k++) {
-    const float ph = dx2[k] < rem ? row[k] : 0.f;
-    unsigned long long w2, p2;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(w2) : "f"(wx[k]), "f"(wdx[k]));
-    asm("mov.b64 %0, {%1, %1};" : "=l"(p2) : "f"(ph));
-    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2), "l"(p2));
-  }
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(acc));
+  s0 = a;
+  s1 = c;
 }
 
 // Shared memory of the gather for calculation type CT and stencil width W:
