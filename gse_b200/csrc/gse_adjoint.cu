@@ -474,11 +474,12 @@ __device__ __forceinline__ void adj_gather_brick(
         nrow += __popc(m);
       }
       __syncwarp();
-      float dx2[W], eu2[W];
+      float dx2[W], ex[W], eux[W], eu2[W];
 #pragma unroll
       for (int k = 0; k < W; k++) {
         dx2[k] = tb[(0 * 3 + 1) * kWPad + k];
-        eu2[k] = tb[(0 * 3 + 2) * kWPad + k] * dx2[k];
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(ex[k]), "=f"(eux[k]) : "l"(w2[k]));
+        eu2[k] = ex[k] * dx2[k];
       }
       double T0 = 0, T1x = 0, T1y = 0, T1z = 0;
       double Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
@@ -488,18 +489,16 @@ __device__ __forceinline__ void adj_gather_brick(
         const float uy2 = tb[(1 * 3 + 1) * kWPad + jy], uz2 = tb[(2 * 3 + 1) * kWPad + jz];
         const float rem = sg.rcut2 - (uy2 + uz2);
         const float* row = tphi + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
-        unsigned long long acc = 0ull;
-        float s2 = 0.f;
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
         for (int k = 0; k < W; k++) {
-          const float ph = dx2[k] < rem ? row[k] : 0.f;
-          unsigned long long p2;
-          asm("mov.b64 %0, {%1, %1};" : "=l"(p2) : "f"(ph));
-          asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(w2[k]), "l"(p2));
-          s2 = fmaf(eu2[k], ph, s2);
+          const float ph = row[k];
+          if (dx2[k] < rem) {  // the test guards the fmas; a skipped point adds nothing
+            s0 = fmaf(ex[k], ph, s0);
+            s1 = fmaf(eux[k], ph, s1);
+            s2 = fmaf(eu2[k], ph, s2);
+          }
         }
-        float s0, s1;
-        asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(acc));
         const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
         const float uy = tb[(1 * 3 + 0) * kWPad + jy], uz = tb[(2 * 3 + 0) * kWPad + jz];
         const float a0 = w * s0, a1 = w * s1;
