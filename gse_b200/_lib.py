@@ -19,6 +19,7 @@ STATUS_NAMES = {
     8: "GSE_ERR_NONFINITE",
 }
 PRECISION = {"fp64": 0, "mixed": 1}
+PATH_TILED, PATH_GREEN_IN_FFT, PATH_GRAPH = 1, 2, 4
 GRID_RHO = 0
 GRID_PHI = 1
 
@@ -93,6 +94,7 @@ SIGNATURES = {
     "gse_spread_mixed_noalloc": (_i, [_i, _i, _i, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp]),
     "gse_adjoint": (_i, [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gse_ewald_recip": (_i, [_i, _vp, _d, _i, _d, _d, _d, _d, _i, _vp, _vp, _vp, _vp, _vp]),
+    "gse_get_paths": (_i, [_vp, ctypes.POINTER(_i)]),
     "gse_batch_create": (_i, [ctypes.POINTER(gse_params_t), _i, ctypes.POINTER(gse_system_t),
                               ctypes.POINTER(_vp)]),
     "gse_batch_destroy": (_i, [_vp]),

@@ -25,9 +25,32 @@ def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+CB_SRC = os.path.join(CSRC, "cufft_cb", "gse_green_cb.cu")
+GEN = os.path.join(PKG, "_gen")
+CB_HEADER = os.path.join(GEN, "gse_green_cb_fatbin.h")
+
+
 def _deps():
     return (_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
-            glob.glob(os.path.join(INCLUDE, "*.h")) + [os.path.abspath(__file__)])
+            glob.glob(os.path.join(INCLUDE, "*.h")) + [os.path.abspath(__file__), CB_SRC])
+
+
+def build_callbacks(verbose: bool = False) -> None:
+    """The cuFFT load callbacks as LTO code, embedded in a generated header
+    (an array the library passes to cufftXtSetJITCallback)."""
+    os.makedirs(GEN, exist_ok=True)
+    fatbin = os.path.join(GEN, "gse_green_cb.fatbin")
+    cmd = [NVCC, "-gencode", "arch=compute_100a,code=lto_100a", "-dc", "-fatbin", "-O3",
+           "-std=c++17", CB_SRC, "-o", fatbin]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    out = subprocess.run([os.path.join(CUDA_HOME, "bin", "bin2c"), "--name", "gse_green_cb_fatbin",
+                          "--type", "char", fatbin], check=True, capture_output=True, text=True)
+    with open(CB_HEADER + ".tmp", "w") as f:
+        f.write("// generated by gse_b200/build.py from csrc/cufft_cb/gse_green_cb.cu\n")
+        f.write(out.stdout)
+    os.replace(CB_HEADER + ".tmp", CB_HEADER)
 
 
 def _stale(target, deps):
@@ -38,7 +61,8 @@ def _stale(target, deps):
 
 
 def nvcc_cmd(out=LIB):
-    return ([NVCC] + ARCH + NVCC_FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC] + _sources() +
+    return ([NVCC] + ARCH + NVCC_FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC, "-I", GEN] +
+            _sources() +
             ["-o", out, "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft",
              "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")])
 
@@ -48,6 +72,7 @@ def build_lib(force: bool = False, verbose: bool = False) -> str:
         return LIB
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
+    build_callbacks(verbose)
     tmp = LIB + ".tmp"
     cmd = nvcc_cmd(tmp)
     if verbose:

@@ -6,6 +6,7 @@
 // the FFTW plans of CpuFFTSolver.cpp:28-69), and staging buffers for atoms
 // and forces.
 #include <cufft.h>
+#include <cufftXt.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -20,6 +21,7 @@
 #include "gse_adjoint.cuh"
 #include "gse_ewald.cuh"
 #include "gse_tiled.cuh"
+#include "gse_green_cb_fatbin.h"  // generated: the c2r load callbacks as LTO code
 
 using namespace gse;
 
@@ -123,6 +125,11 @@ struct gse_context {
   double* h_pinned = nullptr;  // [0] energy, [1] bad flag
   cufftHandle plan_f = 0, plan_b = 0;
   bool plans = false;
+  // c2r plan whose load callback multiplies by the Green's table (the solve
+  // of the context's own sigma2 and box; plan_b stays plain for the others)
+  cufftHandle plan_bg = 0;
+  bool green_cb = false;     // plan_bg exists and is used
+  bool green_cb_tried = false;
   bool rho_valid = false, phi_valid = false, energy_valid = false;
   // replay of repeated gse_forward calls with device inputs and outputs: the
   // second identical call is captured into a CUDA graph, later ones launch it
@@ -417,10 +424,47 @@ gse_status_t do_solve(gse_context_t* c, const void* rho, void* phi, double sigma
 
 // The context's own solve (sigma2, context box) with the tabulated Green's
 // function: r2c -> multiply + energy -> c2r.
+// Grids from this size on use the callback plan: its cuFFT link step takes
+// about half a second once per context, which smaller grids do not earn back.
+constexpr long long kGreenCallbackMinPoints = 64LL * 64 * 64;
+
+// The context's c2r plan with the Green multiply as a load callback (cuFFT's
+// link-time callbacks).  false: the callback plan is not available here and
+// the solve keeps its separate multiply kernel.
+bool make_green_callback_plan(gse_context_t* c) {
+  cufftHandle pl = 0;
+  if (cufftCreate(&pl) != CUFFT_SUCCESS) return false;
+  const char* sym = c->fp64 ? "gse_green_load_z" : "gse_green_load_c";
+  size_t ws = 0;
+  const bool ok =
+      cufftXtSetJITCallback(pl, sym, gse_green_cb_fatbin, sizeof(gse_green_cb_fatbin),
+                            c->fp64 ? CUFFT_CB_LD_COMPLEX_DOUBLE : CUFFT_CB_LD_COMPLEX,
+                            &c->d_gtab) == CUFFT_SUCCESS &&
+      cufftMakePlan3d(pl, c->p.size_z, c->p.size_y, c->p.size_x,
+                      c->fp64 ? CUFFT_Z2D : CUFFT_C2R, &ws) == CUFFT_SUCCESS &&
+      cufftSetStream(pl, c->stream) == CUFFT_SUCCESS;
+  if (!ok) {
+    cufftDestroy(pl);
+    cudaGetLastError();
+    return false;
+  }
+  c->plan_bg = pl;
+  return true;
+}
+
 gse_status_t do_solve_ctx(gse_context_t* c) {
   const GreenGeom g = green_geom(c, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true);
+  if (!c->d_gtab) CU(cudaMalloc(&c->d_gtab, c->ksize * c->ct));  // fixed address from here on
+  if (!c->green_cb_tried && c->size >= kGreenCallbackMinPoints) {
+    // linked once, on the first solve outside any stream capture
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+      c->green_cb = make_green_callback_plan(c);
+      c->green_cb_tried = true;
+    }
+    cudaGetLastError();
+  }
   if (!c->gtab_valid) {
-    if (!c->d_gtab) CU(cudaMalloc(&c->d_gtab, c->ksize * c->ct));
     if (c->fp64)
       CU(launch_green_table<double>(g, (double*)c->d_gtab, c->stream));
     else
@@ -430,6 +474,28 @@ gse_status_t do_solve_ctx(gse_context_t* c) {
   {
     StageTimer tm(c, GSE_STAGE_FFT_FORWARD);
     TRY(fft_forward(c, c->d_rho, c->d_rhok));
+  }
+  if (c->green_cb) {
+    // Green multiply inside the c2r (load callback); the energy then as the
+    // reference computes it, 1/2 ccelec h^3 sum rho phi (CpuGSE.cpp:86-103)
+    {
+      StageTimer tm(c, GSE_STAGE_FFT_BACKWARD);
+      if (c->fp64)
+        CUFFT(cufftExecZ2D(c->plan_bg, (cufftDoubleComplex*)c->d_rhok, (cufftDoubleReal*)c->d_phi));
+      else
+        CUFFT(cufftExecC2R(c->plan_bg, (cufftComplex*)c->d_rhok, (cufftReal*)c->d_phi));
+    }
+    StageTimer tm(c, GSE_STAGE_GREEN);
+    c->launches += 1;
+    if (c->fp64)
+      CU(launch_dot_energy<double>((const double*)c->d_rho, (const double*)c->d_phi, c->size,
+                                   c->d_partials, kEnergyPartials, energy_factor(c),
+                                   c->d_scalars, c->stream));
+    else
+      CU(launch_dot_energy<float>((const float*)c->d_rho, (const float*)c->d_phi, c->size,
+                                  c->d_partials, kEnergyPartials, energy_factor(c),
+                                  c->d_scalars, c->stream));
+    return GSE_OK;
   }
   {
     StageTimer tm(c, GSE_STAGE_GREEN);
@@ -633,6 +699,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
     cufftDestroy(c->plan_f);
     cufftDestroy(c->plan_b);
   }
+  if (c->green_cb) cufftDestroy(c->plan_bg);
   cudaFree(c->d_rho);
   cudaFree(c->d_phi);
   cudaFree(c->d_rhok);
@@ -670,6 +737,7 @@ gse_status_t gse_set_stream(gse_context_t* c, void* stream) {
   c->stream = (cudaStream_t)stream;
   CUFFT(cufftSetStream(c->plan_f, c->stream));
   CUFFT(cufftSetStream(c->plan_b, c->stream));
+  if (c->green_cb) CUFFT(cufftSetStream(c->plan_bg, c->stream));
   return GSE_OK;
 }
 
@@ -993,6 +1061,20 @@ gse_status_t gse_set_timing(gse_context_t* c, int enable) {
     for (int i = 0; i < GSE_NUM_STAGES; i++) harvest(c, i);
   }
   c->timing = enable != 0;
+  return GSE_OK;
+}
+
+gse_status_t gse_get_paths(gse_context_t* c, int* flags) {
+  TRY(check_ctx(c));
+  if (!flags) return fail(GSE_ERR_INVALID_ARG, "NULL flags");
+  const Box3 box = ctx_box(c);
+  int f = 0;
+  if (c->fp64 ? tiled_ok<double>(c, stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false))
+              : tiled_ok<float>(c, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false)))
+    f |= GSE_PATH_TILED;
+  if (c->green_cb) f |= GSE_PATH_GREEN_IN_FFT;
+  if (c->fwd_exec) f |= GSE_PATH_GRAPH;
+  *flags = f;
   return GSE_OK;
 }
 

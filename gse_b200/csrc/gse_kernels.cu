@@ -179,6 +179,38 @@ __device__ __forceinline__ void block_sum_to(double v, double* partials) {
   }
 }
 
+// After block_sum_to: the block that finishes last (a counter in
+// partials[gridDim.x], zero between launches) adds the partials in index
+// order -- the result does not depend on which block ran when -- and writes
+// factor * sum to out[0].
+__device__ __forceinline__ void last_block_sum(double* partials, double factor, double* out) {
+  __shared__ bool last;
+  unsigned* done = reinterpret_cast<unsigned*>(partials + gridDim.x);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;  // uniform in the block
+  __threadfence();
+  __shared__ double red[32];
+  double t = 0.0;
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+    t += ((volatile double*)partials)[i];
+  t = warp_sum(t);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = t;
+  __syncthreads();
+  if (w == 0) {
+    double u = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+    u = warp_sum(u);
+    if (lane == 0) {
+      out[0] = u * factor;
+      *done = 0u;
+    }
+  }
+}
+
 // Green's-function multiply on the r2c half spectrum [nz][ny][nx/2+1],
 // CpuGreensFuncGSE.cpp:28-56, with the energy sum_k G |rho(k)|^2 over the
 // full spectrum (the half-spectrum bins kx = 1 .. ceil(nx/2)-1 stand for two
@@ -252,10 +284,7 @@ __global__ void k_green_table(GreenGeom g, CT* __restrict__ tab) {
 
 // rhok *= G (table) with the energy sum_k G |rho(k)|^2 over the full
 // spectrum: every bin counts twice except kx = 0 and the kx Nyquist bin.
-// Each block leaves its partial sum in partials[blockIdx.x]; the block that
-// finishes last (a counter in partials[gridDim.x], zero between launches)
-// adds the partials in index order, so the energy does not depend on which
-// block ran when, and writes factor * sum to energy_out.
+// The energy is finished in the kernel by its last block (last_block_sum).
 template <typename CT>
 __global__ void __launch_bounds__(256)
     k_green_apply(typename Cplx<CT>::type* __restrict__ rhok, const CT* __restrict__ tab,
@@ -278,43 +307,21 @@ __global__ void __launch_bounds__(256)
     rhok[idx] = v;
   }
   block_sum_to(e, partials);
-  __shared__ bool last;
-  unsigned* done = reinterpret_cast<unsigned*>(partials + gridDim.x);
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!last) return;  // uniform in the block
-  __threadfence();
-  __shared__ double red[32];
-  double t = 0.0;
-  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
-    t += ((volatile double*)partials)[i];
-  t = warp_sum(t);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) red[w] = t;
-  __syncthreads();
-  if (w == 0) {
-    double u = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
-    u = warp_sum(u);
-    if (lane == 0) {
-      energy_out[0] = u * factor;
-      *done = 0u;
-    }
-  }
+  last_block_sum(partials, factor, energy_out);
 }
 
-// sum_i (double)(a[i]*b[i]) per block (the product in CT, as CpuGSE.cpp:97)
+// factor * sum_i (double)(a[i]*b[i]) (the product in CT, as CpuGSE.cpp:97),
+// finished by the last block
 template <typename CT>
 __global__ void __launch_bounds__(256)
     k_dot(const CT* __restrict__ a, const CT* __restrict__ b, long long size,
-          double* __restrict__ partials) {
+          double* __restrict__ partials, double factor, double* __restrict__ out) {
   double e = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
        i += (long long)gridDim.x * blockDim.x)
     e += (double)(a[i] * b[i]);
   block_sum_to(e, partials);
+  last_block_sum(partials, factor, out);
 }
 
 __global__ void k_energy_finalize(const double* __restrict__ partials, int np, double factor,
@@ -484,8 +491,7 @@ cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, con
 template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st) {
-  k_dot<CT><<<np, 256, 0, st>>>(a, b, size, partials);
-  k_energy_finalize<<<1, 1024, 0, st>>>(partials, np, factor, energy_out);
+  k_dot<CT><<<np, 256, 0, st>>>(a, b, size, partials, factor, energy_out);
   return cudaGetLastError();
 }
 

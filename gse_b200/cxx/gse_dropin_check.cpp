@@ -35,6 +35,9 @@ int run(int M[3], double L[3], double sigma, const std::vector<double>& raw) {
   gse.solvePoisson();
   const double E = gse.calculateEnergy();
   gse.interpolateForce(n, xyzq.data(), fx.data(), fy.data(), fz.data());
+  int paths = 0;
+  gse_b200::check(gse_get_paths(gse.context(), &paths));
+  printf("PATHS %d\n", paths);
   printf("E %.17g\n", E);
   for (int i = 0; i < n; i++) printf("F %.17g %.17g %.17g\n", fx[i], fy[i], fz[i]);
 

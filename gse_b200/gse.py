@@ -142,6 +142,12 @@ class Context:
         check(self._L.gse_adjoint(self.h, int(n), ptr(xyzq), float(dLdE), ptr(gfx), ptr(gfy),
                                   ptr(gfz), ptr(dq), ptr(dx), ptr(dy), ptr(dz)))
 
+    def paths(self) -> int:
+        """Bits of the implementation paths taken (_lib.PATH_*)."""
+        f = ctypes.c_int()
+        check(self._L.gse_get_paths(self.h, ctypes.byref(f)))
+        return f.value
+
     def set_timing(self, enable: bool):
         check(self._L.gse_set_timing(self.h, int(bool(enable))))
 

@@ -223,6 +223,24 @@ gse_status_t gse_get_timing(gse_context_t* ctx, double* ms_total, long long* cou
  * (library calls such as cuFFT's are not counted). */
 gse_status_t gse_get_launch_count(gse_context_t* ctx, long long* launches);
 
+/* Which implementation paths the context takes (bits of *flags):
+ *  GSE_PATH_TILED        brick-tiled spread and gather (grids >= 10 points per
+ *                        side, stencil widths 9-15); otherwise atom-parallel kernels
+ *  GSE_PATH_GREEN_IN_FFT the Green's-function multiply runs inside the c2r
+ *                        transform as a cuFFT load callback, linked on the
+ *                        context's first solve (grids of 64^3 points or more,
+ *                        when the process's cuFFT and nvJitLink accept the
+ *                        callback code -- not when an older cuFFT, such as the
+ *                        one bundled with PyTorch, was loaded first); the energy
+ *                        is then 1/2 ccelec h^3 sum rho phi in real space.
+ *                        Otherwise a separate multiply kernel that also sums
+ *                        the energy in k-space
+ *  GSE_PATH_GRAPH        repeated gse_forward calls replay a captured CUDA graph */
+#define GSE_PATH_TILED 1
+#define GSE_PATH_GREEN_IN_FFT 2
+#define GSE_PATH_GRAPH 4
+gse_status_t gse_get_paths(gse_context_t* ctx, int* flags);
+
 /* ---- spreading without allocation ------------------------------------- */
 
 /* Largest grid (size_x*size_y*size_z points) gse_spread_mixed_noalloc takes. */

@@ -32,6 +32,8 @@ def parse(text):
     F, Fs = [], []
     for line in text.splitlines():
         tag, *vals = line.split()
+        if tag == "PATHS":
+            continue
         if tag == "E":
             E = float(vals[0])
         elif tag == "E_stages":
@@ -75,3 +77,25 @@ def test_dropin_classes_match_reference(goldens, tmp_path, case, precision, tol)
     assert rms(F, Fref) <= tol
     assert abs(Es - Eref) <= tol * abs(Eref)
     assert rms(Fs, Fref) <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
+def test_dropin_64cubed_green_multiply_inside_the_fft(tmp_path, precision, tol):
+    """A process without PyTorch links the Green's multiply into the c2r
+    transform (cuFFT load callback) for grids of 64^3 points and more; the
+    23,559-charge water box (M = 64) checks that path against the reference."""
+    from conftest import GOLDEN
+    from gse_b200 import workloads as W
+    z = np.load(os.path.join(GOLDEN, "water_23559.npz"))
+    s = W.config_water_23k()
+    g = {"M": np.array(s.grid), "box": np.array(s.boxes), "sigma": np.array(s.sigma),
+         "xyzq": s.xyzq.astype(np.float64)}
+    out = run(program(), precision, g, tmp_path)
+    assert out.returncode == 0, out.stderr
+    paths = int([ln for ln in out.stdout.splitlines() if ln.startswith("PATHS")][0].split()[1])
+    assert paths & 2, "Green's multiply not inside the FFT"
+    E, F, Es, Fs = parse(out.stdout)
+    print(precision, abs(E - float(z["E"])) / abs(float(z["E"])), rms(F, z["F"]))
+    assert abs(E - float(z["E"])) <= tol * abs(float(z["E"]))
+    assert rms(F, z["F"]) <= tol
