@@ -294,17 +294,41 @@ __global__ void __launch_bounds__(256)
   const unsigned sx = (unsigned)g.sizeX;
   const unsigned nyq = g.nx_even ? (unsigned)(g.nfft[0] / 2) : 0xffffffffu;
   double e = 0.0;
-  for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += gridDim.x * blockDim.x) {
-    auto v = rhok[idx];
-    const CT f = tab[idx];
-    const unsigned ix = idx % sx;
+  auto bin = [&](typename Cplx<CT>::type& v, CT f, unsigned ix) {
     const double re = (double)v.x, im = (double)v.y;
     const double wgt = (ix == 0 || ix == nyq) ? 1.0 : 2.0;
     e += wgt * (double)f * (re * re + im * im);
     v.x *= f;
     v.y *= f;
-    rhok[idx] = v;
+  };
+  if constexpr (sizeof(CT) == 4) {
+    // two bins per thread and step: one 16-byte load of rho(k), one 8-byte
+    // load of G (cudaMalloc'd buffers, even bin index)
+    const unsigned pairs = total / 2;
+    float4* r4 = reinterpret_cast<float4*>(rhok);
+    const float2* t2 = reinterpret_cast<const float2*>(tab);
+    for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < pairs;
+         j += gridDim.x * blockDim.x) {
+      float4 w = r4[j];
+      const float2 f = t2[j];
+      const unsigned ix0 = (2 * j) % sx, ix1 = ix0 + 1 == sx ? 0 : ix0 + 1;
+      float2 a = make_float2(w.x, w.y), b = make_float2(w.z, w.w);
+      bin(a, f.x, ix0);
+      bin(b, f.y, ix1);
+      r4[j] = make_float4(a.x, a.y, b.x, b.y);
+    }
+    if ((total & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+      auto v = rhok[total - 1];
+      bin(v, tab[total - 1], (total - 1) % sx);
+      rhok[total - 1] = v;
+    }
+  } else {
+    for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += gridDim.x * blockDim.x) {
+      auto v = rhok[idx];
+      bin(v, tab[idx], idx % sx);
+      rhok[idx] = v;
+    }
   }
   block_sum_to(e, partials);
   last_block_sum(partials, factor, energy_out);
@@ -317,9 +341,27 @@ __global__ void __launch_bounds__(256)
     k_dot(const CT* __restrict__ a, const CT* __restrict__ b, long long size,
           double* __restrict__ partials, double factor, double* __restrict__ out) {
   double e = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
-       i += (long long)gridDim.x * blockDim.x)
-    e += (double)(a[i] * b[i]);
+  if constexpr (sizeof(CT) == 4) {
+    // four points per thread and step, 16-byte loads (cudaMalloc'd grids)
+    const long long quads = size / 4;
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < quads;
+         i += (long long)gridDim.x * blockDim.x) {
+      const float4 u = a4[i], v = b4[i];
+      e += (double)(u.x * v.x);
+      e += (double)(u.y * v.y);
+      e += (double)(u.z * v.z);
+      e += (double)(u.w * v.w);
+    }
+    if (blockIdx.x == 0)
+      for (long long i = quads * 4 + threadIdx.x; i < size; i += blockDim.x)
+        e += (double)(a[i] * b[i]);
+  } else {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
+         i += (long long)gridDim.x * blockDim.x)
+      e += (double)(a[i] * b[i]);
+  }
   block_sum_to(e, partials);
   last_block_sum(partials, factor, out);
 }
