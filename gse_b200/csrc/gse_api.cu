@@ -122,7 +122,11 @@ struct gse_context {
   double* d_partials = nullptr;
   double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch
   int* d_bad = nullptr;
-  double* h_pinned = nullptr;  // [0] energy, [1] bad flag
+  double* h_pinned = nullptr;  // [0] energy
+  // set by the binning when a position or charge is not finite; host memory
+  // mapped into the device, so reading it after a synchronisation costs no copy
+  volatile int* h_bad = nullptr;
+  int* d_badmap = nullptr;
   cufftHandle plan_f = 0, plan_b = 0;
   bool plans = false;
   // c2r plan whose load callback multiplies by the Green's table (the solve
@@ -293,7 +297,8 @@ template <typename CT>
 gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s) {
   typedef typename Vec4<CT>::type V;
   StageTimer tm(c, GSE_STAGE_BIN);
-  BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax};
+  BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax,
+               c->d_badmap};
   c->launches += n > 0 ? 6 : 3;
   CU(launch_bin_sorted<CT>((const V*)dx, n, c->bl, s.inv_h[0], s.inv_h[1], s.inv_h[2], w,
                            (V*)c->d_sorted, c->d_perm, c->stream));
@@ -522,8 +527,21 @@ gse_status_t copy_out(gse_context_t* c, void* dst, const void* src, size_t bytes
   return GSE_OK;
 }
 
+// After a synchronisation: report (once) non-finite inputs seen since the
+// last report.
+gse_status_t check_finite(gse_context_t* c) {
+  if (c->h_bad && *c->h_bad) {
+    *c->h_bad = 0;
+    return fail(GSE_ERR_NONFINITE, "a position or charge is NaN or infinite");
+  }
+  return GSE_OK;
+}
+
 gse_status_t finish(gse_context_t* c, bool host_outputs) {
-  if (host_outputs) CU(cudaStreamSynchronize(c->stream));
+  if (host_outputs) {
+    CU(cudaStreamSynchronize(c->stream));
+    TRY(check_finite(c));
+  }
   CU(cudaGetLastError());
   return GSE_OK;
 }
@@ -678,6 +696,13 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMemset(c->d_bad, 0, sizeof(int)));
   CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 4));
   CUC(cudaMallocHost(&c->h_pinned, sizeof(double) * 4));
+  {
+    int* hb = nullptr;
+    CUC(cudaHostAlloc(&hb, sizeof(int), cudaHostAllocMapped));
+    *hb = 0;
+    c->h_bad = hb;
+    CUC(cudaHostGetDevicePointer((void**)&c->d_badmap, hb, 0));
+  }
 #undef CUC
   if (cufftPlan3d(&c->plan_f, p.size_z, p.size_y, p.size_x, c->fp64 ? CUFFT_D2Z : CUFFT_R2C) !=
           CUFFT_SUCCESS ||
@@ -723,6 +748,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_partials);
   cudaFree(c->d_scalars);
   cudaFree(c->d_bad);
+  if (c->h_bad) cudaFreeHost((void*)c->h_bad);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   for (int i = 0; i < GSE_NUM_STAGES; i++)
     for (int j = 0; j < 2; j++)
@@ -761,7 +787,7 @@ gse_status_t gse_set_box(gse_context_t* c, double bx, double by, double bz) {
 gse_status_t gse_synchronize(gse_context_t* c) {
   TRY(check_ctx(c));
   CU(cudaStreamSynchronize(c->stream));
-  return GSE_OK;
+  return check_finite(c);
 }
 
 gse_status_t gse_spread_charge(gse_context_t* c, int n, const void* xyzq) {

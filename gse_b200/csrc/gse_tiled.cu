@@ -30,10 +30,13 @@ namespace gse {
 template <typename CT>
 __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, int n, BinLayout b,
                             CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
-                            int* __restrict__ counts, unsigned* __restrict__ qmax_bits) {
+                            int* __restrict__ counts, unsigned* __restrict__ qmax_bits,
+                            int* __restrict__ bad) {
   float qm = 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const auto a = xyzq[i];
+    if (bad && !(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(a.w)))
+      *bad = 1;  // the bin below is still in range (wrap1 of any int)
     qm = fmaxf(qm, fabsf((float)a.w));
     const int cx = wrap1(centre_cell(a.x, inv_hx), b.M[0]);
     const int cy = wrap1(centre_cell(a.y, inv_hy), b.M[1]);
@@ -760,7 +763,7 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
   const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
-                                        qmax);
+                                        qmax, w.bad);
   return launch_bin_scan_place<CT>(xyzq, n, nb, w, sorted, perm, st);
 }
 

@@ -48,6 +48,7 @@ struct BinScratch {
   int* tile_sums;  // [ceil(nbins / 4096)]
   int* tmp;        // [n]
   unsigned* qmax_bits;  // max |q| over the atoms (float bits), written by the binning
+  int* bad = nullptr;   // set to 1 when a position or charge is not finite (may be NULL)
 };
 
 // exp(-2 h^2 / (2 sigma^2)) per axis as an unevaluated sum hi + lo in CT

@@ -46,7 +46,9 @@ typedef enum gse_status {
   GSE_ERR_TIMEOUT = 5,           /* a bounded device-side wait gave up */
   GSE_ERR_NOT_READY = 6,         /* stage called out of order (e.g. energy before solve) */
   GSE_ERR_UNSUPPORTED = 7,       /* no GPU, wrong architecture, or feature not built */
-  GSE_ERR_NONFINITE = 8          /* a position or charge is NaN/Inf */
+  GSE_ERR_NONFINITE = 8          /* a position or charge is NaN/Inf: returned by the call
+                                    that saw it when its outputs are host memory, else by
+                                    the next gse_synchronize (results are then undefined) */
 } gse_status_t;
 
 typedef enum gse_precision {

@@ -109,3 +109,36 @@ def test_every_tiled_stencil_width(h):
     L = M * h
     x = waters(900, L, 12)
     check((M, M, M), (L, L, L), 2.0, x)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_nonfinite_input_is_reported(precision):
+    """A NaN or infinite position or charge makes the call that reads it return
+    GSE_ERR_NONFINITE when its outputs are host memory, or the next
+    gse_synchronize when they are device memory; later calls work again."""
+    import torch
+    from gse_b200._lib import GseError
+    from gse_b200.gse import Context
+    L, M = 24.0, 24
+    x = waters(900, L, 12)
+    ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision=precision)
+    ct = np.float64 if precision == "fp64" else np.float32
+    n = x.shape[0]
+    f = [np.zeros(n) for _ in range(3)]
+    bad = x.copy()
+    bad[17, 1] = np.nan
+    with pytest.raises(GseError) as ei:
+        ctx.forward(n, bad.astype(ct), *f)
+    assert ei.value.status == 8
+    E = ctx.forward(n, x.astype(ct), *f)  # works again
+    assert np.isfinite(E)
+    bad[17, 1] = 1.0
+    bad[3, 3] = np.inf
+    xd = torch.from_numpy(bad.astype(ct)).cuda()
+    fd = torch.zeros(3, n, dtype=torch.float64, device="cuda")
+    ed = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.forward(n, xd, fd[0], fd[1], fd[2], energy_out=ed)  # asynchronous: no status yet
+    with pytest.raises(GseError) as ei:
+        ctx.synchronize()
+    assert ei.value.status == 8
+    ctx.synchronize()  # reported once
