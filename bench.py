@@ -243,6 +243,55 @@ def bench_batch(steps: int, warmup: int, flush):
     return out
 
 
+def bench_grid_ops(steps: int, warmup: int, flush, peak: float):
+    """The grid operations beside the force path at the benchmark grid (144^3,
+    box 140): the on-grid Gaussian convolution of the real-space variant's
+    second spreading (sigma2 of sigma 2.0) and the forward-difference field,
+    device grids in and out, in both calculation types.  Algorithmic bytes:
+    one grid read and one written for the convolution (its two intermediate
+    grids, 12 or 24 MB, are the reference's too and largely stay in L2), one
+    read and three written for the field."""
+    import torch
+    from gse_b200.gse import Context
+    M, L, sigma = 144, 140.0, 2.0
+    s2 = sigma * np.sqrt(1.0 - 2.0 * 0.4)
+    rc2 = 3.0 * np.sqrt(2.0) * s2
+    out = {"workload": f"grid {M}^3, box {L}, sigma2 {s2:.6f} (sigma {sigma}), device grids"}
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(3)
+    for prec, dt in (("mixed", torch.float32), ("fp64", torch.float64)):
+        ctx = Context(M, M, M, sigma, 0.4, 3.0, 3.0, L, L, L, precision=prec)
+        ctx.set_stream(stream.cuda_stream)
+        x = torch.from_numpy(rng.standard_normal((M, M, M))).to(dt).cuda()
+        y = torch.empty_like(x)
+        E = torch.empty((3, M, M, M), dtype=dt, device="cuda")
+        gb = x.numel() * x.element_size() / 1e9
+
+        def timed(fn):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            t = 0.0
+            for _ in range(steps):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                torch.cuda.synchronize()
+                t += a.elapsed_time(b)
+            return t / steps
+
+        ms_c = timed(lambda: ctx.gauss_spread_on_grid(s2, rc2, L, L, L, x, y))
+        ms_e = timed(lambda: ctx.gauss_efield_on_grid(L, L, L, x, E[0], E[1], E[2]))
+        out[prec] = {"spread_on_grid_ms": ms_c, "spread_on_grid_gbs": 2 * gb / (ms_c / 1e3),
+                     "spread_on_grid_frac_hbm": 2 * gb / (ms_c / 1e3) / peak,
+                     "efield_ms": ms_e, "efield_gbs": 4 * gb / (ms_e / 1e3),
+                     "efield_frac_hbm": 4 * gb / (ms_e / 1e3) / peak}
+        ctx.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,6 +498,12 @@ def main():
                 batch = bench_batch(max(3, min(args.steps, 20)), args.warmup, flush)
             except Exception as exc:  # noqa: BLE001
                 batch = {"failed": str(exc)}
+        grid_ops = None
+        if not args.no_batch:
+            try:
+                grid_ops = bench_grid_ops(max(3, min(args.steps, 20)), args.warmup, flush, peak)
+            except Exception as exc:  # noqa: BLE001
+                grid_ops = {"failed": str(exc)}
         per_stage = {k: round(v[0] / max(v[1], 1), 4) for k, v in stage.items()}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -474,6 +529,7 @@ def main():
             "vs_ewald": accuracy,
             "energy": E_main,
             "batch": batch,
+            "grid_ops": grid_ops,
         }
         print(json.dumps(line), flush=True)
 

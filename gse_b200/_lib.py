@@ -88,6 +88,9 @@ SIGNATURES = {
     "gse_gauss_interpolate": (_i, [_vp, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "gse_green_mul": (_i, [_vp, _d, _d, _d, _d, _vp]),
     "gse_fft_solve": (_i, [_vp, _d, _d, _d, _d, _vp, _vp]),
+    "gse_gauss_spread_on_grid": (_i, [_vp, _d, _d, _d, _d, _d, _vp, _vp]),
+    "gse_gauss_efield_on_grid": (_i, [_vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
+    "gse_gauss_dipole_sum": (_i, [_vp, _d, _d, _d, _vp, _vp]),
     "gse_set_timing": (_i, [_vp, _i]),
     "gse_get_timing": (_i, [_vp, _vp, _vp, _i]),
     "gse_get_launch_count": (_i, [_vp, _vp]),

@@ -20,6 +20,7 @@
 #include "gse_kernels.cuh"
 #include "gse_adjoint.cuh"
 #include "gse_ewald.cuh"
+#include "gse_grid_ops.cuh"
 #include "gse_tiled.cuh"
 #include "gse_green_cb_fatbin.h"  // generated: the c2r load callbacks as LTO code
 
@@ -120,7 +121,10 @@ struct gse_context {
   size_t adj_cap = 0;
   double* d_force = nullptr;  // 3 x atom_cap
   double* d_partials = nullptr;
-  double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch
+  double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch, [4..6] dipole
+  // grid scratch of the stand-alone grid operations, allocated on first use
+  void* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
   int* d_bad = nullptr;
   double* h_pinned = nullptr;  // [0] energy
   // set by the binning when a position or charge is not finite; host memory
@@ -582,6 +586,63 @@ gse_status_t energy_out(gse_context_t* c, double* energy, bool* host) {
 
 }  // namespace
 
+// Helpers of the grid operations beside the force path.
+namespace {
+
+// At least `bytes` of grid scratch on the context's device.
+gse_status_t ensure_scratch(gse_context_t* c, size_t bytes) {
+  if (c->scratch_bytes >= bytes) return GSE_OK;
+  CU(cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_scratch);
+  c->d_scratch = nullptr;
+  c->scratch_bytes = 0;
+  if (cudaMalloc(&c->d_scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GSE_ERR_OOM, "grid scratch of %zu bytes", bytes);
+  }
+  c->scratch_bytes = bytes;
+  return GSE_OK;
+}
+
+// Taps of the on-grid convolution, CpuGaussCharge.cpp:413-438, in the
+// reference's own expressions and types: the exponent is formed in CT and
+// handed to the double exp() (the overload an unqualified exp() of a float
+// resolves to there); the z taps multiply the CT prefactor by that double
+// before rounding to CT.
+template <typename CT>
+void conv_taps(const int M[3], const double box[3], double sigma, double rcut,
+               ConvTaps<CT> taps[3]) {
+  double hd[3];
+  for (int d = 0; d < 3; d++) hd[d] = box[d] / (double)M[d];
+  const CT inv_2sigmasq = (CT)(1.0 / (2.0 * sigma * sigma));
+  const CT pref = (CT)(std::pow(2.0 * kPi * sigma * sigma, -3.0 / 2.0) * hd[0] * hd[1] * hd[2]);
+  for (int d = 0; d < 3; d++) {
+    const int n = (int)std::ceil(rcut / hd[d]);
+    const CT hsq = (CT)(hd[d] * hd[d]);
+    taps[d].n = n;
+    for (int i = -n; i <= n; i++) {
+      const CT arg = -hsq * (CT)(i * i) * inv_2sigmasq;
+      const double e = std::exp((double)arg);
+      taps[d].g[i + n] = d == 2 ? (CT)((double)pref * e) : (CT)e;
+    }
+  }
+}
+
+template <typename CT>
+gse_status_t spread_on_grid(gse_context_t* c, const double box[3], double sigma, double rcut,
+                            const CT* in, CT* tmp, CT* out) {
+  const int M[3] = {c->p.size_x, c->p.size_y, c->p.size_z};
+  ConvTaps<CT> taps[3];
+  conv_taps<CT>(M, box, sigma, rcut, taps);
+  CT* rx = (CT*)c->d_rhok;  // the half spectrum holds at least one real grid
+  CU(launch_conv_pass<CT>(in, rx, M, 0, taps[0], c->stream));
+  CU(launch_conv_pass<CT>(rx, tmp, M, 1, taps[1], c->stream));
+  CU(launch_conv_pass<CT>(tmp, out, M, 2, taps[2], c->stream));
+  return GSE_OK;
+}
+
+}  // namespace
+
 // ===========================================================================
 extern "C" {
 
@@ -691,10 +752,10 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
   CUC(cudaMalloc(&c->d_partials, sizeof(double) * (kEnergyPartials + 1)));
   CUC(cudaMemset(c->d_partials, 0, sizeof(double) * (kEnergyPartials + 1)));
-  CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 4));
+  CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 8));
   CUC(cudaMalloc(&c->d_bad, sizeof(int)));
   CUC(cudaMemset(c->d_bad, 0, sizeof(int)));
-  CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 4));
+  CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 8));
   CUC(cudaMallocHost(&c->h_pinned, sizeof(double) * 4));
   {
     int* hb = nullptr;
@@ -728,6 +789,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_rho);
   cudaFree(c->d_phi);
   cudaFree(c->d_rhok);
+  cudaFree(c->d_scratch);
   cudaFree(c->d_fixed);
   cudaFree(c->d_xyzq);
   cudaFree(c->d_sorted);
@@ -1073,6 +1135,122 @@ gse_status_t gse_fft_solve(gse_context_t* c, double sigma, double bx, double by,
   c->energy_valid = false;
   bool host = false;
   if (!pdev) TRY(copy_out(c, phi, c->d_phi, bytes, &host));
+  return finish(c, host);
+}
+
+// ---- grid operations beside the force path -------------------------------
+
+gse_status_t gse_gauss_spread_on_grid(gse_context_t* c, double sigma, double rcut, double bx,
+                                      double by, double bz, const void* rho, void* rho_s) {
+  TRY(check_ctx(c));
+  if (!rho || !rho_s) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  const double box[3] = {bx, by, bz};
+  TRY(check_stencil(c, box, sigma, rcut));
+  const size_t bytes = c->size * c->ct;
+  TRY(ensure_scratch(c, bytes));
+  const void* in = rho;
+  if (!is_device_ptr(rho)) {
+    CU(cudaMemcpyAsync(c->d_scratch, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+    in = c->d_scratch;
+  }
+  // the x pass reads the input before the z pass writes the output, so the
+  // two may be the same device grid
+  const bool odev = is_device_ptr(rho_s);
+  void* out = odev ? rho_s : c->d_rho;
+  if (c->fp64)
+    TRY(spread_on_grid<double>(c, box, sigma, rcut, (const double*)in, (double*)c->d_scratch,
+                               (double*)out));
+  else
+    TRY(spread_on_grid<float>(c, box, sigma, rcut, (const float*)in, (float*)c->d_scratch,
+                              (float*)out));
+  if (out == c->d_rho) {
+    c->rho_valid = true;
+    c->phi_valid = false;
+    c->energy_valid = false;
+  }
+  bool host = false;
+  if (!odev) TRY(copy_out(c, rho_s, c->d_rho, bytes, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_gauss_efield_on_grid(gse_context_t* c, double bx, double by, double bz,
+                                      const void* phi, void* ex, void* ey, void* ez) {
+  TRY(check_ctx(c));
+  if (!phi || !ex || !ey || !ez) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  if (!(bx > 0 && by > 0 && bz > 0) || !std::isfinite(bx) || !std::isfinite(by) ||
+      !std::isfinite(bz))
+    return fail(GSE_ERR_INVALID_ARG, "box lengths must be positive and finite");
+  const int M[3] = {c->p.size_x, c->p.size_y, c->p.size_z};
+  const size_t bytes = c->size * c->ct;
+  void* outs[3] = {ex, ey, ez};
+  bool odev[3];
+  int nhost = 0;
+  for (int d = 0; d < 3; d++) {
+    odev[d] = is_device_ptr(outs[d]);
+    if (!odev[d]) nhost++;
+  }
+  const bool idev = is_device_ptr(phi);
+  TRY(ensure_scratch(c, bytes * ((idev ? 0 : 1) + nhost)));
+  char* sp = (char*)c->d_scratch;
+  const void* in = phi;
+  if (!idev) {
+    CU(cudaMemcpyAsync(sp, phi, bytes, cudaMemcpyHostToDevice, c->stream));
+    in = sp;
+    sp += bytes;
+  }
+  void* dst[3];
+  for (int d = 0; d < 3; d++) {
+    if (odev[d]) {
+      dst[d] = outs[d];
+    } else {
+      dst[d] = sp;
+      sp += bytes;
+    }
+  }
+  const double hd[3] = {bx / (double)M[0], by / (double)M[1], bz / (double)M[2]};
+  if (c->fp64) {
+    const double ih[3] = {1.0 / hd[0], 1.0 / hd[1], 1.0 / hd[2]};
+    CU(launch_efield<double>((const double*)in, (double*)dst[0], (double*)dst[1], (double*)dst[2],
+                             M, ih, c->stream));
+  } else {
+    const float ih[3] = {(float)(1.0 / hd[0]), (float)(1.0 / hd[1]), (float)(1.0 / hd[2])};
+    CU(launch_efield<float>((const float*)in, (float*)dst[0], (float*)dst[1], (float*)dst[2], M,
+                            ih, c->stream));
+  }
+  bool host = false;
+  for (int d = 0; d < 3; d++)
+    if (!odev[d]) TRY(copy_out(c, outs[d], dst[d], bytes, &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_gauss_dipole_sum(gse_context_t* c, double bx, double by, double bz,
+                                  const void* rho, double* dip) {
+  TRY(check_ctx(c));
+  if (!rho || !dip) return fail(GSE_ERR_INVALID_ARG, "NULL argument");
+  if (!(bx > 0 && by > 0 && bz > 0) || !std::isfinite(bx) || !std::isfinite(by) ||
+      !std::isfinite(bz))
+    return fail(GSE_ERR_INVALID_ARG, "box lengths must be positive and finite");
+  const int M[3] = {c->p.size_x, c->p.size_y, c->p.size_z};
+  const size_t bytes = c->size * c->ct;
+  const void* in = rho;
+  if (!is_device_ptr(rho)) {
+    TRY(ensure_scratch(c, bytes));
+    CU(cudaMemcpyAsync(c->d_scratch, rho, bytes, cudaMemcpyHostToDevice, c->stream));
+    in = c->d_scratch;
+  }
+  static_assert(3 * kDipoleBlocks <= kEnergyPartials, "dipole partials fit the energy partials");
+  unsigned* done = reinterpret_cast<unsigned*>(c->d_partials + kEnergyPartials);
+  double* out = c->d_scalars + 4;
+  if (c->fp64) {
+    const double h[3] = {bx / (double)M[0], by / (double)M[1], bz / (double)M[2]};
+    CU(launch_dipole<double>((const double*)in, M, h, c->d_partials, done, out, c->stream));
+  } else {
+    const float h[3] = {(float)(bx / (double)M[0]), (float)(by / (double)M[1]),
+                        (float)(bz / (double)M[2])};
+    CU(launch_dipole<float>((const float*)in, M, h, c->d_partials, done, out, c->stream));
+  }
+  bool host = false;
+  TRY(copy_out(c, dip, out, 3 * sizeof(double), &host));
   return finish(c, host);
 }
 

@@ -163,7 +163,8 @@ class CpuGrid {
 
 // ---------------------------------------------------------------------------
 // CpuGaussCharge<AT,CT>: spreading and interpolation with explicit sigma,
-// cut-off and box (CpuGaussCharge.cpp:105-384).
+// cut-off and box (CpuGaussCharge.cpp:105-384), and the grid operations
+// beside them (CpuGaussCharge.cpp:62-98, :188-226, :390-519).
 // ---------------------------------------------------------------------------
 template <typename AT, typename CT>
 class CpuGaussCharge {
@@ -209,6 +210,40 @@ class CpuGaussCharge {
     same_size(phi);
     check(gse_gauss_interpolate(ctx_.get(), sigma, rcut, numCoord, xyzq, boxx, boxy, boxz,
                                 phi.getDataPointer(), forceX, forceY, forceZ));
+  }
+
+  // On-grid Gaussian convolution, rhoS = G(sigma) * rho (CpuGaussCharge.cpp:390-519).
+  void spreadChargeOnGrid(const double sigma, const double rcut, const double boxx,
+                          const double boxy, const double boxz, const CpuGrid<CT>& rho,
+                          CpuGrid<CT>& rhoS) {
+    same_size(rho);
+    same_size(rhoS);
+    check(gse_gauss_spread_on_grid(ctx_.get(), sigma, rcut, boxx, boxy, boxz,
+                                   rho.getDataPointer(), rhoS.getDataPointer()));
+  }
+
+  // Forward-difference field on the grid (CpuGaussCharge.cpp:62-98).
+  void calcElectricFieldOnGrid(const double boxx, const double boxy, const double boxz,
+                               const CpuGrid<CT>& phi, CpuGrid<CT>& Ex, CpuGrid<CT>& Ey,
+                               CpuGrid<CT>& Ez) {
+    same_size(phi);
+    same_size(Ex);
+    same_size(Ey);
+    same_size(Ez);
+    check(gse_gauss_efield_on_grid(ctx_.get(), boxx, boxy, boxz, phi.getDataPointer(),
+                                   Ex.getDataPointer(), Ey.getDataPointer(),
+                                   Ez.getDataPointer()));
+  }
+
+  // Dipole sum of a charge grid (CpuGaussCharge.cpp:188-226).
+  void calcDipoleSum(const double boxx, const double boxy, const double boxz,
+                     const CpuGrid<CT>& rho, AT& dipSumX, AT& dipSumY, AT& dipSumZ) {
+    same_size(rho);
+    double d[3];
+    check(gse_gauss_dipole_sum(ctx_.get(), boxx, boxy, boxz, rho.getDataPointer(), d));
+    dipSumX = d[0];
+    dipSumY = d[1];
+    dipSumZ = d[2];
   }
 
  private:

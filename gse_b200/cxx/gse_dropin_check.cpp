@@ -8,6 +8,7 @@
 // "E_stages <energy>" and "F_stages ..." lines from the same computation
 // assembled out of CpuGaussCharge, CpuGreensFuncGSE and CpuFFTSolver.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -59,6 +60,24 @@ int run(int M[3], double L[3], double sigma, const std::vector<double>& raw) {
                          fy.data(), fz.data());
   for (int i = 0; i < n; i++)
     printf("F_stages %.17g %.17g %.17g\n", ccelec * fx[i], ccelec * fy[i], ccelec * fz[i]);
+
+  // the real-space variant's second spreading step (CpuGSEr::spreadCharge2)
+  // and the grid field and dipole of the first spreading
+  if (getenv("GSE_CHECK_GRID_OPS")) {
+    const double rcut2 = gse.getLambdaSigma1() * std::sqrt(2.0) * sigma2;
+    CpuGrid<CT> rhoS(M[0], M[1], M[2]), Ex(M[0], M[1], M[2]), Ey(M[0], M[1], M[2]),
+        Ez(M[0], M[1], M[2]);
+    gauss.spreadChargeOnGrid(sigma2, rcut2, L[0], L[1], L[2], rho, rhoS);
+    gauss.calcElectricFieldOnGrid(L[0], L[1], L[2], phi, Ex, Ey, Ez);
+    double dip[3];
+    gauss.calcDipoleSum(L[0], L[1], L[2], rho, dip[0], dip[1], dip[2]);
+    printf("DIP %.17g %.17g %.17g\n", dip[0], dip[1], dip[2]);
+    for (int i = 0; i < rho.getSize(); i++)
+      printf("G %.17g %.17g %.17g %.17g %.17g %.17g\n", (double)rho.getDataPointer()[i],
+             (double)phi.getDataPointer()[i], (double)rhoS.getDataPointer()[i],
+             (double)Ex.getDataPointer()[i], (double)Ey.getDataPointer()[i],
+             (double)Ez.getDataPointer()[i]);
+  }
   return 0;
 }
 

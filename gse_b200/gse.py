@@ -137,6 +137,17 @@ class Context:
     def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
         check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
 
+    def gauss_spread_on_grid(self, sigma, rcut, boxx, boxy, boxz, rho, rho_s):
+        check(self._L.gse_gauss_spread_on_grid(self.h, sigma, rcut, boxx, boxy, boxz, ptr(rho),
+                                               ptr(rho_s)))
+
+    def gauss_efield_on_grid(self, boxx, boxy, boxz, phi, ex, ey, ez):
+        check(self._L.gse_gauss_efield_on_grid(self.h, boxx, boxy, boxz, ptr(phi), ptr(ex),
+                                               ptr(ey), ptr(ez)))
+
+    def gauss_dipole_sum(self, boxx, boxy, boxz, rho, dip):
+        check(self._L.gse_gauss_dipole_sum(self.h, boxx, boxy, boxz, ptr(rho), ptr(dip)))
+
     def adjoint(self, n, xyzq, dLdE, gfx, gfy, gfz, dq, dx, dy, dz):
         """dL/dq and dL/dx for dL/dE = dLdE and dL/dF = (gfx, gfy, gfz) (may be None)."""
         check(self._L.gse_adjoint(self.h, int(n), ptr(xyzq), float(dLdE), ptr(gfx), ptr(gfy),
@@ -263,6 +274,30 @@ class CpuGaussCharge:
         ph = np.ascontiguousarray(phi.data, dtype=self.dtype)
         self._ctx.gauss_interpolate(sigma, rcut, numCoord, _xyzq_arg(xyzq, self.dtype), boxx,
                                     boxy, boxz, ph, forceX, forceY, forceZ)
+
+    def _grid_arg(self, grid: CpuGrid):
+        self._check(grid)
+        if grid.data.dtype != self.dtype:
+            raise GseError(1, "grid dtype does not match precision")
+        return grid.data
+
+    def spreadChargeOnGrid(self, sigma, rcut, boxx, boxy, boxz, rho: CpuGrid, rhoS: CpuGrid):
+        """On-grid Gaussian convolution (CpuGaussCharge.cpp:390-519)."""
+        self._ctx.gauss_spread_on_grid(sigma, rcut, boxx, boxy, boxz, self._grid_arg(rho),
+                                       self._grid_arg(rhoS))
+
+    def calcElectricFieldOnGrid(self, boxx, boxy, boxz, phi: CpuGrid, Ex: CpuGrid, Ey: CpuGrid,
+                                Ez: CpuGrid):
+        """Forward-difference field on the grid (CpuGaussCharge.cpp:62-98)."""
+        self._ctx.gauss_efield_on_grid(boxx, boxy, boxz, self._grid_arg(phi), self._grid_arg(Ex),
+                                       self._grid_arg(Ey), self._grid_arg(Ez))
+
+    def calcDipoleSum(self, boxx, boxy, boxz, rho: CpuGrid):
+        """(dipSumX, dipSumY, dipSumZ) of a charge grid (CpuGaussCharge.cpp:188-226); the
+        reference returns them through reference arguments."""
+        dip = np.zeros(3)
+        self._ctx.gauss_dipole_sum(boxx, boxy, boxz, self._grid_arg(rho), dip)
+        return float(dip[0]), float(dip[1]), float(dip[2])
 
     def calcSupportSize(self, rcut, boxx, boxy, boxz):
         """Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56)."""

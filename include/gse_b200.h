@@ -175,6 +175,37 @@ gse_status_t gse_green_mul(gse_context_t* ctx, double sigma, double box_x, doubl
 gse_status_t gse_fft_solve(gse_context_t* ctx, double sigma, double box_x, double box_y,
                            double box_z, const void* rho, void* phi);
 
+/* ---- grid operations beside the force path ------------------------------ */
+
+/* CpuGaussCharge<AT,CT>::spreadChargeOnGrid (CpuGaussCharge.cpp:390-519), the
+ * second spreading step of the real-space variant (CpuGSEr::spreadCharge2,
+ * CpuGSEr.cpp:39-42): rho_s = rho convolved with the periodic Gaussian of
+ * width sigma, as three 1-D passes x -> y -> z with taps
+ * exp(-h^2 i^2 / (2 sigma^2)), i = -n..n, n = ceil(rcut / h), the z taps
+ * times (2 pi sigma^2)^(-3/2) hx hy hz.  Bit-identical to the reference in
+ * both calculation types.  rho and rho_s are CT grids of the context's size
+ * (host or device; the same device grid may be passed for both).  A host
+ * rho_s also leaves the result in the context's rhoS. */
+gse_status_t gse_gauss_spread_on_grid(gse_context_t* ctx, double sigma, double rcut,
+                                      double box_x, double box_y, double box_z, const void* rho,
+                                      void* rho_s);
+
+/* CpuGaussCharge<AT,CT>::calcElectricFieldOnGrid (CpuGaussCharge.cpp:62-98):
+ * E_d(p) = -(phi(p + e_d) - phi(p)) / h_d, periodic, in CT (bit-identical to
+ * the reference).  phi, ex, ey, ez are CT grids of the context's size (host or
+ * device); phi must not be one of the outputs. */
+gse_status_t gse_gauss_efield_on_grid(gse_context_t* ctx, double box_x, double box_y,
+                                      double box_z, const void* phi, void* ex, void* ey,
+                                      void* ez);
+
+/* CpuGaussCharge<AT,CT>::calcDipoleSum (CpuGaussCharge.cpp:188-226):
+ * dip[d] = sum_p (double)((rho_p hx hy hz) * h_d i_d) for d = x, y, z; each
+ * term as the reference forms it in CT, the terms added in double in a fixed
+ * order (not the reference's loop order).  rho is a CT grid (host or device),
+ * dip three doubles (host or device). */
+gse_status_t gse_gauss_dipole_sum(gse_context_t* ctx, double box_x, double box_y, double box_z,
+                                  const void* rho, double* dip);
+
 /* ---- reverse mode (no reference counterpart) ---------------------------- */
 
 /* Vector-Jacobian product of one force evaluation (gse_forward) for the

@@ -68,6 +68,15 @@ def lib():
             f = getattr(L, f"orc_energy_{sfx}")
             f.argtypes = [_i, _i, _i, _d, _d, _d, _d, p, p]
             f.restype = _d
+            f = getattr(L, f"orc_spread_on_grid_{sfx}")
+            f.argtypes = [_i, _i, _i, _d, _d, _d, _d, _d, p, p]
+            f.restype = _i
+            f = getattr(L, f"orc_efield_{sfx}")
+            f.argtypes = [_i, _i, _i, _d, _d, _d, p, p, p, p]
+            f.restype = None
+            f = getattr(L, f"orc_dipole_{sfx}")
+            f.argtypes = [_i, _i, _i, _d, _d, _d, p, _dp]
+            f.restype = None
         L.orc_fft_r2c_3d.argtypes = [_i, _i, _i, _dp, _dp]
         L.orc_fft_r2c_3d.restype = _i
         L.orc_fft_c2r_3d.argtypes = [_i, _i, _i, _dp, _dp]
@@ -107,6 +116,12 @@ def ref():
         R.ref_spread.restype = _i
         R.ref_gather.argtypes = [_i, _i, _i, _i, _d, _d, _i, _vp, _d, _d, _d, _vp, _dp, _dp, _dp]
         R.ref_gather.restype = _i
+        R.ref_spread_on_grid.argtypes = [_i, _i, _i, _i, _d, _d, _d, _d, _d, _vp, _vp]
+        R.ref_spread_on_grid.restype = _i
+        R.ref_efield.argtypes = [_i, _i, _i, _i, _d, _d, _d, _vp, _vp, _vp, _vp]
+        R.ref_efield.restype = _i
+        R.ref_dipole.argtypes = [_i, _i, _i, _i, _d, _d, _d, _vp, _dp]
+        R.ref_dipole.restype = _i
         R.ref_green_mul_d.argtypes = [_i, _i, _i, _d, _d, _d, _d, _dp]
         R.ref_green_mul_d.restype = _i
         R.ref_ewald_recip.argtypes = [_d, _i, _d, _d, _d, _d, _i, _dp, _dp, _dp, _dp]
@@ -178,6 +193,49 @@ def energy(M, box, rho, phi, ccelec=CCELEC, dtype=np.float64) -> float:
     f = np.ascontiguousarray(phi, dtype=dtype)
     return float(getattr(lib(), f"orc_energy_{sfx}")(sx, sy, sz, box[0], box[1], box[2], ccelec,
                                                      _ptr(r, p), _ptr(f, p)))
+
+
+def _grid(a, dtype, M):
+    sx, sy, sz = M
+    g = np.ascontiguousarray(a, dtype=dtype)
+    if g.size != sx * sy * sz:
+        raise ValueError("grid size mismatch")
+    return g.reshape(sz, sy, sx)
+
+
+def spread_on_grid(M, box, sigma, rcut, rho, dtype=np.float64) -> np.ndarray:
+    """rhoS[z, y, x] from CpuGaussCharge::spreadChargeOnGrid (restated)."""
+    sx, sy, sz = M
+    r = _grid(rho, dtype, M)
+    out = np.zeros_like(r)
+    sfx, p = ("d", _dp) if dtype == np.float64 else ("f", _fp)
+    rc = getattr(lib(), f"orc_spread_on_grid_{sfx}")(sx, sy, sz, sigma, rcut, box[0], box[1],
+                                                     box[2], _ptr(r, p), _ptr(out, p))
+    if rc:
+        raise RuntimeError("orc_spread_on_grid failed")
+    return out
+
+
+def efield(M, box, phi, dtype=np.float64):
+    """(Ex, Ey, Ez)[z, y, x] from CpuGaussCharge::calcElectricFieldOnGrid (restated)."""
+    sx, sy, sz = M
+    f = _grid(phi, dtype, M)
+    E = [np.zeros_like(f) for _ in range(3)]
+    sfx, p = ("d", _dp) if dtype == np.float64 else ("f", _fp)
+    getattr(lib(), f"orc_efield_{sfx}")(sx, sy, sz, box[0], box[1], box[2], _ptr(f, p),
+                                        *(_ptr(e, p) for e in E))
+    return tuple(E)
+
+
+def dipole_sum(M, box, rho, dtype=np.float64) -> np.ndarray:
+    """(x, y, z) from CpuGaussCharge::calcDipoleSum (restated)."""
+    sx, sy, sz = M
+    r = _grid(rho, dtype, M)
+    out = np.zeros(3)
+    sfx, p = ("d", _dp) if dtype == np.float64 else ("f", _fp)
+    getattr(lib(), f"orc_dipole_{sfx}")(sx, sy, sz, box[0], box[1], box[2], _ptr(r, p),
+                                        _ptr(out))
+    return out
 
 
 def fft_r2c(x: np.ndarray) -> np.ndarray:
@@ -287,6 +345,33 @@ def ref_gather(M, box, sigma, rcut, xyzq, phi, dtype=np.float64):
     ref().ref_gather(0 if dtype == np.float64 else 1, sx, sy, sz, sigma, rcut, n, a.ctypes.data,
                      box[0], box[1], box[2], ph.ctypes.data, _ptr(fx), _ptr(fy), _ptr(fz))
     return fx, fy, fz
+
+
+def ref_spread_on_grid(M, box, sigma, rcut, rho, dtype=np.float64):
+    sx, sy, sz = M
+    r = _grid(rho, dtype, M)
+    out = np.zeros_like(r)
+    ref().ref_spread_on_grid(0 if dtype == np.float64 else 1, sx, sy, sz, sigma, rcut, box[0],
+                             box[1], box[2], r.ctypes.data, out.ctypes.data)
+    return out
+
+
+def ref_efield(M, box, phi, dtype=np.float64):
+    sx, sy, sz = M
+    f = _grid(phi, dtype, M)
+    E = [np.zeros_like(f) for _ in range(3)]
+    ref().ref_efield(0 if dtype == np.float64 else 1, sx, sy, sz, box[0], box[1], box[2],
+                     f.ctypes.data, *(e.ctypes.data for e in E))
+    return tuple(E)
+
+
+def ref_dipole_sum(M, box, rho, dtype=np.float64):
+    sx, sy, sz = M
+    r = _grid(rho, dtype, M)
+    out = np.zeros(3)
+    ref().ref_dipole(0 if dtype == np.float64 else 1, sx, sy, sz, box[0], box[1], box[2],
+                     r.ctypes.data, _ptr(out))
+    return out
 
 
 def ref_green_mul(M, box, sigma, rhoK):

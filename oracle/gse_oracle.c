@@ -15,6 +15,9 @@
  *   CpuGSE::calculateEnergy CpuGSE.cpp:86-103
  *   CpuGSE::interpolateForce CpuGSE.cpp:70-80        (x ccelec afterwards)
  *   CpuGSE::setParam     CpuGSE.cpp:33-44
+ *   spreadChargeOnGrid   CpuGaussCharge.cpp:390-519  (on-grid sigma convolution)
+ *   calcElectricFieldOnGrid CpuGaussCharge.cpp:62-98
+ *   calcDipoleSum        CpuGaussCharge.cpp:188-226
  *   CpuGSEk::spreadCharge1/solvePoisson/calculateEnergy CpuGSEk.cpp:30-58
  *   CpuEwaldRecip::calcForceEnergy CpuEwaldRecip.cpp:87-147
  *   CpuEwaldDirect::calcForceEnergy CpuEwaldDirect.cpp:45-131
@@ -264,6 +267,135 @@ DEFINE_GREEN(f, float, exp)
 
 DEFINE_ENERGY(d, double)
 DEFINE_ENERGY(f, float)
+
+/* ------------------------------------------------------------------------ */
+/* On-grid Gaussian convolution, CpuGaussCharge.cpp:390-519.  Three periodic */
+/* 1-D passes, x then y then z, with taps G[i] = exp(-h^2 i^2 / (2 sigma^2)),*/
+/* i = -n..n, n = ceil(rcut / h) per axis; the z taps also carry             */
+/* (2 pi sigma^2)^(-3/2) hx hy hz (the product formed in double, as the      */
+/* reference's float * double(exp) does).  Every output is summed from zero  */
+/* in tap order, each product and sum rounded in CT.                         */
+/* ------------------------------------------------------------------------ */
+#define DEFINE_CONV(SFX, CT, EXPFN)                                                    \
+  int orc_spread_on_grid_##SFX(int sizeX, int sizeY, int sizeZ, double sigma,          \
+                               double rcut, double boxx, double boxy, double boxz,     \
+                               const CT* rho, CT* rhoS) {                              \
+    const double hxd = boxx / (double)sizeX;                                           \
+    const double hyd = boxy / (double)sizeY;                                           \
+    const double hzd = boxz / (double)sizeZ;                                           \
+    const int nx = (int)ceil(rcut / hxd);                                              \
+    const int ny = (int)ceil(rcut / hyd);                                              \
+    const int nz = (int)ceil(rcut / hzd);                                              \
+    const CT inv_2sigmasq = (CT)(1.0 / (2.0 * sigma * sigma));                         \
+    const CT pref = (CT)(pow(2.0 * ORC_PI * sigma * sigma, -3.0 / 2.0) * hxd * hyd * hzd); \
+    const CT hxsq = (CT)(hxd * hxd);                                                   \
+    const CT hysq = (CT)(hyd * hyd);                                                   \
+    const CT hzsq = (CT)(hzd * hzd);                                                   \
+    const long size = (long)sizeX * sizeY * sizeZ;                                     \
+    CT* gx = (CT*)malloc(sizeof(CT) * (2 * nx + 1));                                   \
+    CT* gy = (CT*)malloc(sizeof(CT) * (2 * ny + 1));                                   \
+    CT* gz = (CT*)malloc(sizeof(CT) * (2 * nz + 1));                                   \
+    CT* tx = (CT*)malloc(sizeof(CT) * size);                                           \
+    CT* txy = (CT*)malloc(sizeof(CT) * size);                                          \
+    if (!gx || !gy || !gz || !tx || !txy) {                                            \
+      free(gx); free(gy); free(gz); free(tx); free(txy);                               \
+      return -1;                                                                       \
+    }                                                                                  \
+    for (int i = -nx; i <= nx; i++) gx[i + nx] = EXPFN(-hxsq * (CT)(i * i) * inv_2sigmasq); \
+    for (int i = -ny; i <= ny; i++) gy[i + ny] = EXPFN(-hysq * (CT)(i * i) * inv_2sigmasq); \
+    for (int i = -nz; i <= nz; i++)                                                    \
+      gz[i + nz] = pref * EXPFN(-hzsq * (CT)(i * i) * inv_2sigmasq);                   \
+    for (int z = 0; z < sizeZ; z++)                                                    \
+      for (int y = 0; y < sizeY; y++) {                                                \
+        const long row = ((long)y + (long)z * sizeY) * sizeX;                          \
+        for (int x = 0; x < sizeX; x++) {                                              \
+          CT s = (CT)0;                                                                \
+          for (int i = -nx; i <= nx; i++) s += gx[i + nx] * rho[row + pmod(x + i, sizeX)]; \
+          tx[row + x] = s;                                                             \
+        }                                                                              \
+      }                                                                                \
+    for (int z = 0; z < sizeZ; z++)                                                    \
+      for (int x = 0; x < sizeX; x++)                                                  \
+        for (int y = 0; y < sizeY; y++) {                                              \
+          CT s = (CT)0;                                                                \
+          for (int i = -ny; i <= ny; i++)                                              \
+            s += gy[i + ny] * tx[x + ((long)pmod(y + i, sizeY) + (long)z * sizeY) * sizeX]; \
+          txy[x + ((long)y + (long)z * sizeY) * sizeX] = s;                            \
+        }                                                                              \
+    for (int x = 0; x < sizeX; x++)                                                    \
+      for (int y = 0; y < sizeY; y++)                                                  \
+        for (int z = 0; z < sizeZ; z++) {                                              \
+          CT s = (CT)0;                                                                \
+          for (int i = -nz; i <= nz; i++)                                              \
+            s += gz[i + nz] * txy[x + ((long)y + (long)pmod(z + i, sizeZ) * sizeY) * sizeX]; \
+          rhoS[x + ((long)y + (long)z * sizeY) * sizeX] = s;                           \
+        }                                                                              \
+    free(gx); free(gy); free(gz); free(tx); free(txy);                                 \
+    return 0;                                                                          \
+  }
+
+DEFINE_CONV(d, double, exp)
+DEFINE_CONV(f, float, exp)
+
+/* ------------------------------------------------------------------------ */
+/* Electric field on the grid, CpuGaussCharge.cpp:62-98: forward differences */
+/* E = -(phi(p + e_d) - phi(p)) / h_d, periodic, in CT.                      */
+/* ------------------------------------------------------------------------ */
+#define DEFINE_EFIELD(SFX, CT)                                                         \
+  void orc_efield_##SFX(int sizeX, int sizeY, int sizeZ, double boxx, double boxy,     \
+                        double boxz, const CT* phi, CT* Ex, CT* Ey, CT* Ez) {          \
+    const CT inv_hx = (CT)(1.0 / (boxx / (double)sizeX));                              \
+    const CT inv_hy = (CT)(1.0 / (boxy / (double)sizeY));                              \
+    const CT inv_hz = (CT)(1.0 / (boxz / (double)sizeZ));                              \
+    for (int z = 0; z < sizeZ; z++)                                                    \
+      for (int y = 0; y < sizeY; y++)                                                  \
+        for (int x = 0; x < sizeX; x++) {                                              \
+          const long p = x + ((long)y + (long)z * sizeY) * sizeX;                      \
+          const CT c = phi[p];                                                         \
+          const CT px = phi[pmod(x + 1, sizeX) + ((long)y + (long)z * sizeY) * sizeX]; \
+          const CT py = phi[x + ((long)pmod(y + 1, sizeY) + (long)z * sizeY) * sizeX]; \
+          const CT pz = phi[x + ((long)y + (long)pmod(z + 1, sizeZ) * sizeY) * sizeX]; \
+          Ex[p] = -(px - c) * inv_hx;                                                  \
+          Ey[p] = -(py - c) * inv_hy;                                                  \
+          Ez[p] = -(pz - c) * inv_hz;                                                  \
+        }                                                                              \
+  }
+
+DEFINE_EFIELD(d, double)
+DEFINE_EFIELD(f, float)
+
+/* ------------------------------------------------------------------------ */
+/* Dipole sum of a charge grid, CpuGaussCharge.cpp:188-226: sum over points  */
+/* of (rho hx hy hz) * (hx ix, hy iy, hz iz), each term formed in CT and     */
+/* added in double in z, y, x loop order.                                    */
+/* ------------------------------------------------------------------------ */
+#define DEFINE_DIPOLE(SFX, CT)                                                         \
+  void orc_dipole_##SFX(int sizeX, int sizeY, int sizeZ, double boxx, double boxy,     \
+                        double boxz, const CT* rho, double* dip) {                     \
+    const CT hx = (CT)(boxx / (double)sizeX);                                          \
+    const CT hy = (CT)(boxy / (double)sizeY);                                          \
+    const CT hz = (CT)(boxz / (double)sizeZ);                                          \
+    double sx = 0.0, sy = 0.0, sz = 0.0;                                               \
+    for (int iz = 0; iz < sizeZ; iz++) {                                               \
+      const CT z = hz * (CT)iz;                                                        \
+      for (int iy = 0; iy < sizeY; iy++) {                                             \
+        const CT y = hy * (CT)iy;                                                      \
+        for (int ix = 0; ix < sizeX; ix++) {                                           \
+          const CT x = hx * (CT)ix;                                                    \
+          const CT val = rho[ix + ((long)iy + (long)iz * sizeY) * sizeX] * hx * hy * hz; \
+          sx += (double)(val * x);                                                     \
+          sy += (double)(val * y);                                                     \
+          sz += (double)(val * z);                                                     \
+        }                                                                              \
+      }                                                                                \
+    }                                                                                  \
+    dip[0] = sx;                                                                       \
+    dip[1] = sy;                                                                       \
+    dip[2] = sz;                                                                       \
+  }
+
+DEFINE_DIPOLE(d, double)
+DEFINE_DIPOLE(f, float)
 
 /* ------------------------------------------------------------------------ */
 /* Project-written complex FFT (recursive mixed radix, any length).          */

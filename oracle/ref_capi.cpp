@@ -100,6 +100,69 @@ int ref_gather(int ct, int sx, int sy, int sz, double sigma, double rcut, int n,
   return 0;
 }
 
+// CpuGaussCharge::spreadChargeOnGrid for <double,double> (ct=0) and
+// <double,float> (ct=1).
+int ref_spread_on_grid(int ct, int sx, int sy, int sz, double sigma, double rcut, double boxx,
+                       double boxy, double boxz, const void* rho_in, void* rhoS_out) {
+  const size_t size = (size_t)sx * sy * sz;
+  if (ct == 0) {
+    CpuGaussCharge<double, double> gc(sx, sy, sz);
+    CpuGrid<double> rho(sx, sy, sz), rhoS(sx, sy, sz);
+    std::memcpy(rho.getDataPointer(), rho_in, size * sizeof(double));
+    gc.spreadChargeOnGrid(sigma, rcut, boxx, boxy, boxz, rho, rhoS);
+    std::memcpy(rhoS_out, rhoS.getDataPointer(), size * sizeof(double));
+  } else {
+    CpuGaussCharge<double, float> gc(sx, sy, sz);
+    CpuGrid<float> rho(sx, sy, sz), rhoS(sx, sy, sz);
+    std::memcpy(rho.getDataPointer(), rho_in, size * sizeof(float));
+    gc.spreadChargeOnGrid(sigma, rcut, boxx, boxy, boxz, rho, rhoS);
+    std::memcpy(rhoS_out, rhoS.getDataPointer(), size * sizeof(float));
+  }
+  return 0;
+}
+
+// CpuGaussCharge::calcElectricFieldOnGrid, ct as above.
+int ref_efield(int ct, int sx, int sy, int sz, double boxx, double boxy, double boxz,
+               const void* phi_in, void* ex, void* ey, void* ez) {
+  const size_t size = (size_t)sx * sy * sz;
+  if (ct == 0) {
+    CpuGaussCharge<double, double> gc(sx, sy, sz);
+    CpuGrid<double> phi(sx, sy, sz), Ex(sx, sy, sz), Ey(sx, sy, sz), Ez(sx, sy, sz);
+    std::memcpy(phi.getDataPointer(), phi_in, size * sizeof(double));
+    gc.calcElectricFieldOnGrid(boxx, boxy, boxz, phi, Ex, Ey, Ez);
+    std::memcpy(ex, Ex.getDataPointer(), size * sizeof(double));
+    std::memcpy(ey, Ey.getDataPointer(), size * sizeof(double));
+    std::memcpy(ez, Ez.getDataPointer(), size * sizeof(double));
+  } else {
+    CpuGaussCharge<double, float> gc(sx, sy, sz);
+    CpuGrid<float> phi(sx, sy, sz), Ex(sx, sy, sz), Ey(sx, sy, sz), Ez(sx, sy, sz);
+    std::memcpy(phi.getDataPointer(), phi_in, size * sizeof(float));
+    gc.calcElectricFieldOnGrid(boxx, boxy, boxz, phi, Ex, Ey, Ez);
+    std::memcpy(ex, Ex.getDataPointer(), size * sizeof(float));
+    std::memcpy(ey, Ey.getDataPointer(), size * sizeof(float));
+    std::memcpy(ez, Ez.getDataPointer(), size * sizeof(float));
+  }
+  return 0;
+}
+
+// CpuGaussCharge::calcDipoleSum, ct as above; dip receives (x, y, z).
+int ref_dipole(int ct, int sx, int sy, int sz, double boxx, double boxy, double boxz,
+               const void* rho_in, double* dip) {
+  const size_t size = (size_t)sx * sy * sz;
+  if (ct == 0) {
+    CpuGaussCharge<double, double> gc(sx, sy, sz);
+    CpuGrid<double> rho(sx, sy, sz);
+    std::memcpy(rho.getDataPointer(), rho_in, size * sizeof(double));
+    gc.calcDipoleSum(boxx, boxy, boxz, rho, dip[0], dip[1], dip[2]);
+  } else {
+    CpuGaussCharge<double, float> gc(sx, sy, sz);
+    CpuGrid<float> rho(sx, sy, sz);
+    std::memcpy(rho.getDataPointer(), rho_in, size * sizeof(float));
+    gc.calcDipoleSum(boxx, boxy, boxz, rho, dip[0], dip[1], dip[2]);
+  }
+  return 0;
+}
+
 // CpuGreensFuncGSE<double>::mul on an interleaved half spectrum.
 int ref_green_mul_d(int nx, int ny, int nz, double boxx, double boxy, double boxz, double sigma,
                     double* rhoK) {

@@ -29,6 +29,21 @@ def goldens():
     return load_goldens()
 
 
+def load_grid_goldens():
+    """Cases of tests/golden/grid_ops_goldens.npz (make_grid_ops_goldens.py)."""
+    z = np.load(os.path.join(GOLDEN, "grid_ops_goldens.npz"))
+    cases = {}
+    for k in z.files:
+        name, field = k.split("/")
+        cases.setdefault(name, {})[field] = z[k]
+    return cases
+
+
+@pytest.fixture(scope="session")
+def grid_goldens():
+    return load_grid_goldens()
+
+
 @pytest.fixture(scope="session")
 def oracle_lib():
     import oracle

@@ -99,3 +99,46 @@ def test_dropin_64cubed_green_multiply_inside_the_fft(tmp_path, precision, tol):
     print(precision, abs(E - float(z["E"])) / abs(float(z["E"])), rms(F, z["F"]))
     assert abs(E - float(z["E"])) <= tol * abs(float(z["E"]))
     assert rms(F, z["F"]) <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,dt", [("fp64", np.float64), ("mixed", np.float32)])
+def test_dropin_grid_operations(goldens, tmp_path, precision, dt):
+    """CpuGaussCharge::spreadChargeOnGrid (the real-space variant's second
+    spreading, sigma2), calcElectricFieldOnGrid and calcDipoleSum called by
+    a C++ caller on the grids of its own evaluation, against the oracle
+    restatement of the same reference methods: the grids bit for bit, the
+    dipole within 1e-12 of the sum of its |terms|."""
+    import oracle
+    g = goldens["water300_noncubic"]
+    M = tuple(int(v) for v in g["M"])
+    box = tuple(float(v) for v in g["box"])
+    L = dict(os.environ, GSE_CHECK_GRID_OPS="1")
+    path = tmp_path / "xyzq.txt"
+    np.savetxt(path, g["xyzq"], fmt="%.17g")
+    out = subprocess.run([program(), precision, *map(str, M), *map(repr, box),
+                          repr(float(g["sigma"])), str(path)], capture_output=True, text=True,
+                         timeout=300, env=L)
+    assert out.returncode == 0, out.stderr
+    dip = None
+    rows = []
+    for line in out.stdout.splitlines():
+        tag, *vals = line.split()
+        if tag == "DIP":
+            dip = np.array([float(v) for v in vals])
+        elif tag == "G":
+            rows.append([float(v) for v in vals])
+    G = np.array(rows).astype(dt)
+    assert G.shape == (M[0] * M[1] * M[2], 6)
+    rho, phi, rhoS, ex, ey, ez = (G[:, k].reshape(M[::-1]) for k in range(6))
+    _, s2, _ = oracle.gse_params(float(g["sigma"]))
+    rc2 = 3.0 * np.sqrt(2.0) * s2
+    assert np.array_equal(rhoS, oracle.spread_on_grid(M, box, s2, rc2, rho, dt))
+    for e, w in zip((ex, ey, ez), oracle.efield(M, box, phi, dt)):
+        assert np.array_equal(e, w)
+    ref = oracle.dipole_sum(M, box, rho, dt)
+    h = np.array(box) / np.array(M)
+    z, y, x = np.meshgrid(*(np.arange(m) for m in M[::-1]), indexing="ij")
+    v = np.abs(rho.astype(np.float64)) * h.prod()
+    scale = np.array([(v * x * h[0]).sum(), (v * y * h[1]).sum(), (v * z * h[2]).sum()])
+    assert (np.abs(dip - ref) <= 1e-12 * scale).all()

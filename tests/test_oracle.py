@@ -8,9 +8,10 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_goldens
+from conftest import GOLDEN, load_goldens, load_grid_goldens
 
 CASES = sorted(load_goldens().keys())
+GRID_CASES = sorted(load_grid_goldens().keys())
 
 
 @pytest.mark.parametrize("shape", [(20, 20, 20), (16, 18, 20), (7, 9, 11), (5, 6, 9), (13, 1, 4),
@@ -51,6 +52,23 @@ def test_restatement_float_stages_equal_reference(oracle_lib, goldens, case):
     assert np.array_equal(F, g["F_f"])
     rho_n = oracle_lib.spread(M, box, s1, rc, g["xyzq"], normalize=True)
     assert np.array_equal(rho_n, g["rho_norm"])
+
+
+@pytest.mark.parametrize("case", GRID_CASES)
+@pytest.mark.parametrize("sfx,dt", [("d", np.float64), ("f", np.float32)])
+def test_restatement_grid_ops_equal_reference(oracle_lib, grid_goldens, case, sfx, dt):
+    """spreadChargeOnGrid, calcElectricFieldOnGrid and calcDipoleSum restated:
+    the same operations in the same order, bit-identical to the reference."""
+    g = grid_goldens[case]
+    M, box = tuple(int(v) for v in g["M"]), tuple(float(v) for v in g["box"])
+    rho = g["rho_" + sfx]
+    assert rho.dtype == dt
+    out = oracle_lib.spread_on_grid(M, box, float(g["sigma"]), float(g["rcut"]), rho, dt)
+    assert np.array_equal(out, g["rhoS_" + sfx])
+    E = oracle_lib.efield(M, box, rho, dt)
+    for e, k in zip(E, ("Ex_", "Ey_", "Ez_")):
+        assert np.array_equal(e, g[k + sfx])
+    assert np.array_equal(oracle_lib.dipole_sum(M, box, rho, dt), g["dip_" + sfx])
 
 
 def test_restatement_green_equals_reference(oracle_lib):
