@@ -38,10 +38,10 @@ __device__ __forceinline__ int wrap_any(int v, int m) {
 // run and its 2n-point halo are read into shared memory by independent
 // coalesced loads (several per lane in flight), then each lane sums the taps
 // of its outputs from there.
-constexpr int kConvRunX = 128;
+constexpr int kConvRunX = 160;
 // y and z passes: a CTA of 32 x 8 threads takes 32 x-columns by kConvRun
 // outputs along the axis; the kConvRun + 2n rows it needs are staged first.
-constexpr int kConvRun = 64;
+constexpr int kConvRun = 72;
 
 template <typename CT>
 __global__ void __launch_bounds__(256)
@@ -101,21 +101,19 @@ __global__ void __launch_bounds__(256)
 }
 
 // The same two passes for a tap count W known at compile time: the taps sit
-// in registers and the tap loops unroll, and the CTAs are persistent.  Each
-// one walks its share of the tiles and issues the loads of its next tile
-// before it sums the current one, so the memory system is busy while the
-// sums are formed.  The y/z kernel gives each thread kConvK consecutive
-// outputs, one window of kConvK + W - 1 staged values in registers feeding
-// kConvK independent sums; in the x kernel a warp takes one row run per tile
-// and each lane the outputs lane, lane + 32, ...
-constexpr int kConvK = 8;
+// in registers, the tap loops unroll and each thread issues all of its loads
+// before it stores any of them to shared memory, so that they are in flight
+// together.  The y/z kernel gives each thread kConvK consecutive outputs, one
+// window of kConvK + W - 1 staged values in registers feeding kConvK
+// independent sums; in the x kernel each warp takes one row run and each
+// lane the outputs lane, lane + 32, ...
+constexpr int kConvK = 9;
 static_assert(kConvK * 8 == kConvRun, "8 rows of threads cover one run");
-constexpr int kConvCtas = 148 * 3;  // all resident at once (<= 80 registers, <= 19 KB shared)
 
 template <typename CT, int W>
 __global__ void __launch_bounds__(256)
     k_conv_x_w(const CT* __restrict__ in, CT* __restrict__ out, int mx, long long rows, int run,
-               int nruns, ConvTaps<CT> taps) {
+               ConvTaps<CT> taps) {
   constexpr int n = (W - 1) / 2;
   constexpr int NL = (kConvRunX + W - 1 + 31) / 32;
   __shared__ CT buf[8][kConvRunX + W];
@@ -123,44 +121,33 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
   for (int t = 0; t < W; t++) g[t] = taps.g[t];
   const int lane = threadIdx.x, wp = threadIdx.y;
-  const long long ntiles = rows * nruns;
-  const long long step = (long long)gridDim.x * 8;
+  const long long r = (long long)blockIdx.x * 8 + wp;
+  if (r >= rows) return;
+  const int x0 = blockIdx.y * run;
+  const int len = min(run, mx - x0);
+  if (len <= 0) return;
+  const CT* row = in + r * mx;
   CT* b = buf[wp];
   CT ld[NL];
-  auto fetch = [&](long long t) {
-    const long long r = t / nruns;
-    const int x0 = (int)(t - r * nruns) * run;
-    const int len = min(run, mx - x0);
-    const CT* row = in + r * mx;
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-      const int i = lane + 32 * k;
-      ld[k] = i < len + 2 * n ? row[wrap_any(x0 - n + i, mx)] : (CT)0;
-    }
-  };
-  long long t = (long long)blockIdx.x * 8 + wp;
-  if (t < ntiles) fetch(t);
-  for (; t < ntiles; t += step) {
-    const long long r = t / nruns;
-    const int x0 = (int)(t - r * nruns) * run;
-    const int len = min(run, mx - x0);
-    __syncwarp();  // the previous tile's sums have read the buffer
+  for (int k = 0; k < NL; k++) {
+    const int i = lane + 32 * k;
+    ld[k] = i < len + 2 * n ? row[wrap_any(x0 - n + i, mx)] : (CT)0;
+  }
 #pragma unroll
-    for (int k = 0; k < NL; k++) {
-      const int i = lane + 32 * k;
-      if (i < len + 2 * n) b[i] = ld[k];
-    }
-    __syncwarp();
-    if (t + step < ntiles) fetch(t + step);
+  for (int k = 0; k < NL; k++) {
+    const int i = lane + 32 * k;
+    if (i < len + 2 * n) b[i] = ld[k];
+  }
+  __syncwarp();
 #pragma unroll
-    for (int k = 0; k < kConvRunX / 32; k++) {
-      const int i = lane + 32 * k;
-      if (i < len) {
-        CT s = (CT)0;
+  for (int k = 0; k < kConvRunX / 32; k++) {
+    const int i = lane + 32 * k;
+    if (i < len) {
+      CT s = (CT)0;
 #pragma unroll
-        for (int u = 0; u < W; u++) s = add_rn(s, mul_rn(g[u], b[i + u]));
-        out[r * mx + x0 + i] = s;
-      }
+      for (int t = 0; t < W; t++) s = add_rn(s, mul_rn(g[t], b[i + t]));
+      out[r * mx + x0 + i] = s;
     }
   }
 }
@@ -168,70 +155,49 @@ __global__ void __launch_bounds__(256)
 template <typename CT, int W>
 __global__ void __launch_bounds__(256)
     k_conv_yz_w(const CT* __restrict__ in, CT* __restrict__ out, int mx, int my, int mz,
-                int axis, int run, int nruns, ConvTaps<CT> taps) {
+                int axis, int run, ConvTaps<CT> taps) {
   constexpr int n = (W - 1) / 2;
   constexpr int NL = (kConvRun + W - 1 + 7) / 8;
   __shared__ CT buf[kConvRun + W - 1][33];
   CT g[W];
 #pragma unroll
-  for (int u = 0; u < W; u++) g[u] = taps.g[u];
+  for (int t = 0; t < W; t++) g[t] = taps.g[t];
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int ma = axis == 1 ? my : mz, other = axis == 1 ? mz : my;
+  const int ma = axis == 1 ? my : mz;
   const long long stride = axis == 1 ? (long long)mx : (long long)mx * my;
   const long long ostride = axis == 1 ? (long long)mx * my : (long long)mx;
-  const int nxb = (mx + 31) / 32;
-  const long long ntiles = (long long)nxb * nruns * other;
-  // tile t: x block t % nxb, run (t / nxb) % nruns, other-axis index t / (nxb nruns)
-  CT ld[NL];
-  auto fetch = [&](long long t) {
-    const int xb = (int)(t % nxb);
-    const long long q = t / nxb;
-    const int a0 = (int)(q % nruns) * run;
-    const long long o = q / nruns;
-    const int x = xb * 32 + tx;
-    const int len = min(run, ma - a0);
-    const CT* base = in + o * ostride + x;
+  const int x = blockIdx.x * 32 + tx;
+  const int a0 = blockIdx.y * run;
+  const int len = min(run, ma - a0);
+  const CT* base = in + (long long)blockIdx.z * ostride + x;
+  if (x < mx) {
+    CT ld[NL];
 #pragma unroll
     for (int k = 0; k < NL; k++) {
       const int i = ty + 8 * k;
-      ld[k] = (x < mx && i < len + 2 * n) ? base[(long long)wrap_any(a0 - n + i, ma) * stride]
-                                           : (CT)0;
+      ld[k] = i < len + 2 * n ? base[(long long)wrap_any(a0 - n + i, ma) * stride] : (CT)0;
     }
-  };
-  long long t = blockIdx.x;
-  if (t < ntiles) fetch(t);
-  for (; t < ntiles; t += gridDim.x) {
-    const int xb = (int)(t % nxb);
-    const long long q = t / nxb;
-    const int a0 = (int)(q % nruns) * run;
-    const long long o = q / nruns;
-    const int x = xb * 32 + tx;
-    const int len = min(run, ma - a0);
-    __syncthreads();  // the previous tile's sums have read the buffer
 #pragma unroll
     for (int k = 0; k < NL; k++) {
       const int i = ty + 8 * k;
       if (i < len + 2 * n) buf[i][tx] = ld[k];
     }
-    __syncthreads();
-    if (t + gridDim.x < ntiles) fetch(t + gridDim.x);
-    const int i0 = ty * kConvK;
-    if (x < mx && i0 < len) {
-      // rows past len + 2n were not staged; they feed only outputs past len
-      CT v[kConvK + W - 1];
+  }
+  __syncthreads();
+  const int i0 = ty * kConvK;
+  if (x >= mx || i0 >= len) return;
+  // rows past len + 2n were not staged; they feed only outputs past len
+  CT v[kConvK + W - 1];
 #pragma unroll
-      for (int j = 0; j < kConvK + W - 1; j++)
-        v[j] = i0 + j < len + 2 * n ? buf[i0 + j][tx] : (CT)0;
-      CT* obase = out + o * ostride + x;
+  for (int j = 0; j < kConvK + W - 1; j++) v[j] = i0 + j < len + 2 * n ? buf[i0 + j][tx] : (CT)0;
+  CT* obase = out + (long long)blockIdx.z * ostride + x;
 #pragma unroll
-      for (int k = 0; k < kConvK; k++) {
-        if (i0 + k < len) {
-          CT s = (CT)0;
+  for (int k = 0; k < kConvK; k++) {
+    if (i0 + k < len) {
+      CT s = (CT)0;
 #pragma unroll
-          for (int u = 0; u < W; u++) s = add_rn(s, mul_rn(g[u], v[k + u]));
-          obase[(long long)(a0 + i0 + k) * stride] = s;
-        }
-      }
+      for (int t = 0; t < W; t++) s = add_rn(s, mul_rn(g[t], v[k + t]));
+      obase[(long long)(a0 + i0 + k) * stride] = s;
     }
   }
 }
@@ -346,43 +312,39 @@ cudaError_t launch_conv_pass(const CT* in, CT* out, const int M[3], int axis,
   if (taps.n < 0 || 2 * taps.n + 1 > kMaxStencil || axis < 0 || axis > 2)
     return cudaErrorInvalidValue;
   const int W = 2 * taps.n + 1;
+  const dim3 blk(32, 8);
   if (axis == 0) {
     const long long rows = (long long)M[1] * M[2];
     const int nruns = (M[0] + kConvRunX - 1) / kConvRunX;
     const int run = (M[0] + nruns - 1) / nruns;
     const long long groups = (rows + 7) / 8;
     if (groups > 0x7fffffffLL || nruns > 65535) return cudaErrorInvalidValue;
-    const dim3 blk(32, 8);
-    const unsigned ctas = (unsigned)std::min<long long>((rows * nruns + 7) / 8, kConvCtas);
+    const dim3 grid((unsigned)groups, nruns);
     switch (W) {
 #define CONV_X(WW) \
   case WW:         \
-    k_conv_x_w<CT, WW><<<ctas, blk, 0, st>>>(in, out, M[0], rows, run, nruns, taps); \
+    k_conv_x_w<CT, WW><<<grid, blk, 0, st>>>(in, out, M[0], rows, run, taps); \
     break;
       CONV_X(5) CONV_X(7) CONV_X(9) CONV_X(11) CONV_X(13) CONV_X(15)
 #undef CONV_X
       default:
-        k_conv_x<CT><<<dim3((unsigned)groups, nruns), blk, 0, st>>>(in, out, M[0], rows, run,
-                                                                     taps);
+        k_conv_x<CT><<<grid, blk, 0, st>>>(in, out, M[0], rows, run, taps);
     }
   } else {
     const int ma = axis == 1 ? M[1] : M[2], other = axis == 1 ? M[2] : M[1];
     const int nruns = (ma + kConvRun - 1) / kConvRun;
     const int run = (ma + nruns - 1) / nruns;
-    const dim3 blk(32, 8);
-    const long long ntiles = (long long)((M[0] + 31) / 32) * nruns * other;
-    const unsigned ctas = (unsigned)std::min<long long>(ntiles, kConvCtas);
+    if (other > 65535 || nruns > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((M[0] + 31) / 32, nruns, other);
     switch (W) {
 #define CONV_YZ(WW) \
   case WW:          \
-    k_conv_yz_w<CT, WW><<<ctas, blk, 0, st>>>(in, out, M[0], M[1], M[2], axis, run, nruns, taps); \
+    k_conv_yz_w<CT, WW><<<grid, blk, 0, st>>>(in, out, M[0], M[1], M[2], axis, run, taps); \
     break;
       CONV_YZ(5) CONV_YZ(7) CONV_YZ(9) CONV_YZ(11) CONV_YZ(13) CONV_YZ(15)
 #undef CONV_YZ
       default:
-        if (other > 65535 || nruns > 65535) return cudaErrorInvalidValue;
-        k_conv_yz<CT><<<dim3((M[0] + 31) / 32, nruns, other), blk, 0, st>>>(
-            in, out, M[0], M[1], M[2], axis, run, taps);
+        k_conv_yz<CT><<<grid, blk, 0, st>>>(in, out, M[0], M[1], M[2], axis, run, taps);
     }
   }
   return cudaGetLastError();
