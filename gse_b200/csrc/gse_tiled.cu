@@ -697,8 +697,9 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         wx[k] = tb[(0 * 3 + 2) * kWPad + k];
         wdx[k] = wx[k] * tb[(0 * 3 + 0) * kWPad + k];
       }
-      // rows accumulate in double (the reference's AT), each row's 2n+1 terms in CT
-      double ax = 0, ay = 0, az = 0;
+      // each row's 2n+1 terms and a lane's rows (about rows/16 of them) in CT, the
+      // lanes' sums in double (the reference's AT)
+      CT lx = 0, ly = 0, lz = 0;
       for (int i = gl; i < nrow; i += GL) {
         const int r = rl[i];
         const int jz = r >> 8, jy = r & 255;
@@ -708,10 +709,11 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         CT s0, s1;
         row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
         const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
-        ax += (double)(wyz * s1);
-        ay += (double)(wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0);
-        az += (double)(wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0);
+        lx += wyz * s1;
+        ly += wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0;
+        lz += wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0;
       }
+      double ax = (double)lx, ay = (double)ly, az = (double)lz;
 #pragma unroll
       for (int o = GL / 2; o > 0; o >>= 1) {
         ax += __shfl_xor_sync(0xffffffffu, ax, o);
