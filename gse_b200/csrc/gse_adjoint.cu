@@ -436,8 +436,9 @@ __device__ __forceinline__ void adj_gather_brick(
         const float eu = e * tb[(0 * 3 + 0) * kWPad + k];
         asm("mov.b64 %0, {%1, %2};" : "=l"(w2[k]) : "f"(e), "f"(eu));
       }
-      // cube rows of Psi: P = sum e Psi, V = sum e Psi u
-      double P = 0.0, Vx = 0.0, Vy = 0.0, Vz = 0.0;
+      // cube rows of Psi: P = sum e Psi, V = sum e Psi u (a lane's rows summed in
+      // FP32, the lanes' sums in FP64 below)
+      float P = 0.f, Vx = 0.f, Vy = 0.f, Vz = 0.f;
 #pragma unroll
       for (int g = 0; g < NG; g++) {
         if (g * GL + gl < W * W) {
@@ -454,10 +455,10 @@ __device__ __forceinline__ void adj_gather_brick(
           asm("mov.b64 {%0, %1}, %2;" : "=f"(r0), "=f"(r1) : "l"(acc));
           const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
           const float a0 = w * r0;
-          P += (double)a0;
-          Vx += (double)(w * r1);
-          Vy += (double)(a0 * tb[(1 * 3 + 0) * kWPad + jy]);
-          Vz += (double)(a0 * tb[(2 * 3 + 0) * kWPad + jz]);
+          P += a0;
+          Vx += w * r1;
+          Vy += a0 * tb[(1 * 3 + 0) * kWPad + jy];
+          Vz += a0 * tb[(2 * 3 + 0) * kWPad + jz];
         }
       }
       // sphere rows of phi
@@ -481,8 +482,8 @@ __device__ __forceinline__ void adj_gather_brick(
         asm("mov.b64 {%0, %1}, %2;" : "=f"(ex[k]), "=f"(eux[k]) : "l"(w2[k]));
         eu2[k] = ex[k] * dx2[k];
       }
-      double T0 = 0, T1x = 0, T1y = 0, T1z = 0;
-      double Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
+      float T0 = 0, T1x = 0, T1y = 0, T1z = 0;
+      float Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
       for (int i = gl; i < nrow; i += GL) {
         const int r = rl[i];
         const int jz = r >> 8, jy = r & 255;
@@ -502,16 +503,16 @@ __device__ __forceinline__ void adj_gather_brick(
         const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
         const float uy = tb[(1 * 3 + 0) * kWPad + jy], uz = tb[(2 * 3 + 0) * kWPad + jz];
         const float a0 = w * s0, a1 = w * s1;
-        T0 += (double)a0;
-        T1x += (double)a1;
-        T1y += (double)(a0 * uy);
-        T1z += (double)(a0 * uz);
-        Mxx += (double)(w * s2);
-        Mxy += (double)(a1 * uy);
-        Mxz += (double)(a1 * uz);
-        Myy += (double)(a0 * uy2);
-        Myz += (double)(a0 * uy * uz);
-        Mzz += (double)(a0 * uz2);
+        T0 += a0;
+        T1x += a1;
+        T1y += a0 * uy;
+        T1z += a0 * uz;
+        Mxx += w * s2;
+        Mxy += a1 * uy;
+        Mxz += a1 * uz;
+        Myy += a0 * uy2;
+        Myz += a0 * uy * uz;
+        Mzz += a0 * uz2;
       }
       double acc14[14] = {P, Vx, Vy, Vz, T0, T1x, T1y, T1z, Mxx, Mxy, Mxz, Myy, Myz, Mzz};
 #pragma unroll
