@@ -18,6 +18,8 @@
 //           + c q_j A sum_{sphere} e phi [G_j - (G_j . u) u / s^2],
 // e = exp(-|u|^2 / (2 s^2)).  The sphere's edge is not differentiated (its
 // derivative is zero almost everywhere).
+#include <type_traits>
+
 #include "gse_adjoint.cuh"
 #include "gse_internal.cuh"
 #include "gse_tiled.cuh"
@@ -484,6 +486,10 @@ __device__ __forceinline__ void adj_gather_brick(
       }
       float T0 = 0, T1x = 0, T1y = 0, T1z = 0;
       float Mxx = 0, Mxy = 0, Mxz = 0, Myy = 0, Myz = 0, Mzz = 0;
+      // the end points lie outside the sphere for every row when dx^2 >= rcut^2
+      // there (rem <= rcut^2): the rows are then summed over the inner points
+      const bool ends = dx2[0] < sg.rcut2 || dx2[W - 1] < sg.rcut2;
+      const bool trim = !__any_sync(0xffffffffu, ends);
       for (int i = gl; i < nrow; i += GL) {
         const int r = rl[i];
         const int jz = r >> 8, jy = r & 255;
@@ -491,15 +497,23 @@ __device__ __forceinline__ void adj_gather_brick(
         const float rem = sg.rcut2 - (uy2 + uz2);
         const float* row = tphi + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
         float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+        auto pts = [&](auto tr) {
+          constexpr int K0 = decltype(tr)::value ? 1 : 0;
+          constexpr int K1 = decltype(tr)::value ? W - 1 : W;
 #pragma unroll
-        for (int k = 0; k < W; k++) {
-          const float ph = row[k];
-          if (dx2[k] < rem) {  // the test guards the fmas; a skipped point adds nothing
-            s0 = fmaf(ex[k], ph, s0);
-            s1 = fmaf(eux[k], ph, s1);
-            s2 = fmaf(eu2[k], ph, s2);
+          for (int k = K0; k < K1; k++) {
+            const float ph = row[k];
+            if (dx2[k] < rem) {  // the test guards the fmas; a skipped point adds nothing
+              s0 = fmaf(ex[k], ph, s0);
+              s1 = fmaf(eux[k], ph, s1);
+              s2 = fmaf(eu2[k], ph, s2);
+            }
           }
-        }
+        };
+        if (trim)
+          pts(std::true_type());
+        else
+          pts(std::false_type());
         const float w = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
         const float uy = tb[(1 * 3 + 0) * kWPad + jy], uz = tb[(2 * 3 + 0) * kWPad + jz];
         const float a0 = w * s0, a1 = w * s1;

@@ -183,9 +183,16 @@ __device__ __forceinline__ void block_sum_to(double v, double* partials) {
 // partials[gridDim.x], zero between launches) adds the partials in index
 // order -- the result does not depend on which block ran when -- and writes
 // factor * sum to out[0].
+__device__ __forceinline__ void last_block_sum_counter(double* partials, unsigned* done,
+                                                       double factor, double* out);
 __device__ __forceinline__ void last_block_sum(double* partials, double factor, double* out) {
+  last_block_sum_counter(partials, reinterpret_cast<unsigned*>(partials + gridDim.x), factor,
+                         out);
+}
+// As last_block_sum with the counter at `done`.
+__device__ __forceinline__ void last_block_sum_counter(double* partials, unsigned* done,
+                                                       double factor, double* out) {
   __shared__ bool last;
-  unsigned* done = reinterpret_cast<unsigned*>(partials + gridDim.x);
   if (threadIdx.x == 0) {
     __threadfence();
     last = atomicAdd(done, 1u) == gridDim.x - 1;
@@ -335,35 +342,72 @@ __global__ void __launch_bounds__(256)
 }
 
 // factor * sum_i (double)(a[i]*b[i]) (the product in CT, as CpuGSE.cpp:97),
-// finished by the last block
+// finished by the last block.  done is the zeroed counter the last block
+// resets (the slot after the partials that the other energy kernels use).
 template <typename CT>
 __global__ void __launch_bounds__(256)
     k_dot(const CT* __restrict__ a, const CT* __restrict__ b, long long size,
-          double* __restrict__ partials, double factor, double* __restrict__ out) {
-  double e = 0.0;
+          double* __restrict__ partials, unsigned* __restrict__ done, double factor,
+          double* __restrict__ out) {
+  // four independent partial sums, each step's loads issued together
+  double e[4] = {0.0, 0.0, 0.0, 0.0};
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if constexpr (sizeof(CT) == 4) {
-    // four points per thread and step, 16-byte loads (cudaMalloc'd grids)
+    // four points per 16-byte load (cudaMalloc'd grids), four loads per step
     const long long quads = size / 4;
     const float4* a4 = reinterpret_cast<const float4*>(a);
     const float4* b4 = reinterpret_cast<const float4*>(b);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < quads;
-         i += (long long)gridDim.x * blockDim.x) {
-      const float4 u = a4[i], v = b4[i];
-      e += (double)(u.x * v.x);
-      e += (double)(u.y * v.y);
-      e += (double)(u.z * v.z);
-      e += (double)(u.w * v.w);
+    for (long long i = t0; i < quads; i += 4 * stride) {
+      float4 u[4], v[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const long long j = i + k * stride;
+        if (j < quads) {
+          u[k] = a4[j];
+          v[k] = b4[j];
+        } else {
+          u[k] = v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        e[k] += (double)(u[k].x * v[k].x);
+        e[k] += (double)(u[k].y * v[k].y);
+        e[k] += (double)(u[k].z * v[k].z);
+        e[k] += (double)(u[k].w * v[k].w);
+      }
     }
     if (blockIdx.x == 0)
       for (long long i = quads * 4 + threadIdx.x; i < size; i += blockDim.x)
-        e += (double)(a[i] * b[i]);
+        e[0] += (double)(a[i] * b[i]);
   } else {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < size;
-         i += (long long)gridDim.x * blockDim.x)
-      e += (double)(a[i] * b[i]);
+    const long long pairs = size / 2;
+    const double2* a2 = reinterpret_cast<const double2*>(a);
+    const double2* b2 = reinterpret_cast<const double2*>(b);
+    for (long long i = t0; i < pairs; i += 4 * stride) {
+      double2 u[4], v[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const long long j = i + k * stride;
+        if (j < pairs) {
+          u[k] = a2[j];
+          v[k] = b2[j];
+        } else {
+          u[k] = v[k] = make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        e[k] += u[k].x * v[k].x;
+        e[k] += u[k].y * v[k].y;
+      }
+    }
+    if (blockIdx.x == 0)
+      for (long long i = pairs * 2 + threadIdx.x; i < size; i += blockDim.x) e[0] += a[i] * b[i];
   }
-  block_sum_to(e, partials);
-  last_block_sum(partials, factor, out);
+  block_sum_to((e[0] + e[1]) + (e[2] + e[3]), partials);
+  last_block_sum_counter(partials, done, factor, out);
 }
 
 __global__ void k_energy_finalize(const double* __restrict__ partials, int np, double factor,
@@ -533,7 +577,10 @@ cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, con
 template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st) {
-  k_dot<CT><<<np, 256, 0, st>>>(a, b, size, partials, factor, energy_out);
+  // fewer, fuller blocks than the other energy kernels; the counter stays in
+  // the slot after np partials that they use
+  k_dot<CT><<<std::min(np, 148 * 4), 256, 0, st>>>(
+      a, b, size, partials, reinterpret_cast<unsigned*>(partials + np), factor, energy_out);
   return cudaGetLastError();
 }
 

@@ -18,6 +18,8 @@
 //            potential of the brick plus its n-cell halo in shared memory;
 //            kGatherLanes lanes per atom, over the non-empty (y, z) rows of
 //            its sphere.
+#include <type_traits>
+
 #include "gse_internal.cuh"
 #include "gse_tiled.cuh"
 #include "gse_tiled_dev.cuh"
@@ -552,13 +554,13 @@ __device__ __forceinline__ bool in_sphere<float>(float dx2, float, float, float 
 // s0 = sum_k m_k wx[k] row[k], s1 = sum_k m_k wx[k] dx[k] row[k] over the
 // 2n+1 points of one stencil row, m_k the sphere test.  The test guards the
 // two fmas (predicated, no select); a skipped point adds exactly nothing.
-template <typename CT, int W>
+template <typename CT, int W, int K0 = 0, int K1 = W>
 __device__ __forceinline__ void row_sums(const CT* row, const CT (&dx2)[W], const CT (&wx)[W],
                                          const CT (&wdx)[W], CT dy2, CT dz2, CT rem, CT rcut2,
                                          CT& s0, CT& s1) {
   CT a = (CT)0, c = (CT)0;
 #pragma unroll
-  for (int k = 0; k < W; k++) {
+  for (int k = K0; k < K1; k++) {
     const CT ph = row[k];
     if (in_sphere<CT>(dx2[k], dy2, dz2, rem, rcut2)) {
       a = fma(wx[k], ph, a);
@@ -700,19 +702,31 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
       // each row's 2n+1 terms and a lane's rows (about rows/16 of them) in CT, the
       // lanes' sums in double (the reference's AT)
       CT lx = 0, ly = 0, lz = 0;
-      for (int i = gl; i < nrow; i += GL) {
-        const int r = rl[i];
-        const int jz = r >> 8, jy = r & 255;
-        const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
-        const CT rem = s.rcut2 - (dy2 + dz2);
-        const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
-        CT s0, s1;
-        row_sums<CT, W>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
-        const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
-        lx += wyz * s1;
-        ly += wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0;
-        lz += wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0;
-      }
+      // the end points of the rows lie outside the sphere for every row when
+      // dx^2 >= rcut^2 there (rem <= rcut^2): then the rows are summed over
+      // the inner 2n-1 points only, the same terms in the same order
+      const bool ends = dx2[0] < s.rcut2 || dx2[W - 1] < s.rcut2;
+      auto rows = [&](auto trim) {
+        constexpr int K0 = decltype(trim)::value ? 1 : 0;
+        constexpr int K1 = decltype(trim)::value ? W - 1 : W;
+        for (int i = gl; i < nrow; i += GL) {
+          const int r = rl[i];
+          const int jz = r >> 8, jy = r & 255;
+          const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
+          const CT rem = s.rcut2 - (dy2 + dz2);
+          const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
+          CT s0, s1;
+          row_sums<CT, W, K0, K1>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
+          const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
+          lx += wyz * s1;
+          ly += wyz * tb[(1 * 3 + 0) * kWPad + jy] * s0;
+          lz += wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0;
+        }
+      };
+      if (__any_sync(0xffffffffu, ends))
+        rows(std::false_type());
+      else
+        rows(std::true_type());
       double ax = (double)lx, ay = (double)ly, az = (double)lz;
 #pragma unroll
       for (int o = GL / 2; o > 0; o >>= 1) {
