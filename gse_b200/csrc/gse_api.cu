@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -20,6 +21,7 @@
 #include "gse_kernels.cuh"
 #include "gse_adjoint.cuh"
 #include "gse_ewald.cuh"
+#include "gse_fft.cuh"
 #include "gse_grid_ops.cuh"
 #include "gse_tiled.cuh"
 #include "gse_green_cb_fatbin.h"  // generated: the c2r load callbacks as LTO code
@@ -138,6 +140,11 @@ struct gse_context {
   cufftHandle plan_bg = 0;
   bool green_cb = false;     // plan_bg exists and is used
   bool green_cb_tried = false;
+  // the mixed form's own 3-D FFT solve (cubic M = 16 N2): its twiddles, and
+  // whether the float rho grid still has to be made from the int64 grid
+  float2* d_fft_tw = nullptr;
+  bool own_fft = false;
+  bool fixed_pending = false;
   bool rho_valid = false, phi_valid = false, energy_valid = false;
   // replay of repeated gse_forward calls with device inputs and outputs: the
   // second identical call is captured into a CUDA graph, later ones launch it
@@ -319,8 +326,11 @@ bool tiled_ok(const gse_context_t* c, const Stencil<CT>& s) {
 // Spread into c->d_rho.  `presorted`: c->d_sorted / d_bstart already hold the
 // binned atoms of this call.
 template <typename CT>
+// `defer_rho`: with the own FFT, leave the float grid to the solve that
+// follows (it reads the int64 grid directly and writes rho on the way).
 gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
-                       double rcut, bool normalize, bool presorted = false) {
+                       double rcut, bool normalize, bool presorted = false,
+                       bool defer_rho = false) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
   if (!normalize && tiled_ok<CT>(c, s)) {
@@ -331,9 +341,11 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
       CU(launch_spread_tiled<CT>((const V*)c->d_sorted, c->d_bstart, c->d_qmax, c->bl, s,
                                  (CT*)c->d_rho, c->stream));
     } else if constexpr (sizeof(CT) == 4) {
-      c->launches += 2;
+      const bool defer = defer_rho && c->own_fft;
+      c->launches += defer ? 1 : 2;
       CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl, s, c->d_fixed,
-                               (float*)c->d_rho, c->stream));
+                               defer ? nullptr : (float*)c->d_rho, c->stream));
+      c->fixed_pending = defer;
     }
   } else {
     StageTimer tm(c, GSE_STAGE_SPREAD);
@@ -464,6 +476,37 @@ bool make_green_callback_plan(gse_context_t* c) {
 gse_status_t do_solve_ctx(gse_context_t* c) {
   const GreenGeom g = green_geom(c, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, true);
   if (!c->d_gtab) CU(cudaMalloc(&c->d_gtab, c->ksize * c->ct));  // fixed address from here on
+  if (c->own_fft) {
+    // mixed form, cubic M = 16 N2: three passes of this library's own FFT;
+    // the Green's multiply and the k-space energy sit in the z pass
+    if (!c->gtab_valid) {
+      CU(launch_green_table<float>(g, (float*)c->d_gtab, c->stream));
+      c->gtab_valid = true;
+    }
+    const int M = c->p.size_x;
+    {
+      StageTimer tm(c, GSE_STAGE_FFT_FORWARD);
+      c->launches += 1;
+      const bool fx = c->fixed_pending;
+      CU(launch_own_fft_xy_forward(M, fx ? c->d_fixed : nullptr, fx ? nullptr : (float*)c->d_rho,
+                                   std::exp2(-(double)kFlushBits), fx ? (float*)c->d_rho : nullptr,
+                                   (float2*)c->d_rhok, c->d_fft_tw, c->stream));
+      c->fixed_pending = false;
+    }
+    {
+      StageTimer tm(c, GSE_STAGE_GREEN);
+      c->launches += 1;
+      CU(launch_own_fft_z_green(M, (float2*)c->d_rhok, (const float*)c->d_gtab, c->d_fft_tw,
+                                c->d_partials,
+                                reinterpret_cast<unsigned*>(c->d_partials + kEnergyPartials),
+                                energy_factor(c), c->d_scalars, c->stream));
+    }
+    StageTimer tm(c, GSE_STAGE_FFT_BACKWARD);
+    c->launches += 1;
+    CU(launch_own_fft_xy_inverse(M, (const float2*)c->d_rhok, (float*)c->d_phi, c->d_fft_tw,
+                                 c->stream));
+    return GSE_OK;
+  }
   if (!c->green_cb_tried && c->size >= kGreenCallbackMinPoints) {
     // linked once, on the first solve outside any stream capture
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -742,6 +785,14 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_phi, c->size * c->ct));
   CUC(cudaMalloc(&c->d_rhok, c->ksize * 2 * c->ct));
   if (!c->fp64) CUC(cudaMalloc(&c->d_fixed, c->size * sizeof(long long)));
+  {
+    const char* env = std::getenv("GSE_B200_OWN_FFT");
+    const bool allowed = !(env && env[0] == '0');
+    if (!c->fp64 && allowed && own_fft_supported(M)) {
+      CUC(make_fft_twiddles(M[0], &c->d_fft_tw));
+      c->own_fft = true;
+    }
+  }
   CUC(cudaMalloc(&c->d_counts, sizeof(int) * c->nbins));
   c->bl = make_bin_layout(M, c->fp64 ? kBinX64 : kBinX32);
   c->nbins2 = bin_count(c->bl);
@@ -789,6 +840,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_rho);
   cudaFree(c->d_phi);
   cudaFree(c->d_rhok);
+  cudaFree(c->d_fft_tw);
   cudaFree(c->d_scratch);
   cudaFree(c->d_fixed);
   cudaFree(c->d_xyzq);
@@ -924,7 +976,7 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
   if (c->fp64)
     TRY(do_spread<double>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));
   else
-    TRY(do_spread<float>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));
+    TRY(do_spread<float>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true, true));
   TRY(do_solve_ctx(c));
   c->phi_valid = true;
   c->energy_valid = true;
@@ -1277,6 +1329,7 @@ gse_status_t gse_get_paths(gse_context_t* c, int* flags) {
               : tiled_ok<float>(c, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false)))
     f |= GSE_PATH_TILED;
   if (c->green_cb) f |= GSE_PATH_GREEN_IN_FFT;
+  if (c->own_fft) f |= GSE_PATH_OWN_FFT;
   if (c->fwd_exec) f |= GSE_PATH_GRAPH;
   *flags = f;
   return GSE_OK;

@@ -1,0 +1,470 @@
+// gse_fft.cu -- the mixed form's own 3-D real FFT solve, for cubic grids of
+// M = 16 * N2 points per side (N2 = 4 .. 12; 144^3 is N2 = 9):
+//
+//   k_own_fft_xy_fwd   one CTA per z plane: int64 (or float) plane -> x r2c of
+//                      two real rows per half-warp complex transform -> y
+//                      transform of each x' column in shared memory -> rho^
+//   k_own_fft_z_green  a CTA per (y, 16 x' columns): z transform, Green's
+//                      multiply and k-space energy, inverse z transform
+//   k_own_fft_xy_inv   one CTA per z plane: inverse y, then the c2r x transform
+//                      of two rows per half-warp complex transform -> phi
+//
+// It replaces, on that path, the int64 -> float conversion pass, the cuFFT
+// r2c and c2r plans (three passes each) and the real-space energy pass: the
+// grid crosses memory three times in each direction instead of six, and the
+// plane passes keep a whole 144 x 73 complex plane in shared memory.
+//
+// Every 1-D transform of length N = 16 N2 is done by the 16 lanes of a
+// half-warp (Cooley-Tukey with N = N2 x 16): lane n1 holds x[n1 + 16 n2] for
+// n2 < N2, takes their N2-point DFT in registers, multiplies by w_N^(n1 k2)
+// and finishes with a 16-point decimation-in-frequency transform across the
+// lanes by shuffles, after which lane l holds X[k2 + N2 brev4(l)].  Twiddles
+// come from tables formed in double.  The transforms are unnormalised and use
+// FFTW's signs (forward e^{-2 pi i kn/N}), so the Green's table and the energy
+// factor are those of the cuFFT path.
+#include "gse_fft.cuh"
+
+#include <cmath>
+#include <vector>
+
+#include "gse_reduce.cuh"
+
+namespace gse {
+
+namespace {
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+__device__ __forceinline__ int brev4(int l) { return (int)(__brev((unsigned)l) >> 28); }
+
+// One complex transform of length 16 N2 by a half-warp (mask: its 16 lanes,
+// l: the lane within it).  In: v[n2] = x[l + 16 n2].  Out: v[k2] = X[k2 + N2 brev4(l)].
+template <int N2, bool INV>
+__device__ __forceinline__ void fft16(float2 (&v)[N2], int l, unsigned mask,
+                                      const float2* __restrict__ tw) {
+  const float2* twnk = tw;                // [16][N2]
+  const float2* tw16 = tw + 16 * N2;      // [16]
+  const float2* twn2 = tw16 + 16;         // [N2]
+  float2 c[N2];
+#pragma unroll
+  for (int m = 0; m < N2; m++) {
+    c[m] = twn2[m];
+    if (INV) c[m].y = -c[m].y;
+  }
+  // N2-point DFT of the lane's own values
+  float2 a[N2];
+#pragma unroll
+  for (int k2 = 0; k2 < N2; k2++) {
+    float re = 0.f, im = 0.f;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; n2++) {
+      const int m = (n2 * k2) % N2;
+      if (m == 0) {
+        re += v[n2].x;
+        im += v[n2].y;
+      } else {
+        re = fmaf(v[n2].x, c[m].x, re);
+        re = fmaf(-v[n2].y, c[m].y, re);
+        im = fmaf(v[n2].x, c[m].y, im);
+        im = fmaf(v[n2].y, c[m].x, im);
+      }
+    }
+    a[k2] = make_float2(re, im);
+  }
+  // twiddle w_N^(l k2)
+#pragma unroll
+  for (int k2 = 1; k2 < N2; k2++) {
+    float2 w = twnk[l * N2 + k2];
+    if (INV) w.y = -w.y;
+    a[k2] = cmul(a[k2], w);
+  }
+  // 16-point decimation in frequency across the lanes
+#pragma unroll
+  for (int h = 8; h >= 1; h >>= 1) {
+    const bool up = (l & h) != 0;
+    float2 w = make_float2(1.f, 0.f);
+    if (h > 1 && up) {
+      w = tw16[(l & (h - 1)) * (8 / h)];
+      if (INV) w.y = -w.y;
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) {
+      const float px = __shfl_xor_sync(mask, a[k2].x, h);
+      const float py = __shfl_xor_sync(mask, a[k2].y, h);
+      const float2 d = up ? make_float2(px - a[k2].x, py - a[k2].y)
+                          : make_float2(a[k2].x + px, a[k2].y + py);
+      a[k2] = (h > 1 && up) ? cmul(d, w) : d;
+    }
+  }
+#pragma unroll
+  for (int k2 = 0; k2 < N2; k2++) v[k2] = a[k2];
+}
+
+// 16 half-warps per plane CTA: with the plane and the scratch rows two CTAs
+// fit an SM up to N2 = 9 (144^3), so one can load while the other transforms
+constexpr int kPlaneThreads = 256;
+constexpr int kHalfWarps = kPlaneThreads / 16;
+constexpr int kColThreads = 256;  // 16 half-warps, one per x' column of a tile
+
+template <int N2>
+constexpr size_t plane_smem() {
+  // the plane [M][M/2+1] complex and one scratch row of M complex per half-warp
+  return sizeof(float2) * ((size_t)(16 * N2) * (8 * N2 + 1) + kHalfWarps * (size_t)(16 * N2));
+}
+
+// dst[i] = src[i] for i < count by the whole CTA, kBatch loads per thread
+// issued before their stores so that they are in flight together.
+constexpr int kBatch = 16;
+__device__ __forceinline__ void copy_in(float2* __restrict__ dst, const float2* __restrict__ src,
+                                        int count) {
+  for (int b0 = threadIdx.x; b0 < count; b0 += kPlaneThreads * kBatch) {
+    float2 t[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; b++) {
+      const int i = b0 + b * kPlaneThreads;
+      t[b] = i < count ? src[i] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; b++) {
+      const int i = b0 + b * kPlaneThreads;
+      if (i < count) dst[i] = t[b];
+    }
+  }
+}
+
+}  // namespace
+
+template <int N2, bool FIXED>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_own_fft_xy_fwd(const long long* __restrict__ g64, const float* __restrict__ rho,
+                     double unscale, float* __restrict__ rho_out, float2* __restrict__ rhok,
+                     const float2* __restrict__ tw) {
+  constexpr int M = 16 * N2, X = M / 2 + 1;  // X is odd: column walks are conflict-free
+  extern __shared__ float2 fsm[];
+  float2* P = fsm;          // [M][X]
+  float2* S = fsm + M * X;  // [kHalfWarps][M]
+  const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
+  const unsigned mask = 0xFFFFu << (tid & 16);
+  const long long plane = (long long)M * M;
+  const long long z0 = (long long)blockIdx.x * plane;
+  float2* Z = S + hw * M;
+  // x: rows 2p and 2p+1 as the real and imaginary parts of one transform
+  for (int pr = hw; pr < M / 2; pr += kHalfWarps) {
+    const long long r0 = z0 + (long long)(2 * pr) * M;
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) {
+      const int x = l + 16 * j;
+      float a, b;
+      if (FIXED) {
+        a = (float)((double)g64[r0 + x] * unscale);
+        b = (float)((double)g64[r0 + M + x] * unscale);
+        if (rho_out) {
+          rho_out[r0 + x] = a;
+          rho_out[r0 + M + x] = b;
+        }
+      } else {
+        a = rho[r0 + x];
+        b = rho[r0 + M + x];
+      }
+      v[j] = make_float2(a, b);
+    }
+    fft16<N2, false>(v, l, mask, tw);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) Z[k2 + N2 * k1] = v[k2];
+    __syncwarp(mask);
+    // X_a = (Z[k] + conj Z[M-k]) / 2, X_b = (Z[k] - conj Z[M-k]) / 2i
+    float2* Pa = P + (2 * pr) * X;
+    float2* Pb = Pa + X;
+    for (int k = l; k < X; k += 16) {
+      const float2 zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
+      Pa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      Pb[k] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+    }
+    __syncwarp(mask);
+  }
+  __syncthreads();
+  // y: each x' column in place
+  for (int col = hw; col < X; col += kHalfWarps) {
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
+    fft16<N2, false>(v, l, mask, tw);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
+  }
+  __syncthreads();
+  float2* out = rhok + (long long)blockIdx.x * M * X;
+  for (int i = tid; i < M * X; i += kPlaneThreads) out[i] = P[i];
+}
+
+template <int N2>
+__global__ void __launch_bounds__(kColThreads)
+    k_own_fft_z_green(float2* __restrict__ rhok, const float* __restrict__ tab,
+                      const float2* __restrict__ tw, double* __restrict__ partials,
+                      unsigned* __restrict__ done, double factor, double* __restrict__ out) {
+  constexpr int M = 16 * N2, X = M / 2 + 1, NXT = (X + 15) / 16;
+  __shared__ float2 Q[M][17];
+  __shared__ float G[M][17];
+  const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
+  const unsigned mask = 0xFFFFu << (tid & 16);
+  const int xt = blockIdx.x % NXT, y = blockIdx.x / NXT;
+  const int x0 = xt * 16, nx = min(16, X - x0);
+  const long long zs = (long long)M * X;
+  const long long base = (long long)y * X + x0;
+  // M * 16 / kColThreads = N2 elements per thread, all loads issued first
+  {
+    float2 q[N2];
+    float gq[N2];
+#pragma unroll
+    for (int b = 0; b < N2; b++) {
+      const int i = tid + b * kColThreads, zz = i >> 4, xi = i & 15;
+      if (xi < nx) {
+        q[b] = rhok[zz * zs + base + xi];
+        gq[b] = tab[zz * zs + base + xi];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < N2; b++) {
+      const int i = tid + b * kColThreads, zz = i >> 4, xi = i & 15;
+      if (xi < nx) {
+        Q[zz][xi] = q[b];
+        G[zz][xi] = gq[b];
+      }
+    }
+  }
+  __syncthreads();
+  double e = 0.0;
+  if (hw < nx) {
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = Q[l + 16 * j][hw];
+    fft16<N2, false>(v, l, mask, tw);
+    const int k1 = brev4(l);
+    const int xg = x0 + hw;
+    const double wgt = (xg == 0 || 2 * xg == M) ? 1.0 : 2.0;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) {
+      const int kz = k2 + N2 * k1;
+      const float f = G[kz][hw];
+      const double re = (double)v[k2].x, im = (double)v[k2].y;
+      e += wgt * (double)f * (re * re + im * im);
+      Q[kz][hw] = make_float2(v[k2].x * f, v[k2].y * f);
+    }
+    __syncwarp(mask);
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = Q[l + 16 * j][hw];
+    __syncwarp(mask);
+    fft16<N2, true>(v, l, mask, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) Q[k2 + N2 * k1][hw] = v[k2];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < N2; b++) {
+    const int i = tid + b * kColThreads, zz = i >> 4, xi = i & 15;
+    if (xi < nx) rhok[zz * zs + base + xi] = Q[zz][xi];
+  }
+  block_sum_to(e, partials);
+  last_block_sum_counter(partials, done, factor, out);
+}
+
+template <int N2>
+__global__ void __launch_bounds__(kPlaneThreads, 2)
+    k_own_fft_xy_inv(const float2* __restrict__ rhok, float* __restrict__ phi,
+                     const float2* __restrict__ tw) {
+  constexpr int M = 16 * N2, X = M / 2 + 1;
+  extern __shared__ float2 fsm[];
+  float2* P = fsm;                                     // [M][X]
+  float* S = reinterpret_cast<float*>(fsm + M * X);    // [kHalfWarps][2M]
+  const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
+  const unsigned mask = 0xFFFFu << (tid & 16);
+  copy_in(P, rhok + (long long)blockIdx.x * M * X, M * X);
+  __syncthreads();
+  // inverse y: each x' column in place
+  for (int col = hw; col < X; col += kHalfWarps) {
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
+    fft16<N2, true>(v, l, mask, tw);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
+  }
+  __syncthreads();
+  // c2r x: the half spectra A (row 2p) and B (row 2p+1), extended by
+  // Hermitian symmetry, combined as A + iB; one inverse transform gives row
+  // 2p in the real and row 2p+1 in the imaginary part
+  float* T = S + hw * 2 * M;
+  float* out = phi + (long long)blockIdx.x * M * M;
+  for (int pr = hw; pr < M / 2; pr += kHalfWarps) {
+    const float2* Pa = P + (2 * pr) * X;
+    const float2* Pb = Pa + X;
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) {
+      const int k = l + 16 * j;
+      float2 A, B;
+      if (2 * k <= M) {
+        A = Pa[k];
+        B = Pb[k];
+        if (k == 0 || 2 * k == M) {
+          A.y = 0.f;
+          B.y = 0.f;
+        }
+      } else {
+        A = Pa[M - k];
+        B = Pb[M - k];
+        A.y = -A.y;
+        B.y = -B.y;
+      }
+      v[j] = make_float2(A.x - B.y, A.y + B.x);
+    }
+    fft16<N2, true>(v, l, mask, tw);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) {
+      T[k2 + N2 * k1] = v[k2].x;
+      T[M + k2 + N2 * k1] = v[k2].y;
+    }
+    __syncwarp(mask);
+    float* ra = out + (long long)(2 * pr) * M;
+    for (int i = l; i < M; i += 16) {
+      ra[i] = T[i];
+      ra[M + i] = T[M + i];
+    }
+    __syncwarp(mask);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+bool own_fft_supported(const int M[3]) {
+  if (M[0] != M[1] || M[0] != M[2] || M[0] % 16 != 0) return false;
+  const int n2 = M[0] / 16;
+  return n2 >= kFftMinN2 && n2 <= kFftMaxN2;
+}
+
+cudaError_t make_fft_twiddles(int M, float2** out) {
+  const int n2 = M / 16;
+  std::vector<float2> h(16 * n2 + 16 + n2);
+  auto w = [](long long m, int n) {
+    const double a = -2.0 * kPi * (double)(m % n) / (double)n;
+    return make_float2((float)std::cos(a), (float)std::sin(a));
+  };
+  for (int n1 = 0; n1 < 16; n1++)
+    for (int k2 = 0; k2 < n2; k2++) h[n1 * n2 + k2] = w((long long)n1 * k2, M);
+  for (int m = 0; m < 16; m++) h[16 * n2 + m] = w(m, 16);
+  for (int m = 0; m < n2; m++) h[16 * n2 + 16 + m] = w(m, n2);
+  cudaError_t e = cudaMalloc(out, sizeof(float2) * h.size());
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*out, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+}
+
+namespace {
+
+// Opt each plane kernel in to its shared memory once per device.
+template <typename K>
+cudaError_t allow_smem(K kernel, size_t bytes, bool (&done)[64]) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!done[dev]) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
+template <int N2>
+cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float* rho_out,
+                   float2* rhok, const float2* tw, cudaStream_t st) {
+  constexpr int M = 16 * N2;
+  constexpr size_t smem = plane_smem<N2>();
+  static bool fx[64] = {}, fl[64] = {};
+  if (g64) {
+    cudaError_t e = allow_smem(k_own_fft_xy_fwd<N2, true>, smem, fx);
+    if (e != cudaSuccess) return e;
+    k_own_fft_xy_fwd<N2, true><<<M, kPlaneThreads, smem, st>>>(g64, rho, unscale, rho_out, rhok,
+                                                               tw);
+  } else {
+    cudaError_t e = allow_smem(k_own_fft_xy_fwd<N2, false>, smem, fl);
+    if (e != cudaSuccess) return e;
+    k_own_fft_xy_fwd<N2, false><<<M, kPlaneThreads, smem, st>>>(g64, rho, unscale, rho_out,
+                                                                rhok, tw);
+  }
+  return cudaGetLastError();
+}
+
+template <int N2>
+cudaError_t z_n2(float2* rhok, const float* tab, const float2* tw, double* partials,
+                 unsigned* done, double factor, double* out, cudaStream_t st) {
+  constexpr int M = 16 * N2, X = M / 2 + 1, NXT = (X + 15) / 16;
+  k_own_fft_z_green<N2><<<NXT * M, kColThreads, 0, st>>>(rhok, tab, tw, partials, done, factor,
+                                                          out);
+  return cudaGetLastError();
+}
+
+template <int N2>
+cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, cudaStream_t st) {
+  constexpr int M = 16 * N2;
+  constexpr size_t smem = plane_smem<N2>();
+  static bool fi[64] = {};
+  cudaError_t e = allow_smem(k_own_fft_xy_inv<N2>, smem, fi);
+  if (e != cudaSuccess) return e;
+  k_own_fft_xy_inv<N2><<<M, kPlaneThreads, smem, st>>>(rhok, phi, tw);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+#define GSE_FFT_SWITCH(CALL)                                                                   \
+  switch (M / 16) {                                                                            \
+    case 4: return CALL(4);                                                                    \
+    case 5: return CALL(5);                                                                    \
+    case 6: return CALL(6);                                                                    \
+    case 7: return CALL(7);                                                                    \
+    case 8: return CALL(8);                                                                    \
+    case 9: return CALL(9);                                                                    \
+    case 10: return CALL(10);                                                                  \
+    case 11: return CALL(11);                                                                  \
+    case 12: return CALL(12);                                                                  \
+  }                                                                                            \
+  return cudaErrorInvalidValue;
+
+cudaError_t launch_own_fft_xy_forward(int M, const long long* g64, const float* rho,
+                                      double unscale, float* rho_out, float2* rhok,
+                                      const float2* tw, cudaStream_t st) {
+  if (M % 16) return cudaErrorInvalidValue;
+#define CALL_FWD(N) fwd_n2<N>(g64, rho, unscale, rho_out, rhok, tw, st)
+  GSE_FFT_SWITCH(CALL_FWD)
+#undef CALL_FWD
+}
+
+cudaError_t launch_own_fft_z_green(int M, float2* rhok, const float* tab, const float2* tw,
+                                   double* partials, unsigned* done, double factor,
+                                   double* energy_out, cudaStream_t st) {
+  if (M % 16) return cudaErrorInvalidValue;
+#define CALL_Z(N) z_n2<N>(rhok, tab, tw, partials, done, factor, energy_out, st)
+  GSE_FFT_SWITCH(CALL_Z)
+#undef CALL_Z
+}
+
+cudaError_t launch_own_fft_xy_inverse(int M, const float2* rhok, float* phi, const float2* tw,
+                                      cudaStream_t st) {
+  if (M % 16) return cudaErrorInvalidValue;
+#define CALL_INV(N) inv_n2<N>(rhok, phi, tw, st)
+  GSE_FFT_SWITCH(CALL_INV)
+#undef CALL_INV
+}
+
+#undef GSE_FFT_SWITCH
+
+}  // namespace gse

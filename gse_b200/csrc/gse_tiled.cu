@@ -908,7 +908,8 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
                      (b.M[2] + kSB - 1) / kSB};
   k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(sorted, start, b,
                                                                               s, grid64);
-  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, rho);
+  // rho == nullptr: the caller converts the int64 grid itself (the own FFT)
+  if (rho) k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, rho);
   return cudaGetLastError();
 }
 

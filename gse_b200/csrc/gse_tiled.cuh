@@ -25,6 +25,7 @@ constexpr int kGatherThreads = 256;          // >= kGY * kGZ
 constexpr int kGatherLanes = 16;             // lanes sharing one atom in the gather
 constexpr int kMinTiledGrid = 10;   // smallest grid side on the tiled path
 constexpr int kSB = 16;             // scatter-spread brick (cells per axis)
+constexpr int kFlushBits = 40;  // scale of the int64 accumulation grids
 constexpr int kScatterThreads = 512;  // >= kSB * kSB
 constexpr int kScatterList = 1024;  // atoms per scatter round (per brick)
 constexpr int kGatherList = 512;    // atoms per gather round (per brick)

@@ -59,7 +59,6 @@ struct ScatterGeom {
   static constexpr int words = T * PP;
 };
 
-constexpr int kFlushBits = 40;  // scale of the int64 accumulation grids
 constexpr int kMinShift = 11;   // 2^30 * 2^(40-11) * 8 overlapping tiles < 2^63
 
 // Block prologue of a scatter brick: the brick's atoms (one contiguous range

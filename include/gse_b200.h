@@ -268,10 +268,18 @@ gse_status_t gse_get_launch_count(gse_context_t* ctx, long long* launches);
  *                        is then 1/2 ccelec h^3 sum rho phi in real space.
  *                        Otherwise a separate multiply kernel that also sums
  *                        the energy in k-space
- *  GSE_PATH_GRAPH        repeated gse_forward calls replay a captured CUDA graph */
+ *  GSE_PATH_GRAPH        repeated gse_forward calls replay a captured CUDA graph
+ *  GSE_PATH_OWN_FFT      mixed form on a cubic grid of M = 16 N2 points per side
+ *                        (N2 = 4..12, e.g. 64, 80, 96, 128, 144, 192): the
+ *                        context's own solve is this library's 3-D FFT, with
+ *                        the int64 -> float conversion, the Green's multiply
+ *                        and the k-space energy inside its passes, instead of
+ *                        cuFFT (set GSE_B200_OWN_FFT=0 in the environment
+ *                        before creating the context to keep cuFFT) */
 #define GSE_PATH_TILED 1
 #define GSE_PATH_GREEN_IN_FFT 2
 #define GSE_PATH_GRAPH 4
+#define GSE_PATH_OWN_FFT 8
 gse_status_t gse_get_paths(gse_context_t* ctx, int* flags);
 
 /* ---- spreading without allocation ------------------------------------- */

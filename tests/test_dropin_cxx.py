@@ -17,13 +17,14 @@ def program():
     return build.build_cxx_check()
 
 
-def run(prog, precision, g, tmp_path):
+def run(prog, precision, g, tmp_path, env=None):
     M = [int(v) for v in g["M"]]
     box = [float(v) for v in g["box"]]
     path = tmp_path / "xyzq.txt"
     np.savetxt(path, g["xyzq"], fmt="%.17g")
     out = subprocess.run([prog, precision, *map(str, M), *map(repr, box), repr(float(g["sigma"])),
-                          str(path)], capture_output=True, text=True, timeout=300)
+                          str(path)], capture_output=True, text=True, timeout=300,
+                         env=dict(os.environ, **(env or {})))
     return out
 
 
@@ -80,21 +81,27 @@ def test_dropin_classes_match_reference(goldens, tmp_path, case, precision, tol)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-5)])
-def test_dropin_64cubed_green_multiply_inside_the_fft(tmp_path, precision, tol):
+@pytest.mark.parametrize("precision,tol,own", [("fp64", 1e-12, "1"), ("mixed", 1e-5, "0"),
+                                               ("mixed", 1e-5, "1")])
+def test_dropin_64cubed_green_multiply_inside_the_fft(tmp_path, precision, tol, own):
     """A process without PyTorch links the Green's multiply into the c2r
     transform (cuFFT load callback) for grids of 64^3 points and more; the
-    23,559-charge water box (M = 64) checks that path against the reference."""
+    mixed form on a cubic 16 N2 grid takes the library's own FFT instead
+    unless GSE_B200_OWN_FFT=0.  The 23,559-charge water box (M = 64) checks
+    each path against the reference."""
     from conftest import GOLDEN
     from gse_b200 import workloads as W
     z = np.load(os.path.join(GOLDEN, "water_23559.npz"))
     s = W.config_water_23k()
     g = {"M": np.array(s.grid), "box": np.array(s.boxes), "sigma": np.array(s.sigma),
          "xyzq": s.xyzq.astype(np.float64)}
-    out = run(program(), precision, g, tmp_path)
+    out = run(program(), precision, g, tmp_path, env={"GSE_B200_OWN_FFT": own})
     assert out.returncode == 0, out.stderr
     paths = int([ln for ln in out.stdout.splitlines() if ln.startswith("PATHS")][0].split()[1])
-    assert paths & 2, "Green's multiply not inside the FFT"
+    if precision == "mixed" and own == "1":
+        assert paths & 8 and not paths & 2, paths
+    else:
+        assert paths & 2, "Green's multiply not inside the FFT"
     E, F, Es, Fs = parse(out.stdout)
     print(precision, abs(E - float(z["E"])) / abs(float(z["E"])), rms(F, z["F"]))
     assert abs(E - float(z["E"])) <= tol * abs(float(z["E"]))

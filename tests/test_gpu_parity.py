@@ -223,3 +223,39 @@ def test_repeated_device_forward_replays_a_graph():
     torch.cuda.synchronize()
     assert torch.equal(f2, outs[4][1]) and E2 == outs[4][0]
     assert ctx.launch_count() > 0
+
+
+@pytest.mark.parametrize("n2", [4, 5, 6, 7, 8, 9, 10, 11, 12])
+def test_own_fft_matches_cufft_and_fp64(n2, monkeypatch):
+    """Mixed form on cubic grids of M = 16 N2 points (64 ... 192): the
+    library's own FFT solve (int64 grid read directly, Green's multiply and
+    k-space energy in the z pass) against the same mixed evaluation through
+    cuFFT (GSE_B200_OWN_FFT=0) and against the FP64 form: forces within 1e-5
+    relative RMS of both, energies within 1e-6 of each other."""
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
+    M = 16 * n2
+    L = 0.97 * M
+    x = W.triplets(1500, L, 20 + n2).astype(np.float32)
+    n = x.shape[0]
+
+    def evaluate(precision, own):
+        monkeypatch.setenv("GSE_B200_OWN_FFT", "1" if own else "0")
+        ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision=precision)
+        xx = x.astype(np.float64) if precision == "fp64" else x
+        f = [np.zeros(n) for _ in range(3)]
+        E = ctx.forward(n, xx, *f)
+        paths = ctx.paths()
+        ctx.close()
+        return E, np.stack(f, 1), paths
+
+    Eo, Fo, po = evaluate("mixed", True)
+    Ec, Fc, pc = evaluate("mixed", False)
+    Ed, Fd, _ = evaluate("fp64", True)
+    assert po & 8 and not pc & 8
+    rms = lambda F, R: float(np.sqrt(((F - R) ** 2).sum() / (R ** 2).sum()))
+    print(n2, rms(Fo, Fc), rms(Fo, Fd), rms(Fc, Fd), abs(Eo - Ec) / abs(Ec), abs(Eo - Ed) / abs(Ed))
+    assert rms(Fo, Fc) <= 1e-5
+    assert rms(Fo, Fd) <= 1e-5
+    assert abs(Eo - Ec) <= 1e-6 * abs(Ec)
+    assert abs(Eo - Ed) <= 1e-6 * abs(Ed)
