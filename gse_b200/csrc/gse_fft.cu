@@ -39,72 +39,138 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 
 __device__ __forceinline__ int brev4(int l) { return (int)(__brev((unsigned)l) >> 28); }
 
+// Twiddles a lane uses, loaded once per kernel: c[m] = w_N2^m, the lane's
+// w_N^(l k2), and its three cross-lane stage factors (spans 16, 8, 4).
+template <int N2>
+struct LaneTw {
+  float2 c[N2];
+  float2 wnk[N2];
+  float2 ws[3];
+  __device__ __forceinline__ void load(const float2* __restrict__ tw, int l) {
+    const float2* twnk = tw;            // [16][N2]
+    const float2* tw16 = tw + 16 * N2;  // [16]
+    const float2* twn2 = tw16 + 16;     // [N2]
+#pragma unroll
+    for (int m = 0; m < N2; m++) {
+      c[m] = twn2[m];
+      wnk[m] = twnk[l * N2 + m];
+    }
+    // span 2h: lanes with (l & h) take w_{2h}^(l mod h) = w_16^((l mod h) 8/h)
+    ws[0] = tw16[(l & 7) * 1];
+    ws[1] = tw16[(l & 3) * 2];
+    ws[2] = tw16[(l & 1) * 4];
+  }
+};
+
+template <bool INV>
+__device__ __forceinline__ float2 cmul_tw(float2 a, float2 w) {
+  // a * w (forward) or a * conj(w) (inverse)
+  return INV ? make_float2(fmaf(a.x, w.x, a.y * w.y), fmaf(a.y, w.x, -a.x * w.y)) : cmul(a, w);
+}
+
+constexpr int smallest_factor(int n) {
+  int p = 2;
+  while (n % p) p++;
+  return p;
+}
+
+// In-register DFT of x[0..N) in natural order (N divides N2), by recursive
+// decimation in time: N = P Q with P the smallest prime factor; Q-point DFTs
+// of the P residue classes, twiddles w_N^(p k), P-point DFTs across them.
+// All twiddles are powers of w_N2 from c[].
+template <int N2, bool INV, int N>
+__device__ __forceinline__ void dft_reg(float2 (&x)[N], const float2 (&c)[N2]) {
+  if constexpr (N == 1) {
+    return;
+  } else if constexpr (N == 2) {
+    const float2 a = x[0], b = x[1];
+    x[0] = make_float2(a.x + b.x, a.y + b.y);
+    x[1] = make_float2(a.x - b.x, a.y - b.y);
+  } else if constexpr (N == 3) {
+    // X0 = x0 + s, X1,2 = x0 - s/2 -/+ i (sqrt(3)/2) d (forward), s = x1 + x2, d = x1 - x2
+    constexpr float kS3 = 0.866025403784438646763723170752936183f;
+    const float2 s = make_float2(x[1].x + x[2].x, x[1].y + x[2].y);
+    const float2 d = make_float2(x[1].x - x[2].x, x[1].y - x[2].y);
+    const float2 t = make_float2(fmaf(-0.5f, s.x, x[0].x), fmaf(-0.5f, s.y, x[0].y));
+    const float sg = INV ? -kS3 : kS3;
+    const float2 u = make_float2(sg * d.y, -sg * d.x);  // -i sg d
+    x[0] = make_float2(x[0].x + s.x, x[0].y + s.y);
+    x[1] = make_float2(t.x + u.x, t.y + u.y);
+    x[2] = make_float2(t.x - u.x, t.y - u.y);
+  } else if constexpr (smallest_factor(N) == N) {
+    // other primes: direct sum
+    float2 y[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      float re = x[0].x, im = x[0].y;
+#pragma unroll
+      for (int p = 1; p < N; p++) {
+        const float2 w = c[(p * j * (N2 / N)) % N2];
+        const float2 t = cmul_tw<INV>(x[p], w);
+        re += t.x;
+        im += t.y;
+      }
+      y[j] = make_float2(re, im);
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++) x[j] = y[j];
+  } else {
+    constexpr int P = smallest_factor(N), Q = N / P;
+    float2 a[P][Q];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+#pragma unroll
+      for (int q = 0; q < Q; q++) a[p][q] = x[p + P * q];
+      dft_reg<N2, INV, Q>(a[p], c);
+#pragma unroll
+      for (int k = 1; k < Q; k++)
+        if (p > 0) a[p][k] = cmul_tw<INV>(a[p][k], c[(p * k * (N2 / N)) % N2]);
+    }
+#pragma unroll
+    for (int k = 0; k < Q; k++) {
+      float2 b[P];
+#pragma unroll
+      for (int p = 0; p < P; p++) b[p] = a[p][k];
+      dft_reg<N2, INV, P>(b, c);
+#pragma unroll
+      for (int j = 0; j < P; j++) x[k + Q * j] = b[j];
+    }
+  }
+}
+
 // One complex transform of length 16 N2 by a half-warp (mask: its 16 lanes,
 // l: the lane within it).  In: v[n2] = x[l + 16 n2].  Out: v[k2] = X[k2 + N2 brev4(l)].
 template <int N2, bool INV>
 __device__ __forceinline__ void fft16(float2 (&v)[N2], int l, unsigned mask,
-                                      const float2* __restrict__ tw) {
-  const float2* twnk = tw;                // [16][N2]
-  const float2* tw16 = tw + 16 * N2;      // [16]
-  const float2* twn2 = tw16 + 16;         // [N2]
-  float2 c[N2];
+                                      const LaneTw<N2>& t) {
+  // N2-point DFT of the lane's own values, then the twiddle w_N^(l k2)
+  dft_reg<N2, INV, N2>(v, t.c);
 #pragma unroll
-  for (int m = 0; m < N2; m++) {
-    c[m] = twn2[m];
-    if (INV) c[m].y = -c[m].y;
-  }
-  // N2-point DFT of the lane's own values
-  float2 a[N2];
-#pragma unroll
-  for (int k2 = 0; k2 < N2; k2++) {
-    float re = 0.f, im = 0.f;
-#pragma unroll
-    for (int n2 = 0; n2 < N2; n2++) {
-      const int m = (n2 * k2) % N2;
-      if (m == 0) {
-        re += v[n2].x;
-        im += v[n2].y;
-      } else {
-        re = fmaf(v[n2].x, c[m].x, re);
-        re = fmaf(-v[n2].y, c[m].y, re);
-        im = fmaf(v[n2].x, c[m].y, im);
-        im = fmaf(v[n2].y, c[m].x, im);
-      }
-    }
-    a[k2] = make_float2(re, im);
-  }
-  // twiddle w_N^(l k2)
-#pragma unroll
-  for (int k2 = 1; k2 < N2; k2++) {
-    float2 w = twnk[l * N2 + k2];
-    if (INV) w.y = -w.y;
-    a[k2] = cmul(a[k2], w);
-  }
+  for (int k2 = 1; k2 < N2; k2++) v[k2] = cmul_tw<INV>(v[k2], t.wnk[k2]);
   // 16-point decimation in frequency across the lanes
 #pragma unroll
-  for (int h = 8; h >= 1; h >>= 1) {
+  for (int s = 0; s < 4; s++) {
+    const int h = 8 >> s;
     const bool up = (l & h) != 0;
-    float2 w = make_float2(1.f, 0.f);
-    if (h > 1 && up) {
-      w = tw16[(l & (h - 1)) * (8 / h)];
-      if (INV) w.y = -w.y;
-    }
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) {
-      const float px = __shfl_xor_sync(mask, a[k2].x, h);
-      const float py = __shfl_xor_sync(mask, a[k2].y, h);
-      const float2 d = up ? make_float2(px - a[k2].x, py - a[k2].y)
-                          : make_float2(a[k2].x + px, a[k2].y + py);
-      a[k2] = (h > 1 && up) ? cmul(d, w) : d;
+      const float px = __shfl_xor_sync(mask, v[k2].x, h);
+      const float py = __shfl_xor_sync(mask, v[k2].y, h);
+      const float2 d = up ? make_float2(px - v[k2].x, py - v[k2].y)
+                          : make_float2(v[k2].x + px, v[k2].y + py);
+      if (s < 3) {
+        // lower lanes carry w = 1: multiply every lane, uniform code
+        const float2 w = up ? t.ws[s] : make_float2(1.f, 0.f);
+        v[k2] = cmul_tw<INV>(d, w);
+      } else {
+        v[k2] = d;
+      }
     }
   }
-#pragma unroll
-  for (int k2 = 0; k2 < N2; k2++) v[k2] = a[k2];
 }
 
-// 16 half-warps per plane CTA: with the plane and the scratch rows two CTAs
-// fit an SM up to N2 = 9 (144^3), so one can load while the other transforms
-constexpr int kPlaneThreads = 256;
+// 32 half-warps per plane CTA (one CTA per SM: M planes)
+constexpr int kPlaneThreads = 512;
 constexpr int kHalfWarps = kPlaneThreads / 16;
 constexpr int kColThreads = 256;  // 16 half-warps, one per x' column of a tile
 
@@ -137,7 +203,7 @@ __device__ __forceinline__ void copy_in(float2* __restrict__ dst, const float2* 
 }  // namespace
 
 template <int N2, bool FIXED>
-__global__ void __launch_bounds__(kPlaneThreads, 2)
+__global__ void __launch_bounds__(kPlaneThreads, 1)
     k_own_fft_xy_fwd(const long long* __restrict__ g64, const float* __restrict__ rho,
                      double unscale, float* __restrict__ rho_out, float2* __restrict__ rhok,
                      const float2* __restrict__ tw) {
@@ -147,6 +213,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   float2* S = fsm + M * X;  // [kHalfWarps][M]
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  LaneTw<N2> lt;
+  lt.load(tw, l);
   const long long plane = (long long)M * M;
   const long long z0 = (long long)blockIdx.x * plane;
   float2* Z = S + hw * M;
@@ -171,7 +239,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
       }
       v[j] = make_float2(a, b);
     }
-    fft16<N2, false>(v, l, mask, tw);
+    fft16<N2, false>(v, l, mask, lt);
     const int k1 = brev4(l);
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) Z[k2 + N2 * k1] = v[k2];
@@ -192,7 +260,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     float2 v[N2];
 #pragma unroll
     for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
-    fft16<N2, false>(v, l, mask, tw);
+    fft16<N2, false>(v, l, mask, lt);
     const int k1 = brev4(l);
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
@@ -212,6 +280,8 @@ __global__ void __launch_bounds__(kColThreads)
   __shared__ float G[M][17];
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  LaneTw<N2> lt;
+  lt.load(tw, l);
   const int xt = blockIdx.x % NXT, y = blockIdx.x / NXT;
   const int x0 = xt * 16, nx = min(16, X - x0);
   const long long zs = (long long)M * X;
@@ -243,7 +313,7 @@ __global__ void __launch_bounds__(kColThreads)
     float2 v[N2];
 #pragma unroll
     for (int j = 0; j < N2; j++) v[j] = Q[l + 16 * j][hw];
-    fft16<N2, false>(v, l, mask, tw);
+    fft16<N2, false>(v, l, mask, lt);
     const int k1 = brev4(l);
     const int xg = x0 + hw;
     const double wgt = (xg == 0 || 2 * xg == M) ? 1.0 : 2.0;
@@ -259,7 +329,7 @@ __global__ void __launch_bounds__(kColThreads)
 #pragma unroll
     for (int j = 0; j < N2; j++) v[j] = Q[l + 16 * j][hw];
     __syncwarp(mask);
-    fft16<N2, true>(v, l, mask, tw);
+    fft16<N2, true>(v, l, mask, lt);
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) Q[k2 + N2 * k1][hw] = v[k2];
   }
@@ -274,7 +344,7 @@ __global__ void __launch_bounds__(kColThreads)
 }
 
 template <int N2>
-__global__ void __launch_bounds__(kPlaneThreads, 2)
+__global__ void __launch_bounds__(kPlaneThreads, 1)
     k_own_fft_xy_inv(const float2* __restrict__ rhok, float* __restrict__ phi,
                      const float2* __restrict__ tw) {
   constexpr int M = 16 * N2, X = M / 2 + 1;
@@ -283,6 +353,8 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
   float* S = reinterpret_cast<float*>(fsm + M * X);    // [kHalfWarps][2M]
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  LaneTw<N2> lt;
+  lt.load(tw, l);
   copy_in(P, rhok + (long long)blockIdx.x * M * X, M * X);
   __syncthreads();
   // inverse y: each x' column in place
@@ -290,7 +362,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
     float2 v[N2];
 #pragma unroll
     for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
-    fft16<N2, true>(v, l, mask, tw);
+    fft16<N2, true>(v, l, mask, lt);
     const int k1 = brev4(l);
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
@@ -324,7 +396,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 2)
       }
       v[j] = make_float2(A.x - B.y, A.y + B.x);
     }
-    fft16<N2, true>(v, l, mask, tw);
+    fft16<N2, true>(v, l, mask, lt);
     const int k1 = brev4(l);
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) {
