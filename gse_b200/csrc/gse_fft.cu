@@ -147,24 +147,22 @@ __device__ __forceinline__ void fft16(float2 (&v)[N2], int l, unsigned mask,
   dft_reg<N2, INV, N2>(v, t.c);
 #pragma unroll
   for (int k2 = 1; k2 < N2; k2++) v[k2] = cmul_tw<INV>(v[k2], t.wnk[k2]);
-  // 16-point decimation in frequency across the lanes
+  // 16-point decimation in frequency across the lanes: the lower lane of a
+  // pair keeps v + p, the upper one (p - v) w; as sg v + p with sg = -1 on
+  // upper lanes and w = 1 on lower lanes the code is the same for every lane
 #pragma unroll
   for (int s = 0; s < 4; s++) {
     const int h = 8 >> s;
     const bool up = (l & h) != 0;
+    const float sg = up ? -1.f : 1.f;
+    float2 w = up ? t.ws[s < 3 ? s : 0] : make_float2(1.f, 0.f);
+    if (INV) w.y = -w.y;
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) {
       const float px = __shfl_xor_sync(mask, v[k2].x, h);
       const float py = __shfl_xor_sync(mask, v[k2].y, h);
-      const float2 d = up ? make_float2(px - v[k2].x, py - v[k2].y)
-                          : make_float2(v[k2].x + px, v[k2].y + py);
-      if (s < 3) {
-        // lower lanes carry w = 1: multiply every lane, uniform code
-        const float2 w = up ? t.ws[s] : make_float2(1.f, 0.f);
-        v[k2] = cmul_tw<INV>(d, w);
-      } else {
-        v[k2] = d;
-      }
+      const float2 d = make_float2(fmaf(sg, v[k2].x, px), fmaf(sg, v[k2].y, py));
+      v[k2] = s < 3 ? cmul(d, w) : d;
     }
   }
 }
