@@ -31,6 +31,11 @@
 
 namespace gse {
 
+// w_N2^m of every supported N2, N2 = kFftMinN2 .. kFftMaxN2 one after the
+// other: uniform across the lanes, so read from the constant cache
+constexpr int twc_offset(int n2) { return (n2 - kFftMinN2) * (n2 + kFftMinN2 - 1) / 2; }
+__constant__ float2 c_twn2[twc_offset(kFftMaxN2 + 1)];
+
 namespace {
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -39,22 +44,20 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 
 __device__ __forceinline__ int brev4(int l) { return (int)(__brev((unsigned)l) >> 28); }
 
-// Twiddles a lane uses, loaded once per kernel: c[m] = w_N2^m, the lane's
-// w_N^(l k2), and its three cross-lane stage factors (spans 16, 8, 4).
+// Twiddles a lane uses, loaded once per kernel: the lane's w_N^(l k2) and
+// its three cross-lane stage factors (spans 16, 8, 4).  c points at w_N2^m in
+// constant memory.
 template <int N2>
 struct LaneTw {
-  float2 c[N2];
+  const float2* c;
   float2 wnk[N2];
   float2 ws[3];
   __device__ __forceinline__ void load(const float2* __restrict__ tw, int l) {
     const float2* twnk = tw;            // [16][N2]
     const float2* tw16 = tw + 16 * N2;  // [16]
-    const float2* twn2 = tw16 + 16;     // [N2]
+    c = c_twn2 + twc_offset(N2);
 #pragma unroll
-    for (int m = 0; m < N2; m++) {
-      c[m] = twn2[m];
-      wnk[m] = twnk[l * N2 + m];
-    }
+    for (int m = 0; m < N2; m++) wnk[m] = twnk[l * N2 + m];
     // span 2h: lanes with (l & h) take w_{2h}^(l mod h) = w_16^((l mod h) 8/h)
     ws[0] = tw16[(l & 7) * 1];
     ws[1] = tw16[(l & 3) * 2];
@@ -79,7 +82,7 @@ constexpr int smallest_factor(int n) {
 // of the P residue classes, twiddles w_N^(p k), P-point DFTs across them.
 // All twiddles are powers of w_N2 from c[].
 template <int N2, bool INV, int N>
-__device__ __forceinline__ void dft_reg(float2 (&x)[N], const float2 (&c)[N2]) {
+__device__ __forceinline__ void dft_reg(float2 (&x)[N], const float2* c) {
   if constexpr (N == 1) {
     return;
   } else if constexpr (N == 2) {
@@ -170,7 +173,11 @@ __device__ __forceinline__ void fft16(float2 (&v)[N2], int l, unsigned mask,
 // 32 half-warps per plane CTA (one CTA per SM: M planes)
 constexpr int kPlaneThreads = 512;
 constexpr int kHalfWarps = kPlaneThreads / 16;
-constexpr int kColThreads = 256;  // 16 half-warps, one per x' column of a tile
+constexpr int kColThreads = 256;
+// resident z-pass CTAs per SM that each size fits without spilling
+constexpr int z_blocks(int n2) {
+  return (n2 == 4 || n2 == 5 || n2 == 8 || n2 == 9) ? 4 : (n2 == 11 || n2 == 12) ? 2 : 3;
+}  // 16 half-warps, one per x' column of a tile
 
 template <int N2>
 constexpr size_t plane_smem() {
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
 }
 
 template <int N2>
-__global__ void __launch_bounds__(kColThreads)
+__global__ void __launch_bounds__(kColThreads, z_blocks(N2))
     k_own_fft_z_green(float2* __restrict__ rhok, const float* __restrict__ tab,
                       const float2* __restrict__ tw, double* __restrict__ partials,
                       unsigned* __restrict__ done, double factor, double* __restrict__ out) {
@@ -422,6 +429,7 @@ bool own_fft_supported(const int M[3]) {
 
 cudaError_t make_fft_twiddles(int M, float2** out) {
   const int n2 = M / 16;
+  if (n2 < kFftMinN2 || n2 > kFftMaxN2 || M % 16) return cudaErrorInvalidValue;
   std::vector<float2> h(16 * n2 + 16 + n2);
   auto w = [](long long m, int n) {
     const double a = -2.0 * kPi * (double)(m % n) / (double)n;
@@ -431,7 +439,11 @@ cudaError_t make_fft_twiddles(int M, float2** out) {
     for (int k2 = 0; k2 < n2; k2++) h[n1 * n2 + k2] = w((long long)n1 * k2, M);
   for (int m = 0; m < 16; m++) h[16 * n2 + m] = w(m, 16);
   for (int m = 0; m < n2; m++) h[16 * n2 + 16 + m] = w(m, n2);
-  cudaError_t e = cudaMalloc(out, sizeof(float2) * h.size());
+  // this size's w_N2^m into the constant table (of the current device)
+  cudaError_t e = cudaMemcpyToSymbol(c_twn2, h.data() + 16 * n2 + 16, sizeof(float2) * n2,
+                                     sizeof(float2) * twc_offset(n2));
+  if (e != cudaSuccess) return e;
+  e = cudaMalloc(out, sizeof(float2) * h.size());
   if (e != cudaSuccess) return e;
   return cudaMemcpy(*out, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
 }
