@@ -493,6 +493,13 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
       float wy[W];
 #pragma unroll
       for (int k = 0; k < W; k++) wy[k] = __shfl_sync(0xffffffffu, wl[1], k);
+      // y weights in pairs for the packed fma (two points per instruction)
+      unsigned long long wy2[W / 2];
+#pragma unroll
+      for (int k = 0; k + 1 < W; k += 2)
+        asm("mov.b64 %0, {%1, %2};" : "=l"(wy2[k / 2]) : "f"(wy[k]), "f"(wy[k + 1]));
+      unsigned long long magic2;
+      asm("mov.b64 %0, {%1, %1};" : "=l"(magic2) : "f"(12582912.0f));
       const float qp = a.w * s.pref * tscale;
       int* base = tile + loc[2] * G::PP + loc[1] * G::RP + loc[0];
 #pragma unroll
@@ -502,11 +509,22 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
         if (pass * 32 + lane < W * W) {
           const float t = qp * wx * wz;
           int* cell = base + poff[pass];
+          unsigned long long t2;
+          asm("mov.b64 %0, {%1, %1};" : "=l"(t2) : "f"(t));
 #pragma unroll
-          for (int k = 0; k < W; k++) {
-            // round(t wy): |t wy| < 2^22, so 1.5*2^23 + t wy has unit spacing
-            const int v = __float_as_int(fmaf(t, wy[k], 12582912.0f)) - 0x4B400000;
-            atomicAdd(cell + k * G::RP, v);
+          for (int k = 0; k + 1 < W; k += 2) {
+            // round(t wy) for two points: |t wy| < 2^22, so 1.5*2^23 + t wy has
+            // unit spacing (each half rounded once, as fmaf does)
+            unsigned long long r2;
+            asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r2) : "l"(t2), "l"(wy2[k / 2]), "l"(magic2));
+            unsigned lo, hi;
+            asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(r2));
+            atomicAdd(cell + k * G::RP, (int)lo - 0x4B400000);
+            atomicAdd(cell + (k + 1) * G::RP, (int)hi - 0x4B400000);
+          }
+          {
+            const int v = __float_as_int(fmaf(t, wy[W - 1], 12582912.0f)) - 0x4B400000;
+            atomicAdd(cell + (W - 1) * G::RP, v);
           }
         }
       }
