@@ -277,6 +277,14 @@ __device__ __forceinline__ void adj_scatter_brick(
         eyuy[k] = ey[k] * __shfl_sync(0xffffffffu, ul[1], k);
         uy2[k] = __shfl_sync(0xffffffffu, u2l[1], k);
       }
+      // the same weights in pairs of y points for the packed fma
+      unsigned long long ey2[W / 2], eyuy2[W / 2], magic2;
+#pragma unroll
+      for (int k = 0; k + 1 < W; k += 2) {
+        asm("mov.b64 %0, {%1, %2};" : "=l"(ey2[k / 2]) : "f"(ey[k]), "f"(ey[k + 1]));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(eyuy2[k / 2]) : "f"(eyuy[k]), "f"(eyuy[k + 1]));
+      }
+      asm("mov.b64 %0, {%1, %1};" : "=l"(magic2) : "f"(12582912.0f));
       // compact the (x, z) pairs with u_x^2 + u_z^2 < rcut^2: every point of
       // the other columns lies outside the sphere
       int npair = 0;
@@ -308,14 +316,25 @@ __device__ __forceinline__ void adj_scatter_brick(
           const float t1 = w * (Gx * ux + Gz * uz), t2 = w * Gy;
           const float rem = s.rcut2 - (ux2 + uz2);
           int* cell = base + pz * G::PP + px;
+          unsigned long long t1p, t2p;
+          asm("mov.b64 %0, {%1, %1};" : "=l"(t1p) : "f"(t1));
+          asm("mov.b64 %0, {%1, %1};" : "=l"(t2p) : "f"(t2));
 #pragma unroll
-          for (int k = 0; k < W; k++) {
-            if (uy2[k] < rem) {
-              // |t1 e_y + t2 e_y u_y| < 2^22: both roundings stay at unit spacing
-              const int v =
-                  __float_as_int(fmaf(t1, ey[k], fmaf(t2, eyuy[k], 12582912.0f))) - 0x4B400000;
-              atomicAdd(cell + k * G::RP, v);
-            }
+          for (int k = 0; k + 1 < W; k += 2) {
+            // |t1 e_y + t2 e_y u_y| < 2^22: both roundings stay at unit spacing;
+            // two y points per packed fma, each half rounded as fmaf rounds
+            unsigned long long r2;
+            asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r2) : "l"(t2p), "l"(eyuy2[k / 2]), "l"(magic2));
+            asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(r2) : "l"(t1p), "l"(ey2[k / 2]));
+            unsigned lo, hi;
+            asm("mov.b64 {%0, %1}, %2;" : "=r"(lo), "=r"(hi) : "l"(r2));
+            if (uy2[k] < rem) atomicAdd(cell + k * G::RP, (int)lo - 0x4B400000);
+            if (uy2[k + 1] < rem) atomicAdd(cell + (k + 1) * G::RP, (int)hi - 0x4B400000);
+          }
+          if (uy2[W - 1] < rem) {
+            const int v = __float_as_int(fmaf(t1, ey[W - 1], fmaf(t2, eyuy[W - 1], 12582912.0f))) -
+                          0x4B400000;
+            atomicAdd(cell + (W - 1) * G::RP, v);
           }
         }
       }
