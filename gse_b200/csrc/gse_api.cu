@@ -78,6 +78,18 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Page-locked host memory (cudaHostAlloc / cudaHostRegister): copies to and
+// from it can be recorded in a CUDA graph.
+bool is_pinned_host(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 namespace gse {
@@ -994,18 +1006,25 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
 gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
                          double* fy, double* fz) {
   TRY(check_ctx(c));
-  // Graph replay applies to calls whose inputs and outputs are all device
-  // memory, on a stream that can be captured, without stage timing; the key
-  // (pointers, count, box, stream) must repeat exactly.
-  const bool outs_dev = (!energy || is_device_ptr(energy)) &&
-                        ((!fx && !fy && !fz) || (fx && fy && fz && is_device_ptr(fx) &&
-                                                 is_device_ptr(fy) && is_device_ptr(fz)));
+  // Graph replay applies to calls whose positions and forces are device or
+  // page-locked host memory (the copies to and from the host then sit in the
+  // graph), on a stream that can be captured, without stage timing; the key
+  // (pointers, count, box, stream) must repeat exactly.  A host energy is read
+  // through the context's page-locked scalar after the call has finished.
+  auto io_ok = [](const void* p) { return is_device_ptr(p) || is_pinned_host(p); };
+  const bool host_e = energy && !is_device_ptr(energy);
+  const bool forces_ok = (!fx && !fy && !fz) || (fx && fy && fz && io_ok(fx) && io_ok(fy) &&
+                                                 io_ok(fz));
+  const bool host_io = host_e || (fx && !is_device_ptr(fx)) || (fy && !is_device_ptr(fy)) ||
+                       (fz && !is_device_ptr(fz));
   const bool graphable = c->fwd_graphs && !c->timing && c->stream != nullptr && n > 0 &&
-                         is_device_ptr(xyzq) && outs_dev && c->gtab_valid;
+                         io_ok(xyzq) && forces_ok && c->gtab_valid;
   gse_context_t::FwdKey key;
   key.n = n;
   key.x = xyzq;
-  key.e = energy;
+  // a host energy is not part of the graph (it is read from the scalar after
+  // the call), so its address need not repeat
+  key.e = host_e ? reinterpret_cast<double*>(uintptr_t(1)) : energy;
   key.fx = fx;
   key.fy = fy;
   key.fz = fz;
@@ -1019,27 +1038,42 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
     TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
     return finish(c, host);
   }
+  // the evaluation with the energy copied to the page-locked scalar, no wait
+  auto body = [&](bool* h) -> gse_status_t {
+    TRY(forward_body(c, n, xyzq, host_e ? nullptr : energy, fx, fy, fz, h));
+    if (host_e) {
+      CU(cudaMemcpyAsync(c->h_pinned, c->d_scalars, sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+      *h = true;
+    }
+    return GSE_OK;
+  };
+  auto done = [&](bool h) -> gse_status_t {
+    TRY(finish(c, h));
+    if (host_e) *energy = c->h_pinned[0];
+    return GSE_OK;
+  };
   if (c->fwd_exec && key == c->fwd_key) {
     CU(cudaGraphLaunch(c->fwd_exec, c->stream));
     c->launches += c->fwd_launches;
     c->rho_valid = c->phi_valid = c->energy_valid = true;
-    return finish(c, false);
+    return done(host_io);
   }
   if (!(key == c->fwd_key)) {
     // first call with this key: run it directly and remember the key
     drop_fwd_graph(c);
-    TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
+    TRY(body(&host));
     c->fwd_key = key;
-    return finish(c, host);
+    return done(host);
   }
   // second identical call: capture, instantiate, launch
   const long long l0 = c->launches;
   CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  const gse_status_t st = forward_body(c, n, xyzq, energy, fx, fy, fz, &host);
+  const gse_status_t st = body(&host);
   cudaGraph_t g = nullptr;
   const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
   gse_status_t result = st;
-  if (st == GSE_OK && ec == cudaSuccess && !host) {
+  if (st == GSE_OK && ec == cudaSuccess) {
     const cudaError_t ei = cudaGraphInstantiate(&c->fwd_exec, g, 0);
     if (ei == cudaSuccess) {
       c->fwd_launches = c->launches - l0;
@@ -1057,9 +1091,9 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
     drop_fwd_graph(c);
     c->launches = l0;
     host = false;
-    TRY(forward_body(c, n, xyzq, energy, fx, fy, fz, &host));
+    TRY(body(&host));
   }
-  return finish(c, host);
+  return done(host);
 }
 
 gse_status_t gse_get_grid(gse_context_t* c, int which, void* out) {

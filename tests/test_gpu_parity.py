@@ -225,6 +225,37 @@ def test_repeated_device_forward_replays_a_graph():
     assert ctx.launch_count() > 0
 
 
+def test_repeated_pinned_host_forward_replays_a_graph():
+    """With page-locked host positions and forces (and a stream of its own)
+    the copies go into the captured graph as well: the third identical call
+    replays it, replays pick
+    up new positions written into the same host buffer, and the forces equal
+    those of an eager call from pageable memory."""
+    import torch
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
+    s = W.config_water_23k()
+    M, L = s.M, s.box
+    st = torch.cuda.Stream()  # the legacy default stream cannot be captured
+    ctx = Context(M, M, M, s.sigma, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    ctx.set_stream(st.cuda_stream)
+    hx = torch.from_numpy(s.xyzq.astype(np.float32)).pin_memory()
+    hf = torch.zeros(3, s.n, dtype=torch.float64).pin_memory()
+    xn, fn = hx.numpy(), hf.numpy()
+    outs = []
+    for k in range(5):
+        if k == 3:
+            xn[:, :3] += 0.25
+        ctx.forward(s.n, xn, fn[0], fn[1], fn[2])
+        outs.append(fn.copy())
+    assert ctx.paths() & 4  # GSE_PATH_GRAPH
+    assert np.array_equal(outs[0], outs[2]) and np.array_equal(outs[3], outs[4])
+    fresh = Context(M, M, M, s.sigma, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    f2 = [np.zeros(s.n) for _ in range(3)]
+    fresh.forward(s.n, np.array(xn), *f2)  # pageable copies: the eager path
+    assert np.array_equal(np.stack(f2), outs[4])
+
+
 @pytest.mark.parametrize("n2", [4, 5, 6, 7, 8, 9, 10, 11, 12])
 def test_own_fft_matches_cufft_and_fp64(n2, monkeypatch):
     """Mixed form on cubic grids of M = 16 N2 points (64 ... 192): the
