@@ -384,17 +384,19 @@ def main():
         barrier()
         ctx.set_timing(False)
         stage = ctx.get_timing(reset=True)
-        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-        return ms, stage, launches, clock_info
+        per = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+        pct = {"p10": float(np.percentile(per, 10)), "median": float(np.median(per)),
+               "p90": float(np.percentile(per, 90))}
+        return sum(per), stage, launches, clock_info, pct
 
     # ---- main arm: requested precision, device-resident inputs ----------
     prec = args.precision
     ctx = make_ctx(prec)
     x, f, e = device_inputs(prec)
-    ms_local, _, launches, clock_info = timed_loop(ctx, x, f, e, args.steps, False,
+    ms_local, _, launches, clock_info, pct = timed_loop(ctx, x, f, e, args.steps, False,
                                                    ClockSampler(local))
     # per-stage device times from a separate, shorter run with stage events
-    _, stage, _, _ = timed_loop(ctx, x, f, e, max(3, min(args.steps, 20)), True)
+    _, stage, _, _, _ = timed_loop(ctx, x, f, e, max(3, min(args.steps, 20)), True)
     t = torch.tensor([ms_local], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -434,7 +436,7 @@ def main():
     other = "fp64" if prec == "mixed" else "mixed"
     ctx2 = make_ctx(other)
     x2, f2, e2 = device_inputs(other)
-    ms2, _, _, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 50)), False)
+    ms2, _, _, _, _ = timed_loop(ctx2, x2, f2, e2, max(3, min(args.steps, 50)), False)
     value2 = world * max(3, min(args.steps, 50)) / (ms2 / 1000.0)
     F64 = (f2 if other == "fp64" else F_main).double().cpu().numpy().T
     Fmx = (F_main if other == "fp64" else f2).double().cpu().numpy().T
@@ -524,6 +526,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "stage_ms": per_stage,
+            "eval_ms_percentiles": {k: round(v, 4) for k, v in pct.items()},
             f"{other}_value": value2,
             "mixed_vs_fp64": {"force_rms": force_rms, "energy_rel": energy_rel},
             "vs_ewald": accuracy,
