@@ -135,7 +135,8 @@ struct gse_context {
   size_t adj_cap = 0;
   double* d_force = nullptr;  // 3 x atom_cap
   double* d_partials = nullptr;
-  double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch, [4..6] dipole
+  double* d_scalars = nullptr;  // [0] energy of the last solve, [1] scratch, [4..6] dipole,
+                                // [8..13] virial
   // grid scratch of the stand-alone grid operations, allocated on first use
   void* d_scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -815,10 +816,10 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
   CUC(cudaMalloc(&c->d_partials, sizeof(double) * (kEnergyPartials + 1)));
   CUC(cudaMemset(c->d_partials, 0, sizeof(double) * (kEnergyPartials + 1)));
-  CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 8));
+  CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 16));
   CUC(cudaMalloc(&c->d_bad, sizeof(int)));
   CUC(cudaMemset(c->d_bad, 0, sizeof(int)));
-  CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 8));
+  CUC(cudaMemset(c->d_scalars, 0, sizeof(double) * 16));
   CUC(cudaMallocHost(&c->h_pinned, sizeof(double) * 4));
   {
     int* hb = nullptr;
@@ -1337,6 +1338,41 @@ gse_status_t gse_gauss_dipole_sum(gse_context_t* c, double bx, double by, double
   }
   bool host = false;
   TRY(copy_out(c, dip, out, 3 * sizeof(double), &host));
+  return finish(c, host);
+}
+
+gse_status_t gse_virial(gse_context_t* c, double* virial) {
+  TRY(check_ctx(c));
+  if (!virial) return fail(GSE_ERR_INVALID_ARG, "NULL virial");
+  if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "virial needs rhoS (spread or forward first)");
+  if (c->fixed_pending) {
+    CU(launch_grid64_to_real(c->d_fixed, c->size, (float*)c->d_rho, c->stream));
+    c->fixed_pending = false;
+  }
+  const GreenGeom g = green_geom(c, c->sigma2, c->p.box_x, c->p.box_y, c->p.box_z, false);
+  if (!c->d_gtab) CU(cudaMalloc(&c->d_gtab, c->ksize * c->ct));
+  if (!c->gtab_valid) {
+    if (c->fp64)
+      CU(launch_green_table<double>(g, (double*)c->d_gtab, c->stream));
+    else
+      CU(launch_green_table<float>(g, (float*)c->d_gtab, c->stream));
+    c->gtab_valid = true;
+  }
+  TRY(fft_forward(c, c->d_rho, c->d_rhok));
+  const int nb = 148 * 2;
+  static_assert(6 * 148 * 2 <= kEnergyPartials, "virial partials fit the energy partials");
+  unsigned* done = reinterpret_cast<unsigned*>(c->d_partials + kEnergyPartials);
+  const double hs2 = 0.5 * c->p.sigma * c->p.sigma;
+  double* out = c->d_scalars + 8;
+  c->launches += 1;
+  if (c->fp64)
+    CU(launch_virial<double>((const double2*)c->d_rhok, (const double*)c->d_gtab, g, hs2,
+                             energy_factor(c), c->d_partials, done, nb, out, c->stream));
+  else
+    CU(launch_virial<float>((const float2*)c->d_rhok, (const float*)c->d_gtab, g, hs2,
+                            energy_factor(c), c->d_partials, done, nb, out, c->stream));
+  bool host = false;
+  TRY(copy_out(c, virial, out, 6 * sizeof(double), &host));
   return finish(c, host);
 }
 

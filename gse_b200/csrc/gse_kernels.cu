@@ -287,6 +287,96 @@ __global__ void __launch_bounds__(256)
   last_block_sum(partials, factor, energy_out);
 }
 
+// Reciprocal-space virial from the half spectrum rho^ and the Green's table:
+// with E_k = factor w_k G(k) |rho^(k)|^2 (w_k = 1 on the x' = 0 and Nyquist
+// planes, 2 elsewhere; sum_k E_k is the mesh energy),
+//   W_ab = sum_k E_k (delta_ab - 2 k_a k_b (1/k^2 + sigma^2/2)),
+// sigma the total Gaussian width (the spread's sigma1 enters |rho^|^2 twice,
+// the Green's function sigma2 once: sigma^2 = 2 sigma1^2 + sigma2^2).
+// Components xx, yy, zz, xy, xz, yz into out[0..5]; block sums to
+// partials[c * gridDim.x + block], the last block adds them in index order.
+template <typename CT>
+__global__ void __launch_bounds__(256)
+    k_virial(const typename Cplx<CT>::type* __restrict__ rhok, const CT* __restrict__ tab,
+             GreenGeom g, double half_sigma2, double factor, double* __restrict__ partials,
+             unsigned* __restrict__ done, double* __restrict__ out) {
+  const unsigned total = (unsigned)g.sizeX * g.nfft[1] * g.nfft[2];
+  const unsigned nyq = g.nx_even ? (unsigned)(g.nfft[0] / 2) : 0xffffffffu;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (unsigned idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += gridDim.x * blockDim.x) {
+    const unsigned ix = idx % (unsigned)g.sizeX, t = idx / (unsigned)g.sizeX;
+    const int iy = (int)(t % (unsigned)g.nfft[1]), iz = (int)(t / (unsigned)g.nfft[1]);
+    const double kx = g.twopi_box[0] * (double)ix;
+    const double ky = g.twopi_box[1] * (double)(iy >= g.half[1] ? iy - g.nfft[1] : iy);
+    const double kz = g.twopi_box[2] * (double)(iz >= g.half[2] ? iz - g.nfft[2] : iz);
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    if (k2 == 0.0) continue;
+    const auto r = rhok[idx];
+    const double re = (double)r.x, im = (double)r.y;
+    const double e = ((ix == 0 || ix == nyq) ? 1.0 : 2.0) * (double)tab[idx] * (re * re + im * im);
+    const double c = 2.0 * (1.0 / k2 + half_sigma2);
+    v[0] += e * (1.0 - c * kx * kx);
+    v[1] += e * (1.0 - c * ky * ky);
+    v[2] += e * (1.0 - c * kz * kz);
+    v[3] -= e * c * kx * ky;
+    v[4] -= e * c * kx * kz;
+    v[5] -= e * c * ky * kz;
+  }
+  __shared__ double red[6][32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    const double s = warp_sum(v[d]);
+    if (lane == 0) red[d][wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+      const double s = warp_sum(lane < nw ? red[d][lane] : 0.0);
+      if (lane == 0) partials[d * gridDim.x + blockIdx.x] = s;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    double t = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
+      t += ((volatile double*)partials)[d * gridDim.x + i];
+    t = warp_sum(t);
+    if (lane == 0) red[d][wid] = t;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int d = 0; d < 6; d++) {
+      const double t = warp_sum(lane < nw ? red[d][lane] : 0.0);
+      if (lane == 0) out[d] = t * factor;
+    }
+    if (lane == 0) *done = 0u;
+  }
+}
+
+template <typename CT>
+cudaError_t launch_virial(const typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
+                          double half_sigma2, double factor, double* partials, unsigned* done,
+                          int nblocks, double* out, cudaStream_t st) {
+  k_virial<CT><<<nblocks, 256, 0, st>>>(rhok, tab, g, half_sigma2, factor, partials, done, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_virial<double>(const double2*, const double*, const GreenGeom&, double,
+                                           double, double*, unsigned*, int, double*, cudaStream_t);
+template cudaError_t launch_virial<float>(const float2*, const float*, const GreenGeom&, double,
+                                          double, double*, unsigned*, int, double*, cudaStream_t);
+
 // factor * sum_i (double)(a[i]*b[i]) (the product in CT, as CpuGSE.cpp:97),
 // finished by the last block.  done is the zeroed counter the last block
 // resets (the slot after the partials that the other energy kernels use).

@@ -48,6 +48,14 @@ cudaError_t launch_green_apply(typename Cplx<CT>::type* rhok, const CT* tab, con
                                double* partials, int np, double factor, double* energy_out,
                                cudaStream_t st);
 
+// Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the half spectrum
+// rhok with the Green's table tab; partials holds 6 * nblocks doubles, done is
+// their zeroed counter (reset by the last block).
+template <typename CT>
+cudaError_t launch_virial(const typename Cplx<CT>::type* rhok, const CT* tab, const GreenGeom& g,
+                          double half_sigma2, double factor, double* partials, unsigned* done,
+                          int nblocks, double* out, cudaStream_t st);
+
 template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st);

@@ -370,6 +370,9 @@ class CpuGSE {
     check(gse_get_grid(ctx_.get(), GSE_GRID_PHI, phiM.getDataPointer()));
     return phiM;
   }
+  // Reciprocal-space virial of the current rhoS (xx, yy, zz, xy, xz, yz); the
+  // reference classes compute none (gse_virial).
+  void calculateVirial(double virial[6]) { check(gse_virial(ctx_.get(), virial)); }
   double getSigma1() { return sigma1; }
   double getSigma2() { return sigma2; }
   double getLambdaSigma1() { return lambdaSigma1; }

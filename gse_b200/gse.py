@@ -137,6 +137,15 @@ class Context:
     def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
         check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
 
+    def virial(self, out=None):
+        """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS."""
+        if out is None:
+            v = np.zeros(6)
+            check(self._L.gse_virial(self.h, ptr(v)))
+            return v
+        check(self._L.gse_virial(self.h, ptr(out)))
+        return out
+
     def gauss_spread_on_grid(self, sigma, rcut, boxx, boxy, boxz, rho, rho_s):
         check(self._L.gse_gauss_spread_on_grid(self.h, sigma, rcut, boxx, boxy, boxz, ptr(rho),
                                                ptr(rho_s)))
@@ -400,6 +409,11 @@ class CpuGSE:
     def getPhi(self) -> CpuGrid:
         self._ctx.get_grid(_lib.GRID_PHI, self.phiM.data)
         return self.phiM
+
+    def calculateVirial(self):
+        """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS; the
+        reference classes compute none."""
+        return self._ctx.virial()
 
     def getSigma1(self):
         return self.sigma1

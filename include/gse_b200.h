@@ -206,6 +206,19 @@ gse_status_t gse_gauss_efield_on_grid(gse_context_t* ctx, double box_x, double b
 gse_status_t gse_gauss_dipole_sum(gse_context_t* ctx, double box_x, double box_y, double box_z,
                                   const void* rho, double* dip);
 
+/* ---- virial (no reference counterpart) ----------------------------------- */
+
+/* Reciprocal-space virial of the context's current rhoS (after gse_forward or
+ * gse_spread_charge), in the energy's units: with E_k the mesh energy's
+ * k-space terms (their sum is the energy of gse_calculate_energy),
+ *   W_ab = sum_k E_k (delta_ab - 2 k_a k_b (1/k^2 + sigma^2/2)),
+ * sigma the total Gaussian width (sigma^2 = 2 sigma1^2 + sigma2^2), the strain
+ * derivative W_ab = -dE/d(eps_ab) of the Gaussian-split reciprocal energy.
+ * virial receives xx, yy, zz, xy, xz, yz (6 doubles, host or device).  The
+ * terms and their FP64 sum are formed on the GPU (r2c of rhoS, then one
+ * reduction, deterministic); the context's k-space buffer is overwritten. */
+gse_status_t gse_virial(gse_context_t* ctx, double* virial);
+
 /* ---- reverse mode (no reference counterpart) ---------------------------- */
 
 /* Vector-Jacobian product of one force evaluation (gse_forward) for the
