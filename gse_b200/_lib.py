@@ -92,6 +92,7 @@ SIGNATURES = {
     "gse_gauss_efield_on_grid": (_i, [_vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "gse_gauss_dipole_sum": (_i, [_vp, _d, _d, _d, _vp, _vp]),
     "gse_virial": (_i, [_vp, _vp]),
+    "gse_interpolate_field": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "gse_set_timing": (_i, [_vp, _i]),
     "gse_get_timing": (_i, [_vp, _vp, _vp, _i]),
     "gse_get_launch_count": (_i, [_vp, _vp]),

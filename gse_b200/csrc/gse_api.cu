@@ -975,6 +975,29 @@ gse_status_t gse_interpolate_force(gse_context_t* c, int n, const void* xyzq, do
   return finish(c, host);
 }
 
+gse_status_t gse_interpolate_field(gse_context_t* c, int n, const void* xyzq, double* ex,
+                                   double* ey, double* ez) {
+  TRY(check_ctx(c));
+  if (n > 0 && (!ex || !ey || !ez)) return fail(GSE_ERR_INVALID_ARG, "NULL field array");
+  if (!c->phi_valid) return fail(GSE_ERR_NOT_READY, "field before solvePoisson");
+  const void* dx;
+  TRY(stage_atoms(c, n, xyzq, &dx));
+  // unit charges in the context's own atom buffer (a host input is already there)
+  c->launches += n > 0 ? 1 : 0;
+  if (c->fp64)
+    CU(launch_unit_charges<double>((const double4*)dx, (double4*)c->d_xyzq, n, c->stream));
+  else
+    CU(launch_unit_charges<float>((const float4*)dx, (float4*)c->d_xyzq, n, c->stream));
+  bool host = false;
+  if (c->fp64)
+    TRY(gather_to<double>(c, n, c->d_xyzq, ctx_box(c).v, c->sigma1, c->rcut1,
+                          (const double*)c->d_phi, c->p.ccelec, ex, ey, ez, &host));
+  else
+    TRY(gather_to<float>(c, n, c->d_xyzq, ctx_box(c).v, c->sigma1, c->rcut1,
+                         (const float*)c->d_phi, c->p.ccelec, ex, ey, ez, &host));
+  return finish(c, host);
+}
+
 // The four forward calls in one pass (sorting once for spread and gather).
 gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
                           double* fy, double* fz, bool* host) {

@@ -377,6 +377,28 @@ template cudaError_t launch_virial<double>(const double2*, const double*, const 
 template cudaError_t launch_virial<float>(const float2*, const float*, const GreenGeom&, double,
                                           double, double*, unsigned*, int, double*, cudaStream_t);
 
+// Copy of the atoms with every charge set to 1 (the field at the atoms is
+// the gather of a unit charge); in and out may be the same buffer.
+template <typename CT>
+__global__ void k_unit_charges(const typename Vec4<CT>::type* in, typename Vec4<CT>::type* out,
+                               int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    typename Vec4<CT>::type a = in[i];
+    a.w = (CT)1;
+    out[i] = a;
+  }
+}
+
+template <typename CT>
+cudaError_t launch_unit_charges(const typename Vec4<CT>::type* in, typename Vec4<CT>::type* out,
+                                int n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_unit_charges<CT><<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+template cudaError_t launch_unit_charges<double>(const double4*, double4*, int, cudaStream_t);
+template cudaError_t launch_unit_charges<float>(const float4*, float4*, int, cudaStream_t);
+
 // factor * sum_i (double)(a[i]*b[i]) (the product in CT, as CpuGSE.cpp:97),
 // finished by the last block.  done is the zeroed counter the last block
 // resets (the slot after the partials that the other energy kernels use).

@@ -56,6 +56,11 @@ cudaError_t launch_virial(const typename Cplx<CT>::type* rhok, const CT* tab, co
                           double half_sigma2, double factor, double* partials, unsigned* done,
                           int nblocks, double* out, cudaStream_t st);
 
+// out[i] = in[i] with the charge set to 1 (in place allowed).
+template <typename CT>
+cudaError_t launch_unit_charges(const typename Vec4<CT>::type* in, typename Vec4<CT>::type* out,
+                                int n, cudaStream_t st);
+
 template <typename CT>
 cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* partials, int np,
                               double factor, double* energy_out, cudaStream_t st);

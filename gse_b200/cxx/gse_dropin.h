@@ -370,6 +370,12 @@ class CpuGSE {
     check(gse_get_grid(ctx_.get(), GSE_GRID_PHI, phiM.getDataPointer()));
     return phiM;
   }
+  // Electric field at the atoms (force per unit charge, times ccelec) from
+  // phiM; the reference's interpolation loop serves force and field alike.
+  void interpolateField(const int numCoord, const xyzq_t<CT>* xyzq, AT* fieldX, AT* fieldY,
+                        AT* fieldZ) {
+    check(gse_interpolate_field(ctx_.get(), numCoord, xyzq, fieldX, fieldY, fieldZ));
+  }
   // Reciprocal-space virial of the current rhoS (xx, yy, zz, xy, xz, yz); the
   // reference classes compute none (gse_virial).
   void calculateVirial(double virial[6]) { check(gse_virial(ctx_.get(), virial)); }

@@ -137,6 +137,10 @@ class Context:
     def fft_solve(self, sigma, boxx, boxy, boxz, rho, phi):
         check(self._L.gse_fft_solve(self.h, sigma, boxx, boxy, boxz, ptr(rho), ptr(phi)))
 
+    def interpolate_field(self, n, xyzq, ex, ey, ez):
+        """Electric field at the atoms (force per unit charge) from phiM."""
+        check(self._L.gse_interpolate_field(self.h, int(n), ptr(xyzq), ptr(ex), ptr(ey), ptr(ez)))
+
     def virial(self, out=None):
         """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS."""
         if out is None:
@@ -409,6 +413,10 @@ class CpuGSE:
     def getPhi(self) -> CpuGrid:
         self._ctx.get_grid(_lib.GRID_PHI, self.phiM.data)
         return self.phiM
+
+    def interpolateField(self, numCoord, xyzq, fieldX, fieldY, fieldZ):
+        """Electric field at the atoms (force per unit charge) from phiM."""
+        self._ctx.interpolate_field(numCoord, _xyzq_arg(xyzq, self.dtype), fieldX, fieldY, fieldZ)
 
     def calculateVirial(self):
         """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS; the

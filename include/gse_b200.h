@@ -131,6 +131,15 @@ gse_status_t gse_calculate_energy(gse_context_t* ctx, double* energy);
 gse_status_t gse_interpolate_force(gse_context_t* ctx, int n, const void* xyzq, double* fx,
                                    double* fy, double* fz);
 
+/* The electric field at the atoms from phiM (after gse_solve_poisson or
+ * gse_forward): the gather of interpolateForce (CpuGSE.cpp:70-80,
+ * CpuGaussCharge.cpp:105-172, the loop the reference shares between force and
+ * field) with every charge taken as 1, i.e. the force per unit charge, times
+ * ccelec; defined for neutral sites too.  The charges in xyzq are ignored.
+ * Outputs are overwritten. */
+gse_status_t gse_interpolate_field(gse_context_t* ctx, int n, const void* xyzq, double* ex,
+                                   double* ey, double* ez);
+
 /* One whole force evaluation: spreadCharge1 -> solvePoisson ->
  * calculateEnergy -> interpolateForce, as cpu_gse runs them
  * (cpu_gse.cpp:440-455).  `energy` and the force arrays may be NULL to skip

@@ -290,3 +290,31 @@ def test_own_fft_matches_cufft_and_fp64(n2, monkeypatch):
     assert rms(Fo, Fd) <= 1e-5
     assert abs(Eo - Ec) <= 1e-6 * abs(Ec)
     assert abs(Eo - Ed) <= 1e-6 * abs(Ed)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("mixed", 1e-6)])
+def test_field_at_atoms_is_force_per_unit_charge(precision, tol):
+    """gse_interpolate_field: the gather with unit charges.  On charged atoms
+    q E equals the force (to the rounding of q times the prefactor); a site
+    made neutral keeps the field its charged twin sees."""
+    from gse_b200 import workloads as W
+    from gse_b200.gse import CpuGSEk
+    L, M = 24.0, 24
+    x = W.triplets(900, L, 12).astype(np.float64)
+    ct = np.float64 if precision == "fp64" else np.float32
+    n = x.shape[0]
+    g = CpuGSEk(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision=precision)
+    F = [np.zeros(n) for _ in range(3)]
+    g.forward(n, x.astype(ct), *F)
+    F = np.stack(F, 1)
+    E = [np.zeros(n) for _ in range(3)]
+    g.interpolateField(n, x.astype(ct), *E)
+    E = np.stack(E, 1)
+    q = x[:, 3].astype(ct).astype(np.float64)
+    d = E * q[:, None] - F
+    assert np.sqrt((d * d).sum() / (F * F).sum()) <= tol
+    x0 = x.copy()
+    x0[::7, 3] = 0.0
+    E0 = [np.zeros(n) for _ in range(3)]
+    g.interpolateField(n, x0.astype(ct), *E0)
+    assert np.array_equal(np.stack(E0, 1), E)
