@@ -267,12 +267,16 @@ def test_own_fft_matches_cufft_and_fp64(n2, monkeypatch):
     from gse_b200.gse import Context
     M = 16 * n2
     L = 0.97 * M
+    # one orthorhombic box: the grid stays cubic, the Green's table does not
+    aspect = np.array([1.0, 1.1, 0.9]) if n2 == 5 else np.ones(3)
+    box = tuple(L * aspect)
     x = W.triplets(1500, L, 20 + n2).astype(np.float32)
+    x[:, :3] *= aspect.astype(np.float32)
     n = x.shape[0]
 
     def evaluate(precision, own):
         monkeypatch.setenv("GSE_B200_OWN_FFT", "1" if own else "0")
-        ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision=precision)
+        ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, *box, precision=precision)
         xx = x.astype(np.float64) if precision == "fp64" else x
         f = [np.zeros(n) for _ in range(3)]
         E = ctx.forward(n, xx, *f)
