@@ -99,6 +99,8 @@ SIGNATURES = {
     "gse_spread_mixed_noalloc": (_i, [_i, _i, _i, _d, _d, _i, _vp, _d, _d, _d, _vp, _vp]),
     "gse_adjoint": (_i, [_vp, _i, _vp, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gse_ewald_recip": (_i, [_i, _vp, _d, _i, _d, _d, _d, _d, _i, _vp, _vp, _vp, _vp, _vp]),
+    "gse_ewald_direct": (_i, [_i, _vp, _d, _d, _d, _d, _d, _d, _i, _vp, _i, _vp, _vp, _vp, _vp,
+                              _vp, _vp]),
     "gse_get_paths": (_i, [_vp, ctypes.POINTER(_i)]),
     "gse_batch_create": (_i, [ctypes.POINTER(gse_params_t), _i, ctypes.POINTER(gse_system_t),
                               ctypes.POINTER(_vp)]),

@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <string>
@@ -1644,6 +1645,146 @@ gse_status_t gse_ewald_recip(int device, void* stream, double sigma, int kcut, d
   for (double v : rh) e += v;
   *energy = e;
   cleanup();
+  return GSE_OK;
+}
+
+gse_status_t gse_ewald_direct(int device, void* stream, double sigma, double rcut, double box_x,
+                              double box_y, double box_z, double ccelec, int n, const double* xyzq,
+                              int n_iblo14, const int* iblo14, const int* inb14, double* energy,
+                              double* fx, double* fy, double* fz) {
+  g_last_error.clear();
+  if (!(sigma > 0.0) || !(rcut > 0.0) || !(box_x > 0 && box_y > 0 && box_z > 0) || n < 0 ||
+      (n > 0 && !xyzq) || !energy || !std::isfinite(rcut) || !std::isfinite(sigma) ||
+      !std::isfinite(box_x) || !std::isfinite(box_y) || !std::isfinite(box_z))
+    return fail(GSE_ERR_INVALID_ARG, "bad Ewald direct arguments");
+  const bool want_f = fx || fy || fz;
+  if (want_f && !(fx && fy && fz)) return fail(GSE_ERR_INVALID_ARG, "give all force arrays or none");
+  // exclusions: setupExclusions (CpuEwaldDirect.cpp:31-40) asks for one
+  // cumulative end per atom (CpuEwaldDirect.cpp:47) and reads |inb14| - 1
+  if (n_iblo14 < 0 || (n_iblo14 > 0 && (n_iblo14 != n || !iblo14)))
+    return fail(GSE_ERR_INVALID_ARG, "iblo14 must hold one entry per atom");
+  std::vector<int> ex_start, ex_idx;
+  if (n_iblo14 > 0) {
+    int prev = 0;
+    for (int a = 0; a < n; a++) {
+      if (iblo14[a] < prev)
+        return fail(GSE_ERR_INVALID_ARG, "iblo14 must be non-decreasing from 0 (atom %d)", a);
+      prev = iblo14[a];
+    }
+    if (prev > 0 && !inb14) return fail(GSE_ERR_INVALID_ARG, "inb14 is NULL");
+    // the pair (a, b), a < b, is skipped when b is listed under a
+    // (CpuEwaldDirect.cpp:71-85); entries at or below a never match
+    std::vector<int> cnt(n + 1, 0);
+    auto partner = [&](int k) { return (long long)std::llabs((long long)inb14[k]) - 1; };
+    for (int a = 0, k = 0; a < n; a++)
+      for (; k < iblo14[a]; k++) {
+        const long long b = partner(k);
+        if (b > a && b < n) {
+          cnt[a]++;
+          cnt[b]++;
+        }
+      }
+    ex_start.assign(n + 1, 0);
+    for (int a = 0; a < n; a++) ex_start[a + 1] = ex_start[a] + cnt[a];
+    ex_idx.resize(ex_start[n]);
+    std::vector<int> fill(ex_start.begin(), ex_start.end() - 1);
+    for (int a = 0, k = 0; a < n; a++)
+      for (; k < iblo14[a]; k++) {
+        const long long b = partner(k);
+        if (b > a && b < n) {
+          ex_idx[fill[a]++] = (int)b;
+          ex_idx[fill[b]++] = a;
+        }
+      }
+    for (int a = 0; a < n; a++)
+      std::sort(ex_idx.begin() + ex_start[a], ex_idx.begin() + ex_start[a + 1]);
+  }
+  CU(cudaSetDevice(device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n == 0) {
+    *energy = 0.0;
+    return GSE_OK;
+  }
+  const double box[3] = {box_x, box_y, box_z};
+  const EwdGeom g = ewald_direct_geom(sigma, rcut, box, ccelec);
+  const int ntiles = (g.ncell + 4095) / 4096;
+  // one allocation: ints, then doubles (8-byte aligned), then atoms
+  const size_t n_int = 2 * (size_t)n + (size_t)g.ncell * 2 + 1 + ntiles + n + 1 + ex_idx.size() +
+                       (ex_start.empty() ? 0 : n + 1);
+  const size_t off_d = (n_int * sizeof(int) + 31) / 32 * 32;
+  const size_t n_dbl = (size_t)g.ncell + 1 + (want_f ? 3 * (size_t)n : 0);
+  const size_t off_x = (off_d + n_dbl * sizeof(double) + 31) / 32 * 32;
+  const bool xdev = is_device_ptr(xyzq);
+  const size_t bytes = off_x + (size_t)n * sizeof(double4) * (xdev ? 1 : 2);
+  char* buf = nullptr;
+  {
+    cudaError_t e0 = cudaMalloc(&buf, bytes);
+    if (e0 != cudaSuccess)
+      return fail(e0 == cudaErrorMemoryAllocation ? GSE_ERR_OOM : GSE_ERR_CUDA,
+                  "gse_ewald_direct: cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e0));
+  }
+  gse_status_t status = GSE_OK;
+#define CUE(call)                                                                          \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      status = fail(_e == cudaErrorMemoryAllocation ? GSE_ERR_OOM : GSE_ERR_CUDA,          \
+                    "gse_ewald_direct: %s: %s", #call, cudaGetErrorString(_e));            \
+      cudaFree(buf);                                                                       \
+      return status;                                                                       \
+    }                                                                                      \
+  } while (0)
+  int* ip = (int*)buf;
+  EwdScratch w;
+  w.key = ip;
+  ip += n;
+  w.tmp = ip;
+  ip += n;
+  w.counts = ip;
+  ip += g.ncell;
+  w.start = ip;
+  ip += g.ncell + 1;
+  w.tile_sums = ip;
+  ip += ntiles;
+  w.perm = ip;
+  ip += n;
+  w.done = (unsigned*)ip;
+  ip += 1;
+  int* d_ex_idx = ip;
+  ip += ex_idx.size();
+  int* d_ex_start = ex_start.empty() ? nullptr : ip;
+  double* dp = (double*)(buf + off_d);
+  w.partials = dp;
+  double* d_energy = dp + g.ncell;
+  double* f[3] = {fx, fy, fz};
+  const bool fdev = want_f && is_device_ptr(fx) && is_device_ptr(fy) && is_device_ptr(fz);
+  if (want_f && !fdev)
+    for (int k = 0; k < 3; k++) f[k] = d_energy + 1 + (size_t)k * n;
+  w.sorted = (double4*)(buf + off_x);
+  const double4* xin = (const double4*)xyzq;
+  if (!xdev) {
+    double4* xd = w.sorted + n;
+    CUE(cudaMemcpyAsync(xd, xyzq, sizeof(double4) * n, cudaMemcpyHostToDevice, st));
+    xin = xd;
+  }
+  if (d_ex_start) {
+    if (!ex_idx.empty())
+      CUE(cudaMemcpyAsync(d_ex_idx, ex_idx.data(), sizeof(int) * ex_idx.size(),
+                          cudaMemcpyHostToDevice, st));
+    CUE(cudaMemcpyAsync(d_ex_start, ex_start.data(), sizeof(int) * (n + 1),
+                        cudaMemcpyHostToDevice, st));
+  }
+  CUE(launch_ewald_direct(xin, n, g, w, d_ex_start, d_ex_start ? d_ex_idx : nullptr,
+                          want_f ? f[0] : nullptr, f[1], f[2], d_energy, st));
+  CUE(cudaMemcpyAsync(energy, d_energy, sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (want_f && !fdev) {
+    CUE(cudaMemcpyAsync(fx, f[0], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUE(cudaMemcpyAsync(fy, f[1], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    CUE(cudaMemcpyAsync(fz, f[2], sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
+  CUE(cudaStreamSynchronize(st));
+#undef CUE
+  cudaFree(buf);
   return GSE_OK;
 }
 

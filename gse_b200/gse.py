@@ -472,6 +472,77 @@ def ewald_recip(sigma, kcut, box, xyzq, ccelec=CCELEC, forces=True, device=0, st
     return e.value, None
 
 
+def ewald_direct(sigma, rcut, box, xyzq, iblo14=None, inb14=None, ccelec=CCELEC, forces=True,
+                 device=0, stream=None):
+    """FP64 Ewald direct sum with self energy on the GPU (CpuEwaldDirect::
+    calcForceEnergy, CpuEwaldDirect.cpp:45-131), with the exclusion lists of
+    setupExclusions (CpuEwaldDirect.cpp:31-40) when iblo14 and inb14 are given.
+    Returns (E, F[n, 3]) or (E, None); F is the gradient dE/dx, as the
+    reference's force arrays hold it."""
+    L = _lib.load()
+    a = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)
+    n = a.shape[0]
+    nib, ib, nb = 0, None, None
+    if iblo14 is not None:
+        ib = np.ascontiguousarray(iblo14, dtype=np.int32)
+        nb = np.ascontiguousarray(inb14 if inb14 is not None else [], dtype=np.int32)
+        nib = ib.shape[0]
+        if nib and nb.shape[0] < ib[-1]:
+            raise ValueError("inb14 is shorter than iblo14[-1]")
+    e = ctypes.c_double()
+    f = np.zeros((3, n)) if forces else None
+    fp = [f[k].ctypes.data for k in range(3)] if forces else [None] * 3
+    check(L.gse_ewald_direct(device, stream, sigma, rcut, box[0], box[1], box[2], ccelec, n,
+                             a.ctypes.data, nib, None if ib is None else ib.ctypes.data,
+                             None if nb is None else nb.ctypes.data, ctypes.addressof(e), *fp))
+    return e.value, (f.T.copy() if forces else None)
+
+
+class CpuEwaldRecip:
+    """CpuEwaldRecip (CpuEwaldRecip.h:11-44) on the GPU in FP64:
+    calcForceEnergy(n, xyzq, fx, fy, fz) -> energy, writing the force arrays."""
+
+    def __init__(self, sigma, kcut, boxx, boxy, boxz, ccelec=CCELEC, device=0):
+        self.sigma, self.kcut, self.ccelec, self.device = float(sigma), int(kcut), ccelec, device
+        self.box = (float(boxx), float(boxy), float(boxz))
+
+    def setSigma(self, sigma):
+        self.sigma = float(sigma)
+
+    def setBoxsize(self, boxx, boxy, boxz):
+        self.box = (float(boxx), float(boxy), float(boxz))
+
+    def calcForceEnergy(self, n, xyzq, fx, fy, fz) -> float:
+        a = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)[:n]
+        e, f = ewald_recip(self.sigma, self.kcut, self.box, a, self.ccelec, True, self.device)
+        fx[:n], fy[:n], fz[:n] = f[:, 0], f[:, 1], f[:, 2]
+        return e
+
+
+class CpuEwaldDirect:
+    """CpuEwaldDirect (CpuEwaldDirect.h:10-44) on the GPU in FP64:
+    setupExclusions(n_iblo14, iblo14, inb14), then calcForceEnergy(n, xyzq,
+    fx, fy, fz) -> energy including the self energy, writing the gradient
+    into the force arrays."""
+
+    def __init__(self, sigma, rcut, boxx, boxy, boxz, ccelec=CCELEC, device=0):
+        self.sigma, self.rcut, self.ccelec, self.device = float(sigma), float(rcut), ccelec, device
+        self.box = (float(boxx), float(boxy), float(boxz))
+        self._iblo14 = self._inb14 = None
+
+    def setupExclusions(self, n_iblo14, iblo14, inb14):
+        ib = np.array(iblo14[:n_iblo14], dtype=np.int32)
+        self._iblo14 = ib
+        self._inb14 = np.array(inb14[:ib[-1] if n_iblo14 else 0], dtype=np.int32)
+
+    def calcForceEnergy(self, n, xyzq, fx, fy, fz) -> float:
+        a = np.ascontiguousarray(xyzq, dtype=np.float64).reshape(-1, 4)[:n]
+        e, f = ewald_direct(self.sigma, self.rcut, self.box, a, self._iblo14, self._inb14,
+                            self.ccelec, True, self.device)
+        fx[:n], fy[:n], fz[:n] = f[:, 0], f[:, 1], f[:, 2]
+        return e
+
+
 def ewald_kcut(sigma, box, tol=1e-12):
     """Smallest integer k cut-off with exp(-sigma^2 k^2 / 2) below tol along the longest box side."""
     import math

@@ -116,6 +116,23 @@ def random_charges(n: int, box: float, seed: int = 1) -> np.ndarray:
     return out
 
 
+def triplet_exclusions(n_atoms: int):
+    """Exclusion lists of rigid 3-site molecules in CHARMM's format, as
+    CpuEwaldDirect::setupExclusions reads them (CpuEwaldDirect.cpp:31-40):
+    iblo14[a] is the cumulative end of atom a's entries in inb14, whose
+    entries are 1-based partners.  Each molecule (O, H, H) lists O-H1 and
+    O-H2 under O and H1-H2 under H1; an atom left over after the last whole
+    molecule has none."""
+    iblo14 = np.zeros(n_atoms, dtype=np.int32)
+    inb14 = []
+    for a in range(n_atoms):
+        m0 = a - a % 3
+        if m0 + 2 < n_atoms:
+            inb14.extend(b + 1 for b in range(a + 1, m0 + 3))
+        iblo14[a] = len(inb14)
+    return iblo14, np.array(inb14, dtype=np.int32)
+
+
 # --------------------------------------------------------------------------
 # Named workloads (sizes as the GSE-k benchmark configurations state them)
 # --------------------------------------------------------------------------

@@ -255,6 +255,27 @@ gse_status_t gse_ewald_recip(int device, void* stream, double sigma, int kcut, d
                              double box_y, double box_z, double ccelec, int n, const double* xyzq,
                              double* energy, double* fx, double* fy, double* fz);
 
+/* CpuEwaldDirect (CpuEwaldDirect.h:10-44): the constructor's sigma, rcut, box
+ * and ccelec, setupExclusions (CpuEwaldDirect.cpp:31-40) and calcForceEnergy
+ * (CpuEwaldDirect.cpp:45-131) in one call, on the GPU in FP64.  Over the pairs
+ * at minimum-image distance r < rcut that are not excluded,
+ * E = sum ccelec q_i q_j erfc(r / (sqrt(2) sigma)) / r
+ *     - ccelec / sqrt(2 pi sigma^2) sum_i q_i^2,
+ * and fx, fy, fz receive the gradient dE/dx of every atom, as the reference's
+ * force arrays do (all three may be NULL).  Exclusions in CHARMM's format:
+ * n_iblo14 = 0 for none (iblo14, inb14 may then be NULL), else n_iblo14 = n,
+ * iblo14[a] the cumulative end of atom a's entries in inb14 (non-decreasing
+ * from 0) and |inb14[k]| the 1-based partner; the pair (a, b), a < b, is
+ * skipped when b is listed under a.  Exclusion arrays and energy are host
+ * memory; xyzq (double4 per atom) and the force arrays host or device memory.
+ * Independent of any context; it allocates its own scratch and returns after
+ * the results are written.  The result does not depend on the order in which
+ * the GPU runs its blocks. */
+gse_status_t gse_ewald_direct(int device, void* stream, double sigma, double rcut, double box_x,
+                              double box_y, double box_z, double ccelec, int n, const double* xyzq,
+                              int n_iblo14, const int* iblo14, const int* inb14, double* energy,
+                              double* fx, double* fy, double* fz);
+
 /* ---- instrumentation (no reference counterpart) ------------------------ */
 
 typedef enum gse_stage {

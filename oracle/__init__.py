@@ -29,6 +29,7 @@ CCELEC = 332.0716
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int)
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _d = ctypes.c_double
@@ -86,7 +87,8 @@ def lib():
         L.orc_gsek_forward_d.restype = _i
         L.orc_ewald_recip.argtypes = [_d, _i, _d, _d, _d, _d, _i, _dp, _dp, _dp, _dp]
         L.orc_ewald_recip.restype = _d
-        L.orc_ewald_direct.argtypes = [_d, _d, _d, _d, _d, _d, _i, _dp, _dp, _dp, _dp]
+        L.orc_ewald_direct.argtypes = [_d, _d, _d, _d, _d, _d, _i, _dp, _i, _ip, _ip, _dp, _dp,
+                                       _dp]
         L.orc_ewald_direct.restype = _d
         _lib = L
     return _lib
@@ -126,7 +128,8 @@ def ref():
         R.ref_green_mul_d.restype = _i
         R.ref_ewald_recip.argtypes = [_d, _i, _d, _d, _d, _d, _i, _dp, _dp, _dp, _dp]
         R.ref_ewald_recip.restype = _d
-        R.ref_ewald_direct.argtypes = [_d, _d, _d, _d, _d, _d, _i, _dp, _dp, _dp, _dp]
+        R.ref_ewald_direct.argtypes = [_d, _d, _d, _d, _d, _d, _i, _dp, _i, _ip, _ip, _dp, _dp,
+                                       _dp]
         R.ref_ewald_direct.restype = _d
         _ref = R
     return _ref
@@ -291,12 +294,26 @@ def ewald_recip(sigma, kcut, box, xyzq, ccelec=CCELEC, forces=True):
     return float(e), None
 
 
-def ewald_direct(sigma, rcut, box, xyzq, ccelec=CCELEC):
+def _excl(iblo14, inb14):
+    """(n_iblo14, iblo14, inb14) as int32 arrays for the exclusion arguments."""
+    if iblo14 is None:
+        return 0, None, None
+    ib = np.ascontiguousarray(iblo14, dtype=np.int32)
+    nb = np.ascontiguousarray(inb14 if inb14 is not None else [0], dtype=np.int32)
+    if len(ib) and len(nb) < ib[-1]:
+        raise ValueError("inb14 is shorter than iblo14[-1]")
+    return len(ib), ib, nb
+
+
+def ewald_direct(sigma, rcut, box, xyzq, ccelec=CCELEC, iblo14=None, inb14=None):
+    """CpuEwaldDirect::calcForceEnergy restated (gse_oracle.c), with the
+    exclusion lists of setupExclusions when iblo14/inb14 are given."""
     a = _xyzq(xyzq, np.float64)
     n = a.shape[0]
     fx, fy, fz = (np.zeros(n) for _ in range(3))
-    e = lib().orc_ewald_direct(sigma, rcut, box[0], box[1], box[2], ccelec, n, _ptr(a), _ptr(fx),
-                               _ptr(fy), _ptr(fz))
+    ne, ib, nb = _excl(iblo14, inb14)
+    e = lib().orc_ewald_direct(sigma, rcut, box[0], box[1], box[2], ccelec, n, _ptr(a), ne,
+                               _ptr(ib, _ip), _ptr(nb, _ip), _ptr(fx), _ptr(fy), _ptr(fz))
     return float(e), np.stack([fx, fy, fz], axis=1)
 
 
@@ -390,10 +407,11 @@ def ref_ewald_recip(sigma, kcut, box, xyzq, ccelec=CCELEC):
     return float(e), np.stack([fx, fy, fz], axis=1)
 
 
-def ref_ewald_direct(sigma, rcut, box, xyzq, ccelec=CCELEC):
+def ref_ewald_direct(sigma, rcut, box, xyzq, ccelec=CCELEC, iblo14=None, inb14=None):
     a = _xyzq(xyzq, np.float64)
     n = a.shape[0]
     fx, fy, fz = (np.zeros(n) for _ in range(3))
-    e = ref().ref_ewald_direct(sigma, rcut, box[0], box[1], box[2], ccelec, n, _ptr(a), _ptr(fx),
-                               _ptr(fy), _ptr(fz))
+    ne, ib, nb = _excl(iblo14, inb14)
+    e = ref().ref_ewald_direct(sigma, rcut, box[0], box[1], box[2], ccelec, n, _ptr(a), ne,
+                               _ptr(ib, _ip), _ptr(nb, _ip), _ptr(fx), _ptr(fy), _ptr(fz))
     return float(e), np.stack([fx, fy, fz], axis=1)

@@ -726,11 +726,14 @@ double orc_ewald_recip(double sigma, int kcut, double boxx, double boxy, double 
 }
 
 /* ------------------------------------------------------------------------ */
-/* Ewald direct sum with self energy (no exclusion lists),                   */
-/* CpuEwaldDirect.cpp:45-131.                                                */
+/* Ewald direct sum with self energy, CpuEwaldDirect.cpp:45-131, with the   */
+/* exclusion lists of setupExclusions (CpuEwaldDirect.cpp:31-40) when        */
+/* n_iblo14 > 0: the pair (j, i), j < i, is skipped when i + 1 equals        */
+/* |inb14[k]| for some k in [iblo14[j-1], iblo14[j]) (:71-85).               */
 /* ------------------------------------------------------------------------ */
 double orc_ewald_direct(double sigma, double rcut, double boxx, double boxy, double boxz,
-                        double ccelec, int n, const double* xyzq, double* fx, double* fy,
+                        double ccelec, int n, const double* xyzq, int n_iblo14,
+                        const int* iblo14, const int* inb14, double* fx, double* fy,
                         double* fz) {
   const double rcut2 = rcut * rcut;
   const double hboxx = 0.5 * boxx, hboxy = 0.5 * boxy, hboxz = 0.5 * boxz;
@@ -742,7 +745,12 @@ double orc_ewald_direct(double sigma, double rcut, double boxx, double boxy, dou
   for (int j = 0; j < n - 1; j++) {
     const double xj = xyzq[4 * j], yj = xyzq[4 * j + 1], zj = xyzq[4 * j + 2];
     const double qj = xyzq[4 * j + 3] * ccelec;
+    const int ex0 = (n_iblo14 > 0 && j >= 1) ? iblo14[j - 1] : 0;
+    const int ex1 = n_iblo14 > 0 ? iblo14[j] : 0;
     for (int i = j + 1; i < n; i++) {
+      int skip = 0;
+      for (int k = ex0; k < ex1 && !skip; k++) skip = (abs(inb14[k]) - 1 == i);
+      if (skip) continue;
       double dx = xyzq[4 * i] - xj, dy = xyzq[4 * i + 1] - yj, dz = xyzq[4 * i + 2] - zj;
       while (dx < -hboxx) dx += boxx;
       while (dx > hboxx) dx -= boxx;

@@ -183,9 +183,11 @@ double ref_ewald_recip(double sigma, int kcut, double boxx, double boxy, double 
 }
 
 double ref_ewald_direct(double sigma, double rcut, double boxx, double boxy, double boxz,
-                        double ccelec, int n, const double* xyzq, double* fx, double* fy,
+                        double ccelec, int n, const double* xyzq, int n_iblo14,
+                        const int* iblo14, const int* inb14, double* fx, double* fy,
                         double* fz) {
   CpuEwaldDirect e(sigma, rcut, boxx, boxy, boxz, ccelec);
+  if (n_iblo14 > 0) e.setupExclusions(n_iblo14, iblo14, inb14);
   return e.calcForceEnergy(n, reinterpret_cast<const xyzq_t<double>*>(xyzq), fx, fy, fz);
 }
 

@@ -117,6 +117,36 @@ def test_ewald_direct_restatement_matches_reference(oracle_lib):
     assert np.array_equal(f1, f2)
 
 
+def odd_exclusions(n):
+    """Water exclusions plus entries the reference reads but never matches or
+    matches in one direction only: a negative (1-4) entry, a partner listed
+    under the larger index, a duplicate, a zero and one beyond the last atom."""
+    from gse_b200 import workloads as W
+    ib, nb = W.triplet_exclusions(n)
+    lists = [list(nb[(ib[a - 1] if a else 0):ib[a]]) for a in range(n)]
+    lists[0] += [-5, 2, 0, n + 7]  # -5: pair (0, 4); 2 again; 0 and n + 7 match nothing
+    lists[7] += [2]                # (7, 1) listed under 7 only: not excluded
+    lists[9] += [-(n)]             # pair (9, n - 1)
+    ib2 = np.cumsum([len(l) for l in lists]).astype(np.int32)
+    nb2 = np.array([v for l in lists for v in l], dtype=np.int32)
+    return ib2, nb2
+
+
+def test_ewald_direct_exclusions_match_reference(oracle_lib):
+    if not oracle_lib.have_reference():
+        pytest.skip("reference build not present")
+    from gse_b200 import workloads as W
+    xyzq = W.triplets(300, 14.0, 6).astype(np.float64)
+    ib, nb = odd_exclusions(300)
+    box = (14.0, 13.0, 15.0)
+    e0, _ = oracle_lib.ewald_direct(2.0, 6.0, box, xyzq)
+    e1, f1 = oracle_lib.ewald_direct(2.0, 6.0, box, xyzq, iblo14=ib, inb14=nb)
+    e2, f2 = oracle_lib.ref_ewald_direct(2.0, 6.0, box, xyzq, iblo14=ib, inb14=nb)
+    assert e1 == e2
+    assert np.array_equal(f1, f2)
+    assert abs(e1 - e0) > 1.0  # the intramolecular pairs carry most of the direct energy
+
+
 def test_ewald_known_answer():
     """cpu_gse.cpp:324-330: energy_ew = 1733.61 for data/xyzq_48k.txt,
     sigma 2.12132034355964, box 80, kcut 64 (tests/golden/make_ewald_kat.py)."""
