@@ -463,6 +463,25 @@ def main():
                     "oracle_seconds": t_ew,
                     "mixed": {"force_rms": rel_rms(Fmx), "energy_rel": abs(Emx - e_ew) / abs(e_ew)},
                     "fp64": {"force_rms": rel_rms(F64), "energy_rel": abs(E64 - e_ew) / abs(e_ew)}}
+        # the whole Ewald sum: the same direct (real-space) sum beside GSE-k and
+        # beside the Ewald reciprocal sum (rcut 9, as the reference's drivers use;
+        # no exclusions, as GSE-k's k-space sum has none); the direct sum returns
+        # the gradient dE/dx, GSE-k and the reciprocal sum the force -dE/dx
+        from gse_b200.gse import ewald_direct
+        t0 = time.perf_counter()
+        e_dir, g_dir = ewald_direct(s.sigma, 9.0, s.boxes, s.xyzq.astype(np.float64), device=local)
+        t_dir = time.perf_counter() - t0
+        f_tot = f_ew - g_dir
+
+        def tot_err(F, E):
+            dd = F - f_ew
+            return {"force_rms": float(np.sqrt((dd * dd).sum() / (f_tot * f_tot).sum())),
+                    "energy_rel": abs(E - e_ew) / abs(e_dir + e_ew)}
+
+        accuracy["total"] = {"oracle": f"FP64 Ewald direct (rcut 9.0) + reciprocal (kcut {kc}) "
+                                       "sums on the GPU; GSE-k with the same direct sum",
+                             "direct_seconds": t_dir,
+                             "mixed": tot_err(Fmx, Emx), "fp64": tot_err(F64, E64)}
 
     if rank == 0:
         # roofline of the dominant kernel

@@ -11,6 +11,8 @@
 //   CpuGreensFuncGSE<T>        CpuGreensFuncGSE.h:10-19
 //   CpuFFTSolver<T>            CpuFFTSolver.h:12-42
 //   CpuGSE<AT,CT>, CpuGSEk     CpuGSE.h:19-68, CpuGSEk.h:19-37
+//   CpuEwaldRecip              CpuEwaldRecip.h:11-44 (calcForceEnergy, FP64)
+//   CpuEwaldDirect             CpuEwaldDirect.h:10-44 (FP64)
 //
 // so that a caller switches by including this header instead of the
 // reference's and bringing the names into scope (`using namespace gse_b200;`
@@ -410,6 +412,69 @@ class CpuGSEk : public CpuGSE<AT, CT> {
     check(gse_calculate_energy(this->ctx_.get(), &e));
     return e;
   }
+};
+
+// The FP64 Ewald sums, the accuracy references of the GSE-k forms.  Their
+// arrays are host memory, as in the reference; each call returns with the
+// results written.
+class CpuEwaldRecip {
+ public:
+  CpuEwaldRecip(const double sigma, const int kcut, const double boxx_in, const double boxy_in,
+                const double boxz_in, const double ccelec = 332.0716)
+      : ccelec(ccelec), sigma(sigma), kcut(kcut) {
+    setBoxsize(boxx_in, boxy_in, boxz_in);
+  }
+  // E over the k != 0 with |k|^2 <= kcut^2 and the force -dE/dx
+  // (CpuEwaldRecip.cpp:87-147)
+  double calcForceEnergy(const int n, const xyzq_t<double>* xyzq, double* fx, double* fy,
+                         double* fz) {
+    double e = 0.0;
+    check(gse_ewald_recip(0, nullptr, sigma, kcut, boxx, boxy, boxz, ccelec, n,
+                          reinterpret_cast<const double*>(xyzq), &e, fx, fy, fz));
+    return e;
+  }
+  void setSigma(const double sigma_in) { sigma = sigma_in; }
+  void setBoxsize(const double boxx_in, const double boxy_in, const double boxz_in) {
+    boxx = boxx_in;
+    boxy = boxy_in;
+    boxz = boxz_in;
+  }
+
+ private:
+  const double ccelec;
+  double sigma;
+  int kcut;
+  double boxx, boxy, boxz;
+};
+
+class CpuEwaldDirect {
+ public:
+  CpuEwaldDirect(const double sigma, const double rcut, const double boxx, const double boxy,
+                 const double boxz, const double ccelec = 332.0716)
+      : ccelec(ccelec), sigma(sigma), rcut(rcut), boxx(boxx), boxy(boxy), boxz(boxz) {}
+  // CHARMM exclusion lists (CpuEwaldDirect.cpp:31-40): iblo14[a] is the
+  // cumulative end of atom a's 1-based partners in inb14
+  void setupExclusions(const int n_iblo14_in, const int* iblo14_in, const int* inb14_in) {
+    iblo14.assign(iblo14_in, iblo14_in + n_iblo14_in);
+    const int n_inb14 = n_iblo14_in > 0 ? iblo14.back() : 0;
+    inb14.assign(inb14_in, inb14_in + std::max(n_inb14, 0));
+  }
+  // E including the self energy, and the gradient dE/dx in fx, fy, fz, as
+  // the reference's arrays hold it (CpuEwaldDirect.cpp:45-131)
+  double calcForceEnergy(const int n, const xyzq_t<double>* xyzq, double* fx, double* fy,
+                         double* fz) {
+    double e = 0.0;
+    check(gse_ewald_direct(0, nullptr, sigma, rcut, boxx, boxy, boxz, ccelec, n,
+                           reinterpret_cast<const double*>(xyzq), (int)iblo14.size(),
+                           iblo14.empty() ? nullptr : iblo14.data(),
+                           inb14.empty() ? nullptr : inb14.data(), &e, fx, fy, fz));
+    return e;
+  }
+
+ private:
+  const double ccelec;
+  double sigma, rcut, boxx, boxy, boxz;
+  std::vector<int> iblo14, inb14;
 };
 
 }  // namespace gse_b200

@@ -14,6 +14,8 @@
 
 #include "gse_dropin.h"
 
+using gse_b200::CpuEwaldDirect;
+using gse_b200::CpuEwaldRecip;
 using gse_b200::CpuFFTSolver;
 using gse_b200::CpuGaussCharge;
 using gse_b200::CpuGreensFuncGSE;
@@ -77,6 +79,29 @@ int run(int M[3], double L[3], double sigma, const std::vector<double>& raw) {
              (double)phi.getDataPointer()[i], (double)rhoS.getDataPointer()[i],
              (double)Ex.getDataPointer()[i], (double)Ey.getDataPointer()[i],
              (double)Ez.getDataPointer()[i]);
+  }
+  // the FP64 Ewald references of the same charges (the sequence of
+  // cpu_gse.cpp:555-560), with the water exclusions of rigid 3-site molecules
+  if (getenv("GSE_CHECK_EWALD")) {
+    std::vector<xyzq_t<double>> x64(n);
+    for (int i = 0; i < n; i++)
+      x64[i] = {raw[4 * i], raw[4 * i + 1], raw[4 * i + 2], raw[4 * i + 3]};
+    std::vector<int> iblo14(n), inb14;
+    for (int a = 0; a < n; a++) {
+      const int m0 = a - a % 3;
+      if (m0 + 2 < n)
+        for (int b = a + 1; b < m0 + 3; b++) inb14.push_back(b + 1);
+      iblo14[a] = (int)inb14.size();
+    }
+    CpuEwaldRecip rec(sigma, 12, L[0], L[1], L[2]);
+    const double er = rec.calcForceEnergy(n, x64.data(), fx.data(), fy.data(), fz.data());
+    printf("EWR %.17g\n", er);
+    for (int i = 0; i < n; i++) printf("FWR %.17g %.17g %.17g\n", fx[i], fy[i], fz[i]);
+    CpuEwaldDirect dir(sigma, 9.0, L[0], L[1], L[2]);
+    dir.setupExclusions(n, iblo14.data(), inb14.data());
+    const double ed = dir.calcForceEnergy(n, x64.data(), fx.data(), fy.data(), fz.data());
+    printf("EWD %.17g\n", ed);
+    for (int i = 0; i < n; i++) printf("FWD %.17g %.17g %.17g\n", fx[i], fy[i], fz[i]);
   }
   return 0;
 }

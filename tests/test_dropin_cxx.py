@@ -149,3 +149,30 @@ def test_dropin_grid_operations(goldens, tmp_path, precision, dt):
     v = np.abs(rho.astype(np.float64)) * h.prod()
     scale = np.array([(v * x * h[0]).sum(), (v * y * h[1]).sum(), (v * z * h[2]).sum()])
     assert (np.abs(dip - ref) <= 1e-12 * scale).all()
+
+
+@pytest.mark.gpu
+def test_dropin_ewald_classes(goldens, tmp_path):
+    """CpuEwaldRecip (kcut 12) and CpuEwaldDirect (rcut 9, with the exclusion
+    lists of rigid 3-site molecules) called by a C++ caller, the sequence of
+    cpu_gse.cpp:555-560, against the oracle restatements of the same methods."""
+    import oracle
+    from gse_b200 import workloads as W
+    g = goldens["water300_noncubic"]
+    box = tuple(float(v) for v in g["box"])
+    sigma = float(g["sigma"])
+    out = run(program(), "fp64", g, tmp_path, env={"GSE_CHECK_EWALD": "1"})
+    assert out.returncode == 0, out.stderr
+    vals = {"EWR": [], "FWR": [], "EWD": [], "FWD": []}
+    for line in out.stdout.splitlines():
+        tag, *v = line.split()
+        if tag in vals:
+            vals[tag].append([float(t) for t in v])
+    x = np.asarray(g["xyzq"], dtype=np.float64)
+    er, fr = oracle.ewald_recip(sigma, 12, box, x)
+    ib, nb = W.triplet_exclusions(x.shape[0])
+    ed, fd = oracle.ewald_direct(sigma, 9.0, box, x, iblo14=ib, inb14=nb)
+    assert abs(vals["EWR"][0][0] - er) <= 1e-11 * abs(er)
+    assert rms(np.array(vals["FWR"]), fr) <= 1e-11
+    assert abs(vals["EWD"][0][0] - ed) <= 1e-12 * abs(ed)
+    assert rms(np.array(vals["FWD"]), fd) <= 1e-12
