@@ -13,6 +13,7 @@
 //   CpuGSE<AT,CT>, CpuGSEk     CpuGSE.h:19-68, CpuGSEk.h:19-37
 //   CpuEwaldRecip              CpuEwaldRecip.h:11-44 (calcForceEnergy, FP64)
 //   CpuEwaldDirect             CpuEwaldDirect.h:10-44 (FP64)
+//   Erms, loadArray, saveForce, readForce   cpu_gse.cpp:128-196 (driver text I/O)
 //
 // so that a caller switches by including this header instead of the
 // reference's and bringing the names into scope (`using namespace gse_b200;`
@@ -413,6 +414,56 @@ class CpuGSEk : public CpuGSE<AT, CT> {
     return e;
   }
 };
+
+// ---------------------------------------------------------------------------
+// Text I/O and the force error measure of the reference's driver
+// (cpu_gse.cpp:128-198): the same formats (iostream defaults, one record per
+// line), throwing gse_b200::Error where the reference calls exit(1).
+// ---------------------------------------------------------------------------
+// Relative RMS difference sqrt(sum |x - ref|^2 / sum |ref|^2) (cpu_gse.cpp:128-145).
+inline double Erms(const int n, const double* refx, const double* refy, const double* refz,
+                   const double* x, const double* y, const double* z) {
+  double rms = 0.0, ref = 0.0;
+  for (int i = 0; i < n; i++) {
+    const double dx = x[i] - refx[i], dy = y[i] - refy[i], dz = z[i] - refz[i];
+    rms += dx * dx + dy * dy + dz * dz;
+    ref += refx[i] * refx[i] + refy[i] * refy[i] + refz[i] * refz[i];
+  }
+  return std::sqrt(rms / ref);
+}
+
+// numLine records of `width` whitespace-separated values (cpu_gse.cpp:150-170).
+template <typename T>
+void loadArray(const int width, const int numLine, const char* filename, T* array) {
+  std::ifstream file(filename);
+  if (!file.is_open())
+    throw Error(GSE_ERR_INVALID_ARG, std::string("cannot open ") + filename);
+  for (int i = 0; i < numLine * width; i++)
+    if (!(file >> array[i]))
+      throw Error(GSE_ERR_INVALID_ARG, std::string("error reading ") + filename);
+}
+
+// "fx fy fz" per line (cpu_gse.cpp:172-182).
+template <typename T>
+void saveForce(const char* filename, const int numCoord, const T* forceX, const T* forceY,
+               const T* forceZ) {
+  std::ofstream file(filename);
+  if (!file.is_open())
+    throw Error(GSE_ERR_INVALID_ARG, std::string("cannot open ") + filename);
+  for (int i = 0; i < numCoord; i++)
+    file << forceX[i] << " " << forceY[i] << " " << forceZ[i] << "\n";
+}
+
+// The file saveForce writes (cpu_gse.cpp:185-196).
+template <typename T>
+void readForce(const char* filename, const int numCoord, T* forceX, T* forceY, T* forceZ) {
+  std::ifstream file(filename);
+  if (!file.is_open())
+    throw Error(GSE_ERR_INVALID_ARG, std::string("cannot open ") + filename);
+  for (int i = 0; i < numCoord; i++)
+    if (!(file >> forceX[i] >> forceY[i] >> forceZ[i]))
+      throw Error(GSE_ERR_INVALID_ARG, std::string("error reading ") + filename);
+}
 
 // The FP64 Ewald sums, the accuracy references of the GSE-k forms.  Their
 // arrays are host memory, as in the reference; each call returns with the

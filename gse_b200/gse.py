@@ -257,6 +257,43 @@ class CpuGrid:
                 f.write(f"{v:g}\n")
 
 
+def Erms(n, refx, refy, refz, x, y, z) -> float:
+    """Relative RMS difference of two force sets, sqrt(sum |F - Fref|^2 / sum
+    |Fref|^2) (cpu_gse.cpp:128-145)."""
+    r = np.stack([np.asarray(v, np.float64)[:n] for v in (refx, refy, refz)])
+    d = np.stack([np.asarray(v, np.float64)[:n] for v in (x, y, z)]) - r
+    return float(np.sqrt((d * d).sum() / (r * r).sum()))
+
+
+def loadArray(width, numLine, filename, dtype=np.float64) -> np.ndarray:
+    """numLine records of `width` whitespace-separated values
+    (cpu_gse.cpp:150-170), as an array [numLine, width]; GseError where the
+    reference exits on a short or unreadable file."""
+    try:
+        with open(filename) as f:
+            tok = f.read().split()
+    except OSError as e:
+        raise GseError(1, f"cannot open {filename}: {e}") from None
+    if len(tok) < width * numLine:
+        raise GseError(1, f"error reading {filename}")
+    conv = int if np.issubdtype(np.dtype(dtype), np.integer) else float
+    return np.array([conv(t) for t in tok[:width * numLine]], dtype=dtype).reshape(numLine, width)
+
+
+def saveForce(filename, numCoord, forceX, forceY, forceZ):
+    """'fx fy fz' per line in the iostream default format, six significant
+    digits (cpu_gse.cpp:172-182)."""
+    with open(filename, "w") as f:
+        for i in range(numCoord):
+            f.write(f"{forceX[i]:g} {forceY[i]:g} {forceZ[i]:g}\n")
+
+
+def readForce(filename, numCoord, dtype=np.float64):
+    """The file saveForce writes (cpu_gse.cpp:185-196): (fx, fy, fz)."""
+    a = loadArray(3, numCoord, filename, dtype)
+    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
+
+
 class CpuGaussCharge:
     """CpuGaussCharge<AT,CT> (CpuGaussCharge.h:11-49) on the GPU."""
 
