@@ -44,6 +44,21 @@ def grid_goldens():
     return load_grid_goldens()
 
 
+def load_ref48k():
+    """The reference's own real-system case test48K (make_ref48k.py): the
+    48,191-charge input as float64 [n, 4] and the reference's outputs."""
+    import lzma
+    with lzma.open(os.path.join(GOLDEN, "xyzq_48k.txt.xz"), "rt") as f:
+        x = np.array([float(t) for t in f.read().split()], dtype=np.float64).reshape(-1, 4)
+    z = np.load(os.path.join(GOLDEN, "ref48k.npz"))
+    return x, {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope="session")
+def ref48k():
+    return load_ref48k()
+
+
 @pytest.fixture(scope="session")
 def oracle_lib():
     import oracle
