@@ -18,6 +18,7 @@
 //           + c q_j A sum_{sphere} e phi [G_j - (G_j . u) u / s^2],
 // e = exp(-|u|^2 / (2 s^2)).  The sphere's edge is not differentiated (its
 // derivative is zero almost everywhere).
+#include <atomic>
 #include <type_traits>
 
 #include "gse_adjoint.cuh"
@@ -638,7 +639,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
 
 namespace {
 template <class K>
-cudaError_t set_smem_once(K kernel, size_t bytes, bool* done) {
+cudaError_t set_smem_once(K kernel, size_t bytes, std::atomic<bool>* done) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -654,7 +655,7 @@ cudaError_t adj_scatter_w(const float4* sorted, const int* perm, const int* star
                           const BinLayout& b, const Stencil<float>& s, double c, const double* gfx,
                           const double* gfy, const double* gfz, long long* grid64, float* lambda,
                           cudaStream_t st) {
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   const size_t smem = sizeof(int) * ScatterGeom<W>::words;
   cudaError_t e = set_smem_once(k_adj_scatter<W>, smem, done);
   if (e != cudaSuccess) return e;
@@ -676,7 +677,7 @@ cudaError_t adj_gather_w(const float4* sorted, const int* perm, const int* start
                          double c, double gE_ch3, const float* psi, const float* phi,
                          const double* gfx, const double* gfy, const double* gfz, double* dq,
                          double* dx, double* dy, double* dz, cudaStream_t st) {
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   const size_t smem = AdjGatherGeom<W>::bytes;
   const cudaError_t e = set_smem_once(k_adj_gather_tiled<W>, smem, done);
   if (e != cudaSuccess) return e;
@@ -729,7 +730,7 @@ cudaError_t launch_batch_adj_scatter(const float4* sorted, const int* perm, cons
     if (ni <= 0) continue;
 #define GSE_BAS(WW)                                                                          \
   case WW: {                                                                                 \
-    static bool done[64] = {};                                                               \
+    static std::atomic<bool> done[64];                                                               \
     const size_t smem = sizeof(int) * ScatterGeom<WW>::words;                                \
     e = set_smem_once(k_batch_adj_scatter<WW>, smem, done);                                  \
     if (e == cudaSuccess)                                                                    \
@@ -767,7 +768,7 @@ cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm,
     cudaError_t e;
 #define GSE_BAG(WW)                                                                          \
   case WW: {                                                                                 \
-    static bool done[64] = {};                                                               \
+    static std::atomic<bool> done[64];                                                               \
     const size_t smem = AdjGatherGeom<WW>::bytes;                                            \
     e = set_smem_once(k_batch_adj_gather_tiled<WW>, smem, done);                             \
     if (e == cudaSuccess)                                                                    \

@@ -24,6 +24,7 @@
 // factor are those of the cuFFT path.
 #include "gse_fft.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <vector>
 
@@ -452,7 +453,7 @@ namespace {
 
 // Opt each plane kernel in to its shared memory once per device.
 template <typename K>
-cudaError_t allow_smem(K kernel, size_t bytes, bool (&done)[64]) {
+cudaError_t allow_smem(K kernel, size_t bytes, std::atomic<bool> (&done)[64]) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -470,7 +471,7 @@ cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float
                    float2* rhok, const float2* tw, cudaStream_t st) {
   constexpr int M = 16 * N2;
   constexpr size_t smem = plane_smem<N2>();
-  static bool fx[64] = {}, fl[64] = {};
+  static std::atomic<bool> fx[64], fl[64];
   if (g64) {
     cudaError_t e = allow_smem(k_own_fft_xy_fwd<N2, true>, smem, fx);
     if (e != cudaSuccess) return e;
@@ -498,7 +499,7 @@ template <int N2>
 cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, cudaStream_t st) {
   constexpr int M = 16 * N2;
   constexpr size_t smem = plane_smem<N2>();
-  static bool fi[64] = {};
+  static std::atomic<bool> fi[64];
   cudaError_t e = allow_smem(k_own_fft_xy_inv<N2>, smem, fi);
   if (e != cudaSuccess) return e;
   k_own_fft_xy_inv<N2><<<M, kPlaneThreads, smem, st>>>(rhok, phi, tw);

@@ -18,6 +18,7 @@
 //            potential of the brick plus its n-cell halo in shared memory;
 //            kGatherLanes lanes per atom, over the non-empty (y, z) rows of
 //            its sphere.
+#include <atomic>
 #include <type_traits>
 
 #include "gse_internal.cuh"
@@ -867,7 +868,7 @@ static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* pe
                             const CT* phi, double outscale, double* fx, double* fy, double* fz,
                             cudaStream_t st) {
   const size_t smem = GatherGeom<CT, W>::bytes;
-  static bool attr[64] = {};
+  static std::atomic<bool> attr[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -909,7 +910,7 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
                              cudaStream_t st) {
   typedef ScatterGeom<W> G;
   const size_t smem = sizeof(int) * G::words;
-  static bool attr[64] = {};
+  static std::atomic<bool> attr[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -1049,7 +1050,7 @@ __global__ void __launch_bounds__(kGatherThreads, 2)
 }
 
 template <class K>
-static cudaError_t set_max_smem(K kernel, size_t bytes, bool* done) {
+static cudaError_t set_max_smem(K kernel, size_t bytes, std::atomic<bool>* done) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -1064,7 +1065,7 @@ template <int W>
 static cudaError_t batch_scatter_w(const float4* sorted, const int* start, const BatchSys* sys,
                                    const BatchItem* items, int nitems, int ctas,
                                    long long* grid64, cudaStream_t st) {
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   const size_t smem = sizeof(int) * ScatterGeom<W>::words;
   const cudaError_t e = set_max_smem(k_batch_scatter<W>, smem, done);
   if (e != cudaSuccess) return e;
@@ -1078,7 +1079,7 @@ static cudaError_t batch_gather_w(const float4* sorted, const int* perm, const i
                                   const BatchSys* sys, const BatchItem* items, int nitems,
                                   int ctas, const float* phi, double outscale, double* fx,
                                   double* fy, double* fz, cudaStream_t st) {
-  static bool done[64] = {};
+  static std::atomic<bool> done[64];
   const size_t smem = GatherGeom<float, W>::bytes;
   const cudaError_t e = set_max_smem(k_batch_gather<W>, smem, done);
   if (e != cudaSuccess) return e;
