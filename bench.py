@@ -13,7 +13,9 @@ each evaluation; L2 is flushed between timed evaluations).  `e2e` is the same
 metric through the public call with pinned host buffers (host->device copy of
 the positions and device->host copy of forces and energy inside every step).
 With N > 1 (torchrun) every rank evaluates its own independent replica:
-replicas only, no collective on the data path.
+replicas only, no collective on the data path.  The batched workload (256
+independent systems) is partitioned across the ranks (gse_b200.multi) and
+reported as 256 systems over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -193,23 +195,29 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-def bench_batch(steps: int, warmup: int, flush):
+def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
     """The batching workload: 256 independent triplet systems, N log-uniform in
     [501, 8001], forward + reverse pass replayed from one CUDA graph after the
-    autotuner has picked the persistent-CTA counts and the work order."""
+    autotuner has picked the persistent-CTA counts and the work order.  With
+    several ranks the systems are partitioned across them (no collective on the
+    data path); every rank times its share, and the rate is the 256 systems over
+    the slowest rank's time.  All ranks must call it."""
     import tempfile
 
     import torch
+    from gse_b200 import multi
     from gse_b200 import workloads as W
     from gse_b200.gse import Batch
-    syst = W.config_batch(256)
+    every = W.config_batch(256)
+    part = multi.partition_systems([multi.system_cost(y.n, y.grid) for y in every], world)
+    syst = [every[i] for i in part[rank]]
     desc = [{"size": y.grid, "box": y.boxes, "n": y.n} for y in syst]
     b = Batch(desc, sigma=2.0, kappa=0.4, lambdaSigma1=3.0)
     xyzq = np.concatenate([y.xyzq for y in syst]).astype(np.float32)
     rng = np.random.default_rng(5)
     G = rng.standard_normal((b.n_total, 3)).astype(np.float32).astype(np.float64)
     b.forward(xyzq)
-    cache = os.path.join(tempfile.gettempdir(), "gse_batch_tune.txt")
+    cache = os.path.join(tempfile.gettempdir(), f"gse_batch_tune_r{rank}.txt")
     b.autotune(cache, use_cache=False)
     bufs = b.buffers()
     bufs["xyzq"].copy_(torch.from_numpy(xyzq))
@@ -221,6 +229,7 @@ def bench_batch(steps: int, warmup: int, flush):
     for _ in range(warmup):
         b.launch()
     torch.cuda.synchronize()
+    multi.barrier()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     for k in range(steps):
@@ -229,14 +238,18 @@ def bench_batch(steps: int, warmup: int, flush):
         b.launch()
         ends[k].record(stream)
     torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(c) for a, c in zip(starts, ends)) / steps
+    multi.barrier()
+    ms = multi.max_over_ranks(sum(a.elapsed_time(c) for a, c in zip(starts, ends)) / steps,
+                              device=torch.device("cuda", torch.cuda.current_device()))
+    n_all = sum(y.n for y in every)
     i = b.info()
     out = {"workload": "256 independent triplet systems, N log-uniform in [501, 8001], "
                        "M = nearest multiple of 8 to L, sigma 2.0, mixed form",
-           "n_total": b.n_total, "size_classes": int(i.n_size_classes),
+           "n_total": n_all, "size_classes": int(i.n_size_classes),
            "grid_points": int(i.grid_points), "step": "forward + reverse pass, one CUDA graph",
+           "ranks": world, "systems_rank0": len(part[0]),
            "ms_per_step": ms, "systems_per_s": 256 / (ms / 1000.0),
-           "charges_per_s": b.n_total / (ms / 1000.0),
+           "charges_per_s": n_all / (ms / 1000.0),
            "autotuned": {"scatter_ctas": int(i.scatter_ctas), "gather_ctas": int(i.gather_ctas),
                          "largest_first": bool(i.largest_first)}}
     b.close()
@@ -483,6 +496,16 @@ def main():
                              "direct_seconds": t_dir,
                              "mixed": tot_err(Fmx, Emx), "fp64": tot_err(F64, E64)}
 
+    # the batched workload, partitioned across the ranks (every rank takes part)
+    batch = None
+    if not args.no_batch:
+        try:
+            batch = bench_batch(max(3, min(args.steps, 20)), args.warmup, flush, rank, world)
+        except Exception as exc:  # noqa: BLE001
+            if world > 1:
+                raise  # the other ranks wait in its collectives: fail the job
+            batch = {"failed": str(exc)}
+
     if rank == 0:
         # roofline of the dominant kernel
         peak, peak_kind = hbm_peak()
@@ -513,12 +536,6 @@ def main():
             except Exception as exc:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                        "sample": f"failed: {exc}"}
-        batch = None
-        if not args.no_batch:
-            try:
-                batch = bench_batch(max(3, min(args.steps, 20)), args.warmup, flush)
-            except Exception as exc:  # noqa: BLE001
-                batch = {"failed": str(exc)}
         grid_ops = None
         if not args.no_batch:
             try:
