@@ -155,18 +155,24 @@ __device__ __forceinline__ void brick_flush(const int* __restrict__ tile, const 
   constexpr int n = G::n, T = G::T;
   static_assert(T <= 32, "one lane per tile column");
   const long long mul = 1LL << (kFlushBits - shift);
-  // one (y, z) row of the tile per warp iteration, one lane per x; the
-  // wrapped x of a lane is the same for every row
+  // one lane per x (its wrapped x is the same everywhere); warp w takes the
+  // tile rows y = w, w + NT/32, ..., and walks each row's z column with the
+  // global plane advanced by one step (wrapping at M[2]), so the index
+  // arithmetic per element is one step, not a wrap per axis
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gx = lane < T ? wrap1(x0 - n + lane, b.M[0]) : 0;
-  for (int r = warp; r < T * T; r += NT / 32) {
-    const int zz = r / T, yy = r - zz * T;
-    const int v = lane < T ? tile[zz * G::PP + yy * T + lane] : 0;
-    if (v != 0) {
-      const int gy = wrap1(y0 - n + yy, b.M[1]), gz = wrap1(z0 - n + zz, b.M[2]);
-      atomicAdd((unsigned long long*)(grid64 + gx +
-                                      ((long long)gy + (long long)gz * b.M[1]) * b.M[0]),
-                (unsigned long long)((long long)v * mul));
+  if (lane >= T) return;
+  const long long zs = (long long)b.M[0] * b.M[1];
+  unsigned long long* gxp = (unsigned long long*)grid64 + wrap1(x0 - n + lane, b.M[0]);
+  const int gz0 = wrap1(z0 - n, b.M[2]);
+  for (int yy = warp; yy < T; yy += NT / 32) {
+    unsigned long long* gyp = gxp + (long long)wrap1(y0 - n + yy, b.M[1]) * b.M[0];
+    const int* t = tile + yy * T + lane;
+    int gz = gz0;
+#pragma unroll 4
+    for (int zz = 0; zz < T; zz++) {
+      const int v = t[zz * G::PP];
+      if (v != 0) atomicAdd(gyp + gz * zs, (unsigned long long)((long long)v * mul));
+      gz = (gz + 1 == b.M[2]) ? 0 : gz + 1;
     }
   }
 }
@@ -179,19 +185,26 @@ template <typename CT, int TX, int TY, int TZ, int TP, int ZP, int NW>
 __device__ __forceinline__ void stage_tile_async(const CT* __restrict__ src, const BinLayout& b,
                                                  int x0, int y0, int z0, int n, CT* tile) {
   static_assert(TX <= 32, "one lane per tile column");
+  // one lane per x (its wrapped x is the same everywhere); warp w takes the
+  // tile rows y = w, w + NW, ..., and walks each row's z column with the
+  // global plane advanced by one step (wrapping at M[2])
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane >= TX) return;
   const long long zs = (long long)b.M[0] * b.M[1];
-  const int gx = lane < TX ? wrap1(x0 - n + lane, b.M[0]) : 0;
-  for (int r = warp; r < TY * TZ; r += NW) {
-    const int ty = r % TY, tz = r / TY;
-    const int gy = wrap1(y0 - n + ty, b.M[1]);
-    const int gz = wrap1(z0 - n + tz, b.M[2]);
-    const CT* s = src + (long long)gy * b.M[0] + gz * zs + gx;
-    if (lane < TX) {
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tz * ZP + ty * TP + lane);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(s),
+  const CT* sx = src + wrap1(x0 - n + lane, b.M[0]);
+  const int gz0 = wrap1(z0 - n, b.M[2]);
+  const unsigned base = (unsigned)__cvta_generic_to_shared(tile + lane);
+  for (int ty = warp; ty < TY; ty += NW) {
+    const CT* sy = sx + (long long)wrap1(y0 - n + ty, b.M[1]) * b.M[0];
+    unsigned dst = base + (unsigned)(ty * TP * sizeof(CT));
+    int gz = gz0;
+#pragma unroll 4
+    for (int tz = 0; tz < TZ; tz++) {
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(sy + gz * zs),
                    "n"(sizeof(CT))
                    : "memory");
+      dst += (unsigned)(ZP * sizeof(CT));
+      gz = (gz + 1 == b.M[2]) ? 0 : gz + 1;
     }
   }
 }
