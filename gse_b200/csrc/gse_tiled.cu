@@ -663,13 +663,28 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
 
   CT* tb = tabs + (warp * APW + grp) * 9 * kWPad;  // [axis][d, d^2, w][j]
   int* rl = rowl + (warp * APW + grp) * W * W;
-  // (jy, jz) of the rows each lane tests, the same for every atom
+  // (jy, jz) of the rows each lane tests, the same for every atom: first the
+  // (W-1)^2 rows with jy, jz >= 1, then the 2W-1 rows with jy = 0 or jz = 0,
+  // which lie outside the sphere whenever dy^2 (dz^2) at index 0 is at least
+  // rcut^2 -- for every atom when n h exceeds rcut by more than rounding
+  constexpr int NI = (W - 1) * (W - 1);
+  constexpr int NGI = (NI + GL - 1) / GL;  // groups that hold the inner rows
   int gjy[NG], gjz[NG];
 #pragma unroll
   for (int g = 0; g < NG; g++) {
     const int r = g * GL + gl;
-    gjz[g] = r < W * W ? r / W : 0;
-    gjy[g] = r < W * W ? r - (r / W) * W : 0;
+    if (r < NI) {
+      gjz[g] = 1 + r / (W - 1);
+      gjy[g] = 1 + r % (W - 1);
+    } else if (r < NI + W) {
+      gjz[g] = r - NI;
+      gjy[g] = 0;
+    } else if (r < W * W) {
+      gjz[g] = 0;
+      gjy[g] = r - NI - W + 1;
+    } else {
+      gjz[g] = gjy[g] = 0;
+    }
   }
   const unsigned gmask = GL == 32 ? 0xffffffffu : ((1u << GL) - 1u);
   for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
@@ -697,10 +712,16 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         }
       }
       __syncwarp();
+      // the rows with jy = 0 or jz = 0 are tested only when one of the warp's
+      // atoms could have one inside (adding dz^2 >= 0 cannot take a sum below
+      // dy^2, so dy^2 >= rcut^2 at jy = 0 rules out its whole plane)
+      const bool edges = !__all_sync(0xffffffffu, tb[(1 * 3 + 1) * kWPad + 0] >= s.rcut2 &&
+                                                      tb[(2 * 3 + 1) * kWPad + 0] >= s.rcut2);
       // non-empty rows (the whole row is outside the sphere when dy^2+dz^2 >= rcut^2)
       int nrow = 0;
 #pragma unroll
       for (int g = 0; g < NG; g++) {
+        if (g >= NGI && !edges) break;  // warp-uniform
         const int r = g * GL + gl;
         bool ne = false;
         if (r < W * W)
@@ -721,13 +742,15 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
       // each row's 2n+1 terms and a lane's rows (about rows/16 of them) in CT, the
       // lanes' sums in double (the reference's AT)
       CT lx = 0, ly = 0, lz = 0;
-      // the end points of the rows lie outside the sphere for every row when
-      // dx^2 >= rcut^2 there (rem <= rcut^2): then the rows are summed over
-      // the inner 2n-1 points only, the same terms in the same order
-      const bool ends = dx2[0] < s.rcut2 || dx2[W - 1] < s.rcut2;
-      auto rows = [&](auto trim) {
-        constexpr int K0 = decltype(trim)::value ? 1 : 0;
-        constexpr int K1 = decltype(trim)::value ? W - 1 : W;
+      // an end point of the rows lies outside the sphere for every row when
+      // dx^2 >= rcut^2 there (rem <= rcut^2): the rows are then summed
+      // without it, the same terms in the same order.  The first point is
+      // outside for nearly every atom (n h >= rcut), the last for about half.
+      const bool head = __any_sync(0xffffffffu, dx2[0] < s.rcut2);
+      const bool tail = __any_sync(0xffffffffu, dx2[W - 1] < s.rcut2);
+      auto rows = [&](auto k0, auto k1) {
+        constexpr int K0 = decltype(k0)::value;
+        constexpr int K1 = decltype(k1)::value;
         for (int i = gl; i < nrow; i += GL) {
           const int r = rl[i];
           const int jz = r >> 8, jy = r & 255;
@@ -742,10 +765,12 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
           lz += wyz * tb[(2 * 3 + 0) * kWPad + jz] * s0;
         }
       };
-      if (__any_sync(0xffffffffu, ends))
-        rows(std::false_type());
+      if (head)
+        rows(std::integral_constant<int, 0>(), std::integral_constant<int, W>());
+      else if (tail)
+        rows(std::integral_constant<int, 1>(), std::integral_constant<int, W>());
       else
-        rows(std::true_type());
+        rows(std::integral_constant<int, 1>(), std::integral_constant<int, W - 1>());
       double ax = (double)lx, ay = (double)ly, az = (double)lz;
 #pragma unroll
       for (int o = GL / 2; o > 0; o >>= 1) {
