@@ -185,9 +185,11 @@ def run_reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": r["evals"], "warmup": 1, "ms_per_step": 1000.0 * r["seconds"] / r["evals"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded water-like triplets)",
+        "data": "synthetic (seeded water-like triplets, 87,381 rigid 3-site molecules)",
         "config": {"workload": WORKLOAD, "n_charges": s.n, "grid": s.M, "box": s.box,
-                   "sigma": s.sigma, "precision": "fp64 (reference CPU)"},
+                   "sigma": s.sigma, "kappa": s.kappa, "lambda_sigma1": s.lambda_sigma1,
+                   "precision": "fp64 (reference CPU classes)",
+                   "parallelism": "host CPU threads of rank 0"},
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": kind,
                          "sample": sample},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
