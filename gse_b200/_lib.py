@@ -142,6 +142,29 @@ def check(status: int) -> None:
         raise GseError(status, msg)
 
 
+def ptr_f64(obj: Any, n: int, name: str):
+    """Address of a per-atom float64 array (numpy or torch) holding at least n
+    contiguous values; GseError (invalid argument) for any other dtype, a
+    strided view or a shorter array, where the library would otherwise write
+    or read doubles past its end.  None and raw integer addresses pass
+    through unchecked."""
+    if obj is None or isinstance(obj, int):
+        return obj
+    if hasattr(obj, "data_ptr"):  # torch.Tensor
+        import torch
+        ok = obj.dtype == torch.float64 and obj.is_contiguous() and obj.numel() >= n
+    elif hasattr(obj, "ctypes") and hasattr(obj, "dtype"):  # numpy.ndarray
+        import numpy as np
+        ok = obj.dtype == np.float64 and obj.flags.c_contiguous and obj.size >= n
+    else:
+        return ptr(obj)
+    if not ok:
+        raise GseError(1, f"{name} must hold at least {n} contiguous float64 values "
+                          f"(got {getattr(obj, 'dtype', type(obj))}, "
+                          f"{getattr(obj, 'size', None) if not hasattr(obj, 'numel') else obj.numel()} values)")
+    return ptr(obj)
+
+
 def ptr(obj: Any):
     """Address of a numpy array, a torch tensor, a ctypes object or an int."""
     if obj is None:

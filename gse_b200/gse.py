@@ -26,7 +26,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import GseError, check, ptr
+from ._lib import GseError, check, ptr, ptr_f64
 
 CCELEC = 332.0716
 
@@ -99,16 +99,19 @@ class Context:
         return e.value
 
     def interpolate_force(self, n, xyzq, fx, fy, fz):
-        check(self._L.gse_interpolate_force(self.h, int(n), ptr(xyzq), ptr(fx), ptr(fy), ptr(fz)))
+        n = int(n)
+        check(self._L.gse_interpolate_force(self.h, n, ptr(xyzq), ptr_f64(fx, n, "fx"),
+                                            ptr_f64(fy, n, "fy"), ptr_f64(fz, n, "fz")))
 
     def forward(self, n, xyzq, fx=None, fy=None, fz=None, energy_out=None) -> Optional[float]:
+        n = int(n)
+        f = [ptr_f64(a, n, k) for a, k in ((fx, "fx"), (fy, "fy"), (fz, "fz"))]
         if energy_out is not None:
-            check(self._L.gse_forward(self.h, int(n), ptr(xyzq), ptr(energy_out), ptr(fx), ptr(fy),
-                                      ptr(fz)))
+            check(self._L.gse_forward(self.h, n, ptr(xyzq), ptr_f64(energy_out, 1, "energy_out"),
+                                      *f))
             return None
         e = ctypes.c_double()
-        check(self._L.gse_forward(self.h, int(n), ptr(xyzq), ctypes.addressof(e), ptr(fx),
-                                  ptr(fy), ptr(fz)))
+        check(self._L.gse_forward(self.h, n, ptr(xyzq), ctypes.addressof(e), *f))
         return e.value
 
     def get_grid(self, which, out=None):
@@ -128,8 +131,10 @@ class Context:
                                        int(bool(normalize)), ptr(rho_out)))
 
     def gauss_interpolate(self, sigma, rcut, n, xyzq, boxx, boxy, boxz, phi, fx, fy, fz):
-        check(self._L.gse_gauss_interpolate(self.h, sigma, rcut, int(n), ptr(xyzq), boxx, boxy,
-                                            boxz, ptr(phi), ptr(fx), ptr(fy), ptr(fz)))
+        n = int(n)
+        check(self._L.gse_gauss_interpolate(self.h, sigma, rcut, n, ptr(xyzq), boxx, boxy,
+                                            boxz, ptr(phi), ptr_f64(fx, n, "fx"),
+                                            ptr_f64(fy, n, "fy"), ptr_f64(fz, n, "fz")))
 
     def green_mul(self, sigma, boxx, boxy, boxz, rho_k):
         check(self._L.gse_green_mul(self.h, sigma, boxx, boxy, boxz, ptr(rho_k)))
@@ -139,7 +144,9 @@ class Context:
 
     def interpolate_field(self, n, xyzq, ex, ey, ez):
         """Electric field at the atoms (force per unit charge) from phiM."""
-        check(self._L.gse_interpolate_field(self.h, int(n), ptr(xyzq), ptr(ex), ptr(ey), ptr(ez)))
+        n = int(n)
+        check(self._L.gse_interpolate_field(self.h, n, ptr(xyzq), ptr_f64(ex, n, "ex"),
+                                            ptr_f64(ey, n, "ey"), ptr_f64(ez, n, "ez")))
 
     def virial(self, out=None):
         """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS."""
@@ -163,8 +170,10 @@ class Context:
 
     def adjoint(self, n, xyzq, dLdE, gfx, gfy, gfz, dq, dx, dy, dz):
         """dL/dq and dL/dx for dL/dE = dLdE and dL/dF = (gfx, gfy, gfz) (may be None)."""
-        check(self._L.gse_adjoint(self.h, int(n), ptr(xyzq), float(dLdE), ptr(gfx), ptr(gfy),
-                                  ptr(gfz), ptr(dq), ptr(dx), ptr(dy), ptr(dz)))
+        n = int(n)
+        g = [ptr_f64(v, n, k) for v, k in ((gfx, "gfx"), (gfy, "gfy"), (gfz, "gfz"))]
+        o = [ptr_f64(v, n, k) for v, k in ((dq, "dq"), (dx, "dx"), (dy, "dy"), (dz, "dz"))]
+        check(self._L.gse_adjoint(self.h, n, ptr(xyzq), float(dLdE), *g, *o))
 
     def paths(self) -> int:
         """Bits of the implementation paths taken (_lib.PATH_*)."""
