@@ -6,7 +6,8 @@
 //
 //   xyzq_t<T>                  TypesGSE.h:19-22
 //   CpuGrid<T>                 Grid.h:12-55, CpuGrid.h:17-108 (host container)
-//   CpuGaussCharge<AT,CT>      CpuGaussCharge.h:11-49
+//   CpuGaussCharge<AT,CT>      CpuGaussCharge.h:11-49 (<double,double>, <double,float>,
+//                              <float,float>)
 //   CpuGreensFunc<T>           CpuGreensFunc.h:10-19
 //   CpuGreensFuncGSE<T>        CpuGreensFuncGSE.h:10-19
 //   CpuFFTSolver<T>            CpuFFTSolver.h:12-42
@@ -171,7 +172,12 @@ class CpuGrid {
 // ---------------------------------------------------------------------------
 template <typename AT, typename CT>
 class CpuGaussCharge {
-  static_assert(std::is_same<AT, double>::value, "forces and energies are accumulated in double");
+  // the reference's instances (CpuGaussCharge.cpp:524-526): <double,double>,
+  // <double,float> and <float,float>; with AT = float the forces and the
+  // dipole are accumulated in double on the GPU and rounded to float once
+  static_assert(std::is_same<AT, double>::value ||
+                    (std::is_same<AT, float>::value && std::is_same<CT, float>::value),
+                "instances: <double,double>, <double,float>, <float,float>");
 
  public:
   // The stage calls carry their own sigma, cut-off and box; the context's
@@ -211,8 +217,21 @@ class CpuGaussCharge {
                         const double boxz, const CpuGrid<CT>& phi, AT* forceX, AT* forceY,
                         AT* forceZ) {
     same_size(phi);
-    check(gse_gauss_interpolate(ctx_.get(), sigma, rcut, numCoord, xyzq, boxx, boxy, boxz,
-                                phi.getDataPointer(), forceX, forceY, forceZ));
+    if constexpr (std::is_same<AT, double>::value) {
+      check(gse_gauss_interpolate(ctx_.get(), sigma, rcut, numCoord, xyzq, boxx, boxy, boxz,
+                                  phi.getDataPointer(), forceX, forceY, forceZ));
+    } else {
+      const size_t n = numCoord > 0 ? (size_t)numCoord : 0;
+      std::vector<double> f(3 * n);
+      check(gse_gauss_interpolate(ctx_.get(), sigma, rcut, numCoord, xyzq, boxx, boxy, boxz,
+                                  phi.getDataPointer(), f.data(), f.data() + n,
+                                  f.data() + 2 * n));
+      for (size_t i = 0; i < n; i++) {
+        forceX[i] = (AT)f[i];
+        forceY[i] = (AT)f[n + i];
+        forceZ[i] = (AT)f[2 * n + i];
+      }
+    }
   }
 
   // On-grid Gaussian convolution, rhoS = G(sigma) * rho (CpuGaussCharge.cpp:390-519).

@@ -176,3 +176,51 @@ def test_dropin_ewald_classes(goldens, tmp_path):
     assert rms(np.array(vals["FWR"]), fr) <= 1e-11
     assert abs(vals["EWD"][0][0] - ed) <= 1e-12 * abs(ed)
     assert rms(np.array(vals["FWD"]), fd) <= 1e-12
+
+
+CXX_INSTANCES = r"""
+#include "gse_dropin.h"
+using namespace gse_b200;
+template <typename AT, typename CT>
+int use(int n) {
+  CpuGaussCharge<AT, CT> g(16, 16, 16);
+  std::vector<xyzq_t<CT>> x(n, xyzq_t<CT>{1, 2, 3, 1});
+  CpuGrid<CT> rho(16, 16, 16), phi(16, 16, 16);
+  std::vector<AT> fx(n), fy(n), fz(n);
+  g.spreadChargeToGrid(1.0, 4.0, n, x.data(), 16.0, 16.0, 16.0, rho);
+  g.interpolateForce(1.0, 4.0, n, x.data(), 16.0, 16.0, 16.0, phi, fx.data(), fy.data(), fz.data());
+  AT d[3];
+  g.calcDipoleSum(16.0, 16.0, 16.0, rho, d[0], d[1], d[2]);
+  return g.calcSupportSize(4.0, 16.0, 16.0, 16.0);
+}
+int main() {
+  try {
+    return use<double, double>(3) + use<double, float>(3) + use<float, float>(3) > 0 ? 0 : 1;
+  } catch (const Error& e) {
+    printf("error %d\n", (int)e.status);
+    return 3;
+  }
+}
+"""
+
+
+def test_reference_instances_compile(tmp_path):
+    """CpuGaussCharge<double,double>, <double,float> and <float,float> (the
+    reference's instances, CpuGaussCharge.cpp:524-526) compile against the
+    drop-in header and link; without a GPU the first call reports the
+    library's error status instead of computing."""
+    import torch
+    from gse_b200 import build
+    lib = build.build_lib()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "instances.cpp"
+    src.write_text(CXX_INSTANCES)
+    exe = tmp_path / "instances"
+    libdir = os.path.dirname(lib)
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(root, "include"),
+                    "-I", os.path.join(root, "gse_b200", "cxx"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lgse_b200", "-Wl,-rpath," + libdir], check=True)
+    if torch.cuda.is_available():
+        return
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 3 and out.stdout.startswith("error "), (out.returncode, out.stdout)
