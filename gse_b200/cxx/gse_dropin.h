@@ -187,20 +187,30 @@ class CpuGaussCharge {
         ctx_(sizeX, sizeY, sizeZ, 1.0, 0.4, 3.0, 3.0, sizeX, sizeY, sizeZ, 332.0716,
              precision_of<CT>()) {}
 
-  // Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56).
+  // Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56): the
+  // spacings and rcut^2 rounded to CT, the distances formed and summed in CT.
   int calcSupportSize(const double rcut, const double boxx, const double boxy,
                       const double boxz) const {
-    const double h[3] = {boxx / sizeX, boxy / sizeY, boxz / sizeZ};
+    const double hd[3] = {boxx / sizeX, boxy / sizeY, boxz / sizeZ};
     int n[3];
-    for (int d = 0; d < 3; d++) n[d] = (int)std::ceil(rcut / h[d]);
+    CT h[3];
+    for (int d = 0; d < 3; d++) {
+      n[d] = (int)std::ceil(rcut / hd[d]);
+      h[d] = (CT)hd[d];
+    }
+    const CT rcut2 = (CT)(rcut * rcut);
     int cnt = 0;
-    for (int tz = -n[2]; tz <= n[2]; tz++)
-      for (int ty = -n[1]; ty <= n[1]; ty++)
+    for (int tz = -n[2]; tz <= n[2]; tz++) {
+      const CT dz = ((CT)(std::abs(tz) - 1)) * h[2];
+      for (int ty = -n[1]; ty <= n[1]; ty++) {
+        const CT dy = ((CT)(std::abs(ty) - 1)) * h[1];
         for (int tx = -n[0]; tx <= n[0]; tx++) {
-          const double dx = (std::abs(tx) - 1) * h[0], dy = (std::abs(ty) - 1) * h[1],
-                       dz = (std::abs(tz) - 1) * h[2];
-          if (dx * dx + dy * dy + dz * dz < rcut * rcut) cnt++;
+          const CT dx = ((CT)(std::abs(tx) - 1)) * h[0];
+          const CT r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 < rcut2) cnt++;
         }
+      }
+    }
     return cnt;
   }
 

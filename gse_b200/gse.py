@@ -359,12 +359,16 @@ class CpuGaussCharge:
         return float(dip[0]), float(dip[1]), float(dip[2])
 
     def calcSupportSize(self, rcut, boxx, boxy, boxz):
-        """Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56)."""
-        h = np.array([boxx / self.sizeX, boxy / self.sizeY, boxz / self.sizeZ])
-        n = np.ceil(rcut / h).astype(int)
-        t = [(np.abs(np.arange(-k, k + 1)) - 1) * hh for k, hh in zip(n, h)]
-        r2 = t[0][None, None, :] ** 2 + t[1][None, :, None] ** 2 + t[2][:, None, None] ** 2
-        return int(np.count_nonzero(r2 < rcut * rcut))
+        """Number of offsets with r^2 < rcut^2 (CpuGaussCharge.cpp:28-56): the
+        spacings and rcut^2 rounded to the calculation type, the distances
+        formed and summed in it, in the reference's order."""
+        ct = np.dtype(getattr(self, "dtype", np.float64)).type
+        hd = [boxx / self.sizeX, boxy / self.sizeY, boxz / self.sizeZ]
+        n = [int(np.ceil(rcut / v)) for v in hd]
+        t = [(np.abs(np.arange(-k, k + 1)) - 1).astype(ct) * ct(v) for k, v in zip(n, hd)]
+        dx, dy, dz = t[0][None, None, :], t[1][None, :, None], t[2][:, None, None]
+        r2 = (dx * dx + dy * dy) + dz * dz
+        return int(np.count_nonzero(r2 < ct(rcut * rcut)))
 
 
 class CpuGreensFunc:

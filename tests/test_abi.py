@@ -142,3 +142,13 @@ def test_support_size_matches_reference_formula():
                 dx, dy, dz = (abs(tx) - 1) * h, (abs(ty) - 1) * h, (abs(tz) - 1) * h
                 cnt += (dx * dx + dy * dy + dz * dz) < rcut * rcut
     assert g.calcSupportSize(rcut, 20.0, 20.0, 20.0) == cnt
+    # the mixed instance forms the distances in float32, as CT = float does
+    g.dtype = np.float32
+    rc2 = np.float32(rcut * rcut)
+    cnt32 = 0
+    for tz in range(-n, n + 1):
+        for ty in range(-n, n + 1):
+            for tx in range(-n, n + 1):
+                dx, dy, dz = (np.float32(abs(t) - 1) * np.float32(h) for t in (tx, ty, tz))
+                cnt32 += (dx * dx + dy * dy) + dz * dz < rc2
+    assert g.calcSupportSize(rcut, 20.0, 20.0, 20.0) == cnt32
