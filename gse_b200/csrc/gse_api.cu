@@ -324,7 +324,9 @@ gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT
   StageTimer tm(c, GSE_STAGE_BIN);
   BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax,
                c->d_badmap};
-  c->launches += n > 0 ? 6 : 3;
+  // count, three scan passes, then the placement: one kernel (mixed, any
+  // order within a bin) or two (FP64, stable)
+  c->launches += n > 0 ? (c->fp64 ? 6 : 5) : 3;
   CU(launch_bin_sorted<CT>((const V*)dx, n, c->bl, s.inv_h[0], s.inv_h[1], s.inv_h[2], w,
                            (V*)c->d_sorted, c->d_perm, c->stream));
   return GSE_OK;
