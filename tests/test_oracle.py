@@ -173,3 +173,20 @@ def test_reference_test48k_golden(oracle_lib, ref48k):
     assert E == float(z["E"])
     assert np.array_equal(F[z["idx"]], z["F"])
     assert (F * F).sum() == float(z["F2sum"])
+
+
+@pytest.mark.parametrize("kappa,lam", [(0.3, 2.5), (0.45, 3.5), (0.25, 4.0)])
+def test_restatement_matches_reference_at_other_splittings(oracle_lib, kappa, lam):
+    """The reference drivers always use kappa 0.4 and lambda 3 (cpu_gse.cpp:424-426);
+    the classes take any kappa < 0.5 and lambda.  The restatement equals the
+    compiled reference bit for bit away from those values too."""
+    if not oracle_lib.have_reference():
+        pytest.skip("reference build not present")
+    from gse_b200 import workloads as W
+    x = W.triplets(300, 15.0, 5).astype(np.float64) * np.array([1.0, 1.1, 1.2, 1.0])
+    M, box = (16, 18, 20), (15.0, 16.5, 18.0)
+    e1, f1 = oracle_lib.gsek_forward(M, box, 2.0, x, kappa=kappa, lambda_sigma1=lam)
+    e2, f2 = oracle_lib.ref_gsek_forward(M, box, 2.0, x, kappa=kappa, lambda_sigma=lam,
+                                         lambda_sigma1=lam)
+    assert e1 == e2
+    assert np.array_equal(f1, f2)
