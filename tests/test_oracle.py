@@ -98,10 +98,13 @@ def test_ewald_recip_restatement_matches_reference(oracle_lib):
     if not oracle_lib.have_reference():
         pytest.skip("reference build not present")
     from gse_b200 import workloads as W
-    for xyzq, L, kcut in [(W.reference_pair(1.0), 20.0, 32), (W.random_charges(40, 12.0, 2), 12.0, 9),
-                          (W.triplets(60, 10.0, 5).astype(np.float64), 10.0, 11)]:
-        e1, f1 = oracle_lib.ewald_recip(2.0, kcut, (L, L, L), xyzq)
-        e2, f2 = oracle_lib.ref_ewald_recip(2.0, kcut, (L, L, L), xyzq)
+    ortho = W.triplets(60, 10.0, 7).astype(np.float64) * np.array([1.0, 1.3, 0.8, 1.0])
+    for xyzq, box, kcut in [(W.reference_pair(1.0), (20.0,) * 3, 32),
+                            (W.random_charges(40, 12.0, 2), (12.0,) * 3, 9),
+                            (W.triplets(60, 10.0, 5).astype(np.float64), (10.0,) * 3, 11),
+                            (ortho, (10.0, 13.0, 8.0), 10)]:
+        e1, f1 = oracle_lib.ewald_recip(2.0, kcut, box, xyzq)
+        e2, f2 = oracle_lib.ref_ewald_recip(2.0, kcut, box, xyzq)
         assert abs(e1 - e2) <= 1e-12 * abs(e2)
         assert oracle_lib.force_rms(f1, f2) <= 1e-12
 
