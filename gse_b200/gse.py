@@ -7,6 +7,9 @@ Class and method names, argument order and meaning follow ap-hynninen/GSE:
   CpuGreensFuncGSE<T>   CpuGreensFuncGSE.h:10-19
   CpuFFTSolver<T>       CpuFFTSolver.h:12-42
   CpuGSE<AT,CT>/CpuGSEk CpuGSE.h:19-68, CpuGSEk.h:19-37
+  CpuEwaldRecip         CpuEwaldRecip.h:11-44 (calcForceEnergy; FP64)
+  CpuEwaldDirect        CpuEwaldDirect.h:10-44 (FP64)
+  Erms, loadArray, saveForce, readForce   cpu_gse.cpp:128-196 (text I/O)
 
 The template parameters become a ``precision`` argument: "fp64" is
 <double,double>; "mixed" is <double,float> (FP32 xyzq and grids, double
