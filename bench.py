@@ -156,7 +156,30 @@ def reference_cpu(xyzq64: np.ndarray, box: float, M: int, sigma: float, budget_s
         R.ref_gsek_destroy(h)
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": len(times) / sum(times), "evals": len(times), "seconds": sum(times),
-            "threads": threads, "energy": float(e[0])}
+            "threads": threads, "energy": float(e[0]), "forces": np.stack([fx, fy, fz], axis=1)}
+
+
+def parity_vs_reference(F64, E64, Fmx, Emx, Fref, Eref, source):
+    """Both GPU forms against the reference's CpuGSEk<double,double> on the same
+    box: relative force RMS (Erms, cpu_gse.cpp:131-146) and relative energy."""
+    def one(F, E):
+        d = F - Fref
+        return {"force_rms": float(np.sqrt((d * d).sum() / (Fref * Fref).sum())),
+                "energy_rel": abs(E - Eref) / abs(Eref), "source": source}
+    return {"fp64": one(F64, E64), "mixed": one(Fmx, Emx)}
+
+
+def parity_vs_golden(F64, E64, Fmx, Emx):
+    """Without the reference build in this run: the committed golden of the
+    same box (tests/golden/make_ref_configs.py), 4096 sampled forces."""
+    path = os.path.join(ROOT, "tests", "golden", f"ref_{WORKLOAD}.npz")
+    if not os.path.exists(path):
+        return None
+    z = np.load(path)
+    idx = z["idx"]
+    src = f"the reference's CpuGSEk<double,double> forces of {len(idx)} sampled atoms (golden)"
+    return {k: dict(v, source=src) for k, v in
+            parity_vs_reference(F64[idx], E64, Fmx[idx], Emx, z["F"], float(z["E"]), src).items()}
 
 
 def make_workload():
@@ -174,7 +197,10 @@ def run_reference_arm(args):
                           "unavailable": "oracle/_ref was not built (no reference sources)"}))
         return
     budget = float(os.environ.get("GSE_REF_BUDGET_S", "120"))
-    warm = reference_cpu(xyzq, s.box, s.M, s.sigma, 0.0, max(1, min(args.warmup, 1)))
+    # the W warm-up evaluations the other arm takes (plan creation, first touch
+    # of the grids), within a budget of their own
+    warm = reference_cpu(xyzq, s.box, s.M, s.sigma, 60.0, max(1, args.warmup))
+    n_warm = warm["evals"]
     del warm
     r = reference_cpu(xyzq, s.box, s.M, s.sigma, budget, max(1, args.steps))
     sample = (f"{r['evals']} full evaluations of the {s.n}-charge box (of {args.steps} requested "
@@ -183,7 +209,7 @@ def run_reference_arm(args):
               f"project FFTW-API shim on {r['threads']} OpenMP threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
-        "steps": r["evals"], "warmup": 1, "ms_per_step": 1000.0 * r["seconds"] / r["evals"],
+        "steps": r["evals"], "warmup": n_warm, "ms_per_step": 1000.0 * r["seconds"] / r["evals"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded water-like triplets, 87,381 rigid 3-site molecules)",
         "config": {"workload": WORKLOAD, "n_charges": s.n, "grid": s.M, "box": s.box,
@@ -524,11 +550,15 @@ def main():
                     if len(parts) == 3 and parts[0] == dom and parts[1] == prec:
                         traffic = int(parts[2])
         cpu = None
+        ref_parity = None
         if world == 1 and not args.no_cpu_baseline:
             try:
                 import oracle
                 if oracle.have_reference():
                     r = reference_cpu(s.xyzq.astype(np.float64), s.box, s.M, s.sigma, 12.0, 3)
+                    ref_parity = parity_vs_reference(F64, E64, Fmx, Emx, r["forces"], r["energy"],
+                                                     "CpuGSEk<double,double> forces of every "
+                                                     "atom, computed in this run")
                     cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"],
                            "kind": "reference",
                            "sample": f"{r['evals']} full evaluations of the same {n}-charge box "
@@ -538,6 +568,8 @@ def main():
             except Exception as exc:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                        "sample": f"failed: {exc}"}
+        if ref_parity is None:
+            ref_parity = parity_vs_golden(F64, E64, Fmx, Emx)
         grid_ops = None
         if not args.no_batch:
             try:
@@ -567,6 +599,8 @@ def main():
             "eval_ms_percentiles": {k: round(v, 4) for k, v in pct.items()},
             f"{other}_value": value2,
             "mixed_vs_fp64": {"force_rms": force_rms, "energy_rel": energy_rel},
+            "fp64_vs_reference": ref_parity and ref_parity["fp64"],
+            "mixed_vs_reference": ref_parity and ref_parity["mixed"],
             "vs_ewald": accuracy,
             "energy": E_main,
             "batch": batch,

@@ -16,7 +16,7 @@ GSE_OK = 0
 STATUS_NAMES = {
     0: "GSE_OK", 1: "GSE_ERR_INVALID_ARG", 2: "GSE_ERR_STENCIL_TOO_LARGE", 3: "GSE_ERR_CUDA",
     4: "GSE_ERR_OOM", 5: "GSE_ERR_TIMEOUT", 6: "GSE_ERR_NOT_READY", 7: "GSE_ERR_UNSUPPORTED",
-    8: "GSE_ERR_NONFINITE",
+    8: "GSE_ERR_NONFINITE", 9: "GSE_ERR_RANGE",
 }
 PRECISION = {"fp64": 0, "mixed": 1}
 PATH_TILED, PATH_GREEN_IN_FFT, PATH_GRAPH = 1, 2, 4
@@ -162,6 +162,35 @@ def ptr_f64(obj: Any, n: int, name: str):
         raise GseError(1, f"{name} must hold at least {n} contiguous float64 values "
                           f"(got {getattr(obj, 'dtype', type(obj))}, "
                           f"{getattr(obj, 'size', None) if not hasattr(obj, 'numel') else obj.numel()} values)")
+    return ptr(obj)
+
+
+def ptr_records(obj: Any, n: int, itemsize: int, name: str = "xyzq"):
+    """Address of n position records {x, y, z, q} of the calculation type
+    (itemsize 4: float32, 8: float64), as numpy or torch.  GseError (invalid
+    argument) for another dtype, a strided view, fewer than 4n values or -- for
+    CUDA tensors, which the kernels read in place as float4/double4 records --
+    a start that is not 4*itemsize-byte aligned.  None and raw integer
+    addresses pass through unchecked (the library checks device addresses
+    itself)."""
+    if obj is None or isinstance(obj, int):
+        return obj
+    if hasattr(obj, "data_ptr"):  # torch.Tensor
+        import torch
+        want = torch.float32 if itemsize == 4 else torch.float64
+        ok = obj.dtype == want and obj.is_contiguous() and obj.numel() >= 4 * n
+        if ok and getattr(obj, "is_cuda", False) and obj.data_ptr() % (4 * itemsize) != 0:
+            raise GseError(1, f"{name} is device memory that is not {4 * itemsize}-byte aligned "
+                              "(its records are read as 16/32-byte vectors)")
+    elif hasattr(obj, "ctypes") and hasattr(obj, "dtype"):  # numpy.ndarray
+        import numpy as np
+        want = np.float32 if itemsize == 4 else np.float64
+        ok = obj.dtype == want and obj.flags.c_contiguous and obj.size >= 4 * n
+    else:
+        return ptr(obj)
+    if not ok:
+        raise GseError(1, f"{name} must hold at least {n} contiguous {{x, y, z, q}} records of "
+                          f"float{8 * itemsize} (got {getattr(obj, 'dtype', type(obj))})")
     return ptr(obj)
 
 

@@ -95,7 +95,45 @@ bool is_pinned_host(const void* p) {
 
 namespace gse {
 gse_status_t set_error(gse_status_t s, const char* msg) { return fail(s, "%s", msg); }
+
+// A caller's pointer that a kernel may read or write in place.  NULL and host
+// memory pass: host memory only reaches the GPU through cudaMemcpyAsync into
+// the library's own buffers.  Device memory must belong to `device` (a kernel
+// of this context cannot address another GPU's allocation) and start on an
+// `align`-byte boundary: the kernels read position records as float4/double4,
+// forces and gradients as doubles and spectra as float4/double2 vectors, and a
+// misaligned vector access faults.  The check runs on the host, before any
+// work of the call is queued.
+gse_status_t check_ptr(const void* p, int device, size_t align, const char* what) {
+  if (!p) return GSE_OK;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return GSE_OK;
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return GSE_OK;
+  if (a.type == cudaMemoryTypeDevice && a.device != device)
+    return fail(GSE_ERR_INVALID_ARG, "%s is memory of device %d, the call runs on device %d", what,
+                a.device, device);
+  if (align > 1 && (uintptr_t)p % align != 0)
+    return fail(GSE_ERR_INVALID_ARG, "%s is device memory that is not %zu-byte aligned", what,
+                align);
+  return GSE_OK;
+}
 }  // namespace gse
+
+namespace {
+using gse::check_ptr;
+
+// The three per-atom double arrays of a force, field or gradient output.
+gse_status_t check_xyz(int device, const double* x, const double* y, const double* z,
+                       const char* what) {
+  TRY(check_ptr(x, device, sizeof(double), what));
+  TRY(check_ptr(y, device, sizeof(double), what));
+  TRY(check_ptr(z, device, sizeof(double), what));
+  return GSE_OK;
+}
+}  // namespace
 
 struct gse_context {
   gse_params_t p;
@@ -300,6 +338,7 @@ gse_status_t ensure_atoms(gse_context_t* c, int n) {
 gse_status_t stage_atoms(gse_context_t* c, int n, const void* xyzq, const void** dptr) {
   if (n < 0) return fail(GSE_ERR_INVALID_ARG, "negative atom count");
   if (n > 0 && !xyzq) return fail(GSE_ERR_INVALID_ARG, "NULL xyzq");
+  TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
   TRY(ensure_atoms(c, n > 0 ? n : 1));
   if (n == 0) {
     *dptr = c->d_xyzq;
@@ -590,11 +629,18 @@ gse_status_t copy_out(gse_context_t* c, void* dst, const void* src, size_t bytes
   return GSE_OK;
 }
 
-// After a synchronisation: report (once) non-finite inputs seen since the
-// last report.
+// After a synchronisation: report (once) non-finite inputs or a charge
+// density beyond the mixed form's fixed-point range seen since the last
+// report.
 gse_status_t check_finite(gse_context_t* c) {
   if (c->h_bad && *c->h_bad) {
+    const int f = *c->h_bad;
     *c->h_bad = 0;
+    if (f == kFlagRange)
+      return fail(GSE_ERR_RANGE,
+                  "the charge in one 16^3-cell brick exceeds the mixed form's fixed-point range "
+                  "(sum of |q| (2 pi sigma1^2)^-1.5 over the brick above about 2^19, or one "
+                  "charge's above 2^11); use the FP64 form");
     return fail(GSE_ERR_NONFINITE, "a position or charge is NaN or infinite");
   }
   return GSE_OK;
@@ -727,6 +773,7 @@ const char* gse_status_string(gse_status_t s) {
     case GSE_ERR_NOT_READY: return "GSE_ERR_NOT_READY";
     case GSE_ERR_UNSUPPORTED: return "GSE_ERR_UNSUPPORTED";
     case GSE_ERR_NONFINITE: return "GSE_ERR_NONFINITE";
+    case GSE_ERR_RANGE: return "GSE_ERR_RANGE";
   }
   return "GSE_ERR_UNKNOWN";
 }
@@ -830,6 +877,7 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
     *hb = 0;
     c->h_bad = hb;
     CUC(cudaHostGetDevicePointer((void**)&c->d_badmap, hb, 0));
+    c->bl.flags = c->d_badmap;
   }
 #undef CUC
   if (cufftPlan3d(&c->plan_f, p.size_z, p.size_y, p.size_x, c->fp64 ? CUFFT_D2Z : CUFFT_R2C) !=
@@ -943,6 +991,7 @@ gse_status_t gse_solve_poisson(gse_context_t* c) {
 gse_status_t gse_calculate_energy(gse_context_t* c, double* energy) {
   TRY(check_ctx(c));
   if (!energy) return fail(GSE_ERR_INVALID_ARG, "NULL energy");
+  TRY(check_ptr(energy, c->p.device, 1, "energy"));
   if (!c->rho_valid || !c->phi_valid)
     return fail(GSE_ERR_NOT_READY, "calculateEnergy needs rhoS and phiM");
   if (!c->energy_valid) {
@@ -965,6 +1014,7 @@ gse_status_t gse_interpolate_force(gse_context_t* c, int n, const void* xyzq, do
                                    double* fy, double* fz) {
   TRY(check_ctx(c));
   if (n > 0 && (!fx || !fy || !fz)) return fail(GSE_ERR_INVALID_ARG, "NULL force array");
+  TRY(check_xyz(c->p.device, fx, fy, fz, "force array"));
   if (!c->phi_valid) return fail(GSE_ERR_NOT_READY, "interpolateForce before solvePoisson");
   const void* dx;
   TRY(stage_atoms(c, n, xyzq, &dx));
@@ -982,6 +1032,7 @@ gse_status_t gse_interpolate_field(gse_context_t* c, int n, const void* xyzq, do
                                    double* ey, double* ez) {
   TRY(check_ctx(c));
   if (n > 0 && (!ex || !ey || !ez)) return fail(GSE_ERR_INVALID_ARG, "NULL field array");
+  TRY(check_xyz(c->p.device, ex, ey, ez, "field array"));
   if (!c->phi_valid) return fail(GSE_ERR_NOT_READY, "field before solvePoisson");
   const void* dx;
   TRY(stage_atoms(c, n, xyzq, &dx));
@@ -1033,6 +1084,9 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
 gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
                          double* fy, double* fz) {
   TRY(check_ctx(c));
+  TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
+  TRY(check_ptr(energy, c->p.device, 1, "energy"));
+  TRY(check_xyz(c->p.device, fx, fy, fz, "force array"));
   // Graph replay applies to calls whose positions and forces are device or
   // page-locked host memory (the copies to and from the host then sit in the
   // graph), on a stream that can be captured, without stage timing; the key
@@ -1126,6 +1180,7 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
 gse_status_t gse_get_grid(gse_context_t* c, int which, void* out) {
   TRY(check_ctx(c));
   if (!out) return fail(GSE_ERR_INVALID_ARG, "NULL out");
+  TRY(check_ptr(out, c->p.device, 1, "out"));
   const void* src;
   if (which == GSE_GRID_RHO) {
     if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "rhoS not computed");
@@ -1144,6 +1199,7 @@ gse_status_t gse_get_grid(gse_context_t* c, int which, void* out) {
 gse_status_t gse_set_grid(gse_context_t* c, int which, const void* in) {
   TRY(check_ctx(c));
   if (!in) return fail(GSE_ERR_INVALID_ARG, "NULL in");
+  TRY(check_ptr(in, c->p.device, 1, "in"));
   void* dst;
   if (which == GSE_GRID_RHO)
     dst = c->d_rho;
@@ -1168,6 +1224,8 @@ gse_status_t gse_gauss_spread(gse_context_t* c, double sigma, double rcut, int n
                               const void* xyzq, double bx, double by, double bz, int normalize,
                               void* rho_out) {
   TRY(check_ctx(c));
+  TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
+  TRY(check_ptr(rho_out, c->p.device, 1, "rho_out"));
   const double box[3] = {bx, by, bz};
   TRY(check_stencil(c, box, sigma, rcut));
   const void* dx;
@@ -1187,6 +1245,9 @@ gse_status_t gse_gauss_interpolate(gse_context_t* c, double sigma, double rcut, 
   TRY(check_ctx(c));
   if (!phi) return fail(GSE_ERR_INVALID_ARG, "NULL phi");
   if (n > 0 && (!fx || !fy || !fz)) return fail(GSE_ERR_INVALID_ARG, "NULL force array");
+  TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
+  TRY(check_ptr(phi, c->p.device, c->ct, "phi"));
+  TRY(check_xyz(c->p.device, fx, fy, fz, "force array"));
   const double box[3] = {bx, by, bz};
   TRY(check_stencil(c, box, sigma, rcut));
   const void* dphi = phi;
@@ -1210,6 +1271,7 @@ gse_status_t gse_green_mul(gse_context_t* c, double sigma, double bx, double by,
                            void* rho_k) {
   TRY(check_ctx(c));
   if (!rho_k) return fail(GSE_ERR_INVALID_ARG, "NULL rho_k");
+  TRY(check_ptr(rho_k, c->p.device, 16, "rho_k"));
   if (!(sigma >= 0.0) || !(bx > 0 && by > 0 && bz > 0))
     return fail(GSE_ERR_INVALID_ARG, "bad sigma or box");
   const bool dev = is_device_ptr(rho_k);
@@ -1232,6 +1294,8 @@ gse_status_t gse_fft_solve(gse_context_t* c, double sigma, double bx, double by,
                            const void* rho, void* phi) {
   TRY(check_ctx(c));
   if (!rho || !phi) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  TRY(check_ptr(rho, c->p.device, 16, "rho"));
+  TRY(check_ptr(phi, c->p.device, 16, "phi"));
   if (!(sigma >= 0.0) || !(bx > 0 && by > 0 && bz > 0))
     return fail(GSE_ERR_INVALID_ARG, "bad sigma or box");
   const size_t bytes = c->size * c->ct;
@@ -1257,6 +1321,8 @@ gse_status_t gse_gauss_spread_on_grid(gse_context_t* c, double sigma, double rcu
                                       double by, double bz, const void* rho, void* rho_s) {
   TRY(check_ctx(c));
   if (!rho || !rho_s) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  TRY(check_ptr(rho, c->p.device, c->ct, "rho"));
+  TRY(check_ptr(rho_s, c->p.device, c->ct, "rho_s"));
   const double box[3] = {bx, by, bz};
   TRY(check_stencil(c, box, sigma, rcut));
   const size_t bytes = c->size * c->ct;
@@ -1290,6 +1356,10 @@ gse_status_t gse_gauss_efield_on_grid(gse_context_t* c, double bx, double by, do
                                       const void* phi, void* ex, void* ey, void* ez) {
   TRY(check_ctx(c));
   if (!phi || !ex || !ey || !ez) return fail(GSE_ERR_INVALID_ARG, "NULL grid");
+  TRY(check_ptr(phi, c->p.device, c->ct, "phi"));
+  TRY(check_ptr(ex, c->p.device, c->ct, "ex"));
+  TRY(check_ptr(ey, c->p.device, c->ct, "ey"));
+  TRY(check_ptr(ez, c->p.device, c->ct, "ez"));
   if (!(bx > 0 && by > 0 && bz > 0) || !std::isfinite(bx) || !std::isfinite(by) ||
       !std::isfinite(bz))
     return fail(GSE_ERR_INVALID_ARG, "box lengths must be positive and finite");
@@ -1340,6 +1410,8 @@ gse_status_t gse_gauss_dipole_sum(gse_context_t* c, double bx, double by, double
                                   const void* rho, double* dip) {
   TRY(check_ctx(c));
   if (!rho || !dip) return fail(GSE_ERR_INVALID_ARG, "NULL argument");
+  TRY(check_ptr(rho, c->p.device, c->ct, "rho"));
+  TRY(check_ptr(dip, c->p.device, 1, "dip"));
   if (!(bx > 0 && by > 0 && bz > 0) || !std::isfinite(bx) || !std::isfinite(by) ||
       !std::isfinite(bz))
     return fail(GSE_ERR_INVALID_ARG, "box lengths must be positive and finite");
@@ -1370,6 +1442,7 @@ gse_status_t gse_gauss_dipole_sum(gse_context_t* c, double bx, double by, double
 gse_status_t gse_virial(gse_context_t* c, double* virial) {
   TRY(check_ctx(c));
   if (!virial) return fail(GSE_ERR_INVALID_ARG, "NULL virial");
+  TRY(check_ptr(virial, c->p.device, 1, "virial"));
   if (!c->rho_valid) return fail(GSE_ERR_NOT_READY, "virial needs rhoS (spread or forward first)");
   if (c->fixed_pending) {
     CU(launch_grid64_to_real(c->d_fixed, c->size, (float*)c->d_rho, c->stream));
@@ -1461,6 +1534,10 @@ gse_status_t gse_adjoint(gse_context_t* c, int n, const void* xyzq, double dLdE,
   const bool have_g = gfx || gfy || gfz;
   if (have_g && !(gfx && gfy && gfz))
     return fail(GSE_ERR_INVALID_ARG, "force gradients: give all three components or none");
+  TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
+  TRY(check_xyz(c->p.device, gfx, gfy, gfz, "force gradient"));
+  TRY(check_ptr(dq, c->p.device, sizeof(double), "dq"));
+  TRY(check_xyz(c->p.device, dx, dy, dz, "position gradient"));
   const void* dxq;
   TRY(stage_atoms(c, n, xyzq, &dxq));
   if (n == 0) return finish(c, false);
@@ -1576,6 +1653,8 @@ gse_status_t gse_ewald_recip(int device, void* stream, double sigma, int kcut, d
     return fail(GSE_ERR_INVALID_ARG, "bad Ewald arguments (kcut must lie in [1, 255])");
   const bool want_f = fx || fy || fz;
   if (want_f && !(fx && fy && fz)) return fail(GSE_ERR_INVALID_ARG, "give all force arrays or none");
+  TRY(check_ptr(xyzq, device, sizeof(double4), "xyzq"));
+  TRY(check_xyz(device, fx, fy, fz, "force array"));
   CU(cudaSetDevice(device));
   cudaStream_t st = (cudaStream_t)stream;
   const std::vector<EwRowHost> rows = ewald_rows(kcut);
@@ -1661,6 +1740,8 @@ gse_status_t gse_ewald_direct(int device, void* stream, double sigma, double rcu
     return fail(GSE_ERR_INVALID_ARG, "bad Ewald direct arguments");
   const bool want_f = fx || fy || fz;
   if (want_f && !(fx && fy && fz)) return fail(GSE_ERR_INVALID_ARG, "give all force arrays or none");
+  TRY(check_ptr(xyzq, device, sizeof(double4), "xyzq"));
+  TRY(check_xyz(device, fx, fy, fz, "force array"));
   // exclusions: setupExclusions (CpuEwaldDirect.cpp:31-40) asks for one
   // cumulative end per atom (CpuEwaldDirect.cpp:47) and reads |inb14| - 1
   if (n_iblo14 < 0 || (n_iblo14 > 0 && (n_iblo14 != n || !iblo14)))

@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <map>
 #include <string>
@@ -29,6 +30,7 @@
 
 namespace gse {
 gse_status_t set_error(gse_status_t s, const char* msg);
+gse_status_t check_ptr(const void* p, int device, size_t align, const char* what);
 }
 
 using namespace gse;
@@ -116,6 +118,13 @@ namespace {
     gse_status_t _s = (call);          \
     if (_s != GSE_OK) return _s;       \
   } while (0)
+
+// A caller's buffer that is device memory must be on the batch's device; the
+// batch only copies into and out of its own buffers, so any alignment does.
+gse_status_t check_bufs(int dev, std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs) BTRY(check_ptr(p, dev, 1, "batch input or output"));
+  return GSE_OK;
+}
 
 bool is_dev(const void* p) {
   if (!p) return false;
@@ -496,6 +505,7 @@ gse_status_t gse_batch_info(gse_batch_t* b, gse_batch_info_t* info) {
 gse_status_t gse_batch_forward(gse_batch_t* b, const void* xyzq, double* energies, double* fx,
                                double* fy, double* fz) {
   if (!b) return set_error(GSE_ERR_INVALID_ARG, "NULL batch");
+  BTRY(check_bufs(b->dev, {xyzq, energies, fx, fy, fz}));
   BCU(cudaSetDevice(b->dev));
   cudaStream_t st = b->stream;
   if (xyzq && xyzq != (const void*)b->d_xyzq && b->ntot > 0)
@@ -525,6 +535,7 @@ gse_status_t gse_batch_adjoint(gse_batch_t* b, const void* xyzq, const double* d
                                const double* gfx, const double* gfy, const double* gfz,
                                double* dq, double* dx, double* dy, double* dz) {
   if (!b) return set_error(GSE_ERR_INVALID_ARG, "NULL batch");
+  BTRY(check_bufs(b->dev, {xyzq, dLdE, gfx, gfy, gfz, dq, dx, dy, dz}));
   BCU(cudaSetDevice(b->dev));
   cudaStream_t st = b->stream;
   const long long nt = b->ntot;

@@ -15,7 +15,10 @@
 // fixed size (GSE_NOALLOC_MAX_GRID_POINTS values, 8 MiB).  Every GPU that
 // loads the library holds these 8 MiB until the process exits.  The caller
 // passes the positions and the output grid in device memory.
+#include <cuda.h>
+
 #include <mutex>
+#include <vector>
 
 #include "gse_b200.h"
 #include "gse_internal.cuh"
@@ -23,29 +26,64 @@
 
 namespace gse {
 gse_status_t set_error(gse_status_t s, const char* msg);
+gse_status_t check_ptr(const void* p, int device, size_t align, const char* what);
 }
 
 namespace {
 
 constexpr long long kMaxPoints = GSE_NOALLOC_MAX_GRID_POINTS;
-constexpr int kMaxDevices = 64;
 
 // The scratch grid.  Host code must not use this name as a device address:
 // on the host it is only a stand-in symbol.  Its device address is looked up
 // once per device with cudaGetSymbolAddress.
 static __device__ __align__(256) long long g_noalloc_fixed_grid[kMaxPoints];
 
-long long* g_scratch[kMaxDevices] = {};
+// Resolved addresses of the scratch array, one per (device, CUDA context):
+// every context that loads the library's device code holds its own copy of
+// the array, so a caller that drives its own driver-API contexts gets the
+// copy of the context current at the call.
+struct ScratchAddr {
+  int dev;
+  CUcontext ctx;
+  long long* ptr;
+};
+std::vector<ScratchAddr> g_scratch;
 std::mutex g_scratch_mu;
 
-bool on_device(const void* p, int dev) {
+// The calling thread's current CUDA context (NULL if none is current yet),
+// through the driver entry point the runtime hands out, so that the library
+// does not link the driver library itself.
+CUcontext current_context() {
+  typedef CUresult (*GetCurrentFn)(CUcontext*);
+  static const GetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (GetCurrentFn) nullptr;
+    }
+    return (GetCurrentFn)f;
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+bool is_device_memory(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
+
+#define TRY_NA(call)                  \
+  do {                                \
+    gse_status_t _s = (call);         \
+    if (_s != GSE_OK) return _s;      \
+  } while (0)
 
 }  // namespace
 
@@ -71,29 +109,38 @@ extern "C" gse_status_t gse_spread_mixed_noalloc(int size_x, int size_y, int siz
     if (2 * (int)std::ceil(rcut / (box[d] / (double)M[d])) + 1 > kMaxStencil)
       return set_error(GSE_ERR_STENCIL_TOO_LARGE, "stencil wider than 64 points");
   int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
     cudaGetLastError();
     return set_error(GSE_ERR_CUDA, "no current CUDA device");
   }
-  if (!rho_out || !on_device(rho_out, dev))
+  if (!rho_out || !is_device_memory(rho_out))
     return set_error(GSE_ERR_INVALID_ARG, "rho_out must be device memory of the current device");
-  if (n > 0 && (!xyzq || !on_device(xyzq, dev)))
+  if (n > 0 && (!xyzq || !is_device_memory(xyzq)))
     return set_error(GSE_ERR_INVALID_ARG, "xyzq must be device memory of the current device");
+  // the right device, and the alignment of the kernels' float4 record loads
+  TRY_NA(check_ptr(rho_out, dev, sizeof(float), "rho_out"));
+  TRY_NA(check_ptr(xyzq, dev, sizeof(float4), "xyzq"));
 
-  // First call on this device: resolve the scratch array's device address.
-  long long* scratch;
+  // First call on this device (in this CUDA context): resolve the scratch
+  // array's device address; later calls reuse it.
+  long long* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch[dev]) {
+    CUcontext ctx = current_context();
+    for (const ScratchAddr& a : g_scratch)
+      if (a.dev == dev && a.ctx == ctx && ctx) scratch = a.ptr;
+    if (!scratch) {
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_fixed_grid);
       if (e != cudaSuccess || !p) {
         cudaGetLastError();
         return set_error(GSE_ERR_CUDA, "cudaGetSymbolAddress of the scratch grid failed");
       }
-      g_scratch[dev] = (long long*)p;
+      scratch = (long long*)p;
+      // the lookup makes the runtime's context current if none was
+      ctx = current_context();
+      if (ctx) g_scratch.push_back({dev, ctx, scratch});
     }
-    scratch = g_scratch[dev];
   }
 
   Stencil<float> s = make_stencil<float>(M, box, sigma, rcut, false, false, 1.0);

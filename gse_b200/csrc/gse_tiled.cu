@@ -39,7 +39,7 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const auto a = xyzq[i];
     if (bad && !(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(a.w)))
-      *bad = 1;  // the bin below is still in range (wrap1 of any int)
+      *bad = kFlagNonFinite;  // the bin below is still in range (wrap1 of any int)
     qm = fmaxf(qm, fabsf((float)a.w));
     const int cx = wrap1(centre_cell(a.x, inv_hx), b.M[0]);
     const int cy = wrap1(centre_cell(a.y, inv_hy), b.M[1]);

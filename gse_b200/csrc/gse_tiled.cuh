@@ -40,7 +40,13 @@ struct BinLayout {
   int M[3];
   int nbx;    // ceil(Mx / bin width)
   int bxs;    // log2 of the bin width in x cells
+  // mixed-form scatter: set to kFlagRange when a brick's charge exceeds the
+  // fixed-point range of its int32 tile (may be NULL: not reported)
+  int* flags = nullptr;
 };
+// Values of the context's status flag (host-mapped int, read after a sync).
+constexpr int kFlagNonFinite = 1;  // a position or charge is NaN or infinite
+constexpr int kFlagRange = 2;      // a brick's charge overflows the mixed form's tile range
 
 struct BinScratch {
   int* key;        // [n]

@@ -126,6 +126,12 @@ __device__ __forceinline__ int brick_prologue(const int* __restrict__ start, con
     while (sh > kMinShift && (sum_b * exp2((double)sh) >= 1073741824.0 ||
                               one_b * exp2((double)sh) >= 4194304.0))
       sh--;
+    // even the coarsest scale leaves the tile's int32 sums without headroom:
+    // the brick's result would wrap, so the call reports a range error
+    // (non-finite charges are the binning's report)
+    if ((sum_b * exp2((double)sh) >= 1073741824.0 || one_b * exp2((double)sh) >= 4194304.0) &&
+        isfinite(sum_b) && b.flags)
+      *b.flags = kFlagRange;
     s_shift = sh;
   }
   __syncthreads();

@@ -29,7 +29,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from ._lib import GseError, check, ptr, ptr_f64
+from ._lib import GseError, check, ptr, ptr_f64, ptr_records
 
 CCELEC = 332.0716
 
@@ -77,6 +77,9 @@ class Context:
         except Exception:
             pass
 
+    def _xyzq(self, xyzq, n):
+        return ptr_records(xyzq, int(n), np.dtype(self.dtype).itemsize)
+
     # -- thin wrappers of the C ABI ---------------------------------------
     def set_stream(self, stream_handle: int):
         check(self._L.gse_set_stream(self.h, stream_handle))
@@ -88,7 +91,7 @@ class Context:
         check(self._L.gse_synchronize(self.h))
 
     def spread_charge(self, n, xyzq):
-        check(self._L.gse_spread_charge(self.h, int(n), ptr(xyzq)))
+        check(self._L.gse_spread_charge(self.h, int(n), self._xyzq(xyzq, n)))
 
     def solve_poisson(self):
         check(self._L.gse_solve_poisson(self.h))
@@ -103,18 +106,19 @@ class Context:
 
     def interpolate_force(self, n, xyzq, fx, fy, fz):
         n = int(n)
-        check(self._L.gse_interpolate_force(self.h, n, ptr(xyzq), ptr_f64(fx, n, "fx"),
-                                            ptr_f64(fy, n, "fy"), ptr_f64(fz, n, "fz")))
+        check(self._L.gse_interpolate_force(self.h, n, self._xyzq(xyzq, n),
+                                            ptr_f64(fx, n, "fx"), ptr_f64(fy, n, "fy"),
+                                            ptr_f64(fz, n, "fz")))
 
     def forward(self, n, xyzq, fx=None, fy=None, fz=None, energy_out=None) -> Optional[float]:
         n = int(n)
         f = [ptr_f64(a, n, k) for a, k in ((fx, "fx"), (fy, "fy"), (fz, "fz"))]
         if energy_out is not None:
-            check(self._L.gse_forward(self.h, n, ptr(xyzq), ptr_f64(energy_out, 1, "energy_out"),
-                                      *f))
+            check(self._L.gse_forward(self.h, n, self._xyzq(xyzq, n),
+                                      ptr_f64(energy_out, 1, "energy_out"), *f))
             return None
         e = ctypes.c_double()
-        check(self._L.gse_forward(self.h, n, ptr(xyzq), ctypes.addressof(e), *f))
+        check(self._L.gse_forward(self.h, n, self._xyzq(xyzq, n), ctypes.addressof(e), *f))
         return e.value
 
     def get_grid(self, which, out=None):
@@ -130,13 +134,13 @@ class Context:
         check(self._L.gse_set_grid(self.h, int(which), ptr(a)))
 
     def gauss_spread(self, sigma, rcut, n, xyzq, boxx, boxy, boxz, normalize, rho_out):
-        check(self._L.gse_gauss_spread(self.h, sigma, rcut, int(n), ptr(xyzq), boxx, boxy, boxz,
-                                       int(bool(normalize)), ptr(rho_out)))
+        check(self._L.gse_gauss_spread(self.h, sigma, rcut, int(n), self._xyzq(xyzq, n), boxx,
+                                       boxy, boxz, int(bool(normalize)), ptr(rho_out)))
 
     def gauss_interpolate(self, sigma, rcut, n, xyzq, boxx, boxy, boxz, phi, fx, fy, fz):
         n = int(n)
-        check(self._L.gse_gauss_interpolate(self.h, sigma, rcut, n, ptr(xyzq), boxx, boxy,
-                                            boxz, ptr(phi), ptr_f64(fx, n, "fx"),
+        check(self._L.gse_gauss_interpolate(self.h, sigma, rcut, n, self._xyzq(xyzq, n), boxx,
+                                            boxy, boxz, ptr(phi), ptr_f64(fx, n, "fx"),
                                             ptr_f64(fy, n, "fy"), ptr_f64(fz, n, "fz")))
 
     def green_mul(self, sigma, boxx, boxy, boxz, rho_k):
@@ -148,8 +152,9 @@ class Context:
     def interpolate_field(self, n, xyzq, ex, ey, ez):
         """Electric field at the atoms (force per unit charge) from phiM."""
         n = int(n)
-        check(self._L.gse_interpolate_field(self.h, n, ptr(xyzq), ptr_f64(ex, n, "ex"),
-                                            ptr_f64(ey, n, "ey"), ptr_f64(ez, n, "ez")))
+        check(self._L.gse_interpolate_field(self.h, n, self._xyzq(xyzq, n),
+                                            ptr_f64(ex, n, "ex"), ptr_f64(ey, n, "ey"),
+                                            ptr_f64(ez, n, "ez")))
 
     def virial(self, out=None):
         """Reciprocal-space virial (xx, yy, zz, xy, xz, yz) of the current rhoS."""
@@ -176,7 +181,7 @@ class Context:
         n = int(n)
         g = [ptr_f64(v, n, k) for v, k in ((gfx, "gfx"), (gfy, "gfy"), (gfz, "gfz"))]
         o = [ptr_f64(v, n, k) for v, k in ((dq, "dq"), (dx, "dx"), (dy, "dy"), (dz, "dz"))]
-        check(self._L.gse_adjoint(self.h, n, ptr(xyzq), float(dLdE), *g, *o))
+        check(self._L.gse_adjoint(self.h, n, self._xyzq(xyzq, n), float(dLdE), *g, *o))
 
     def paths(self) -> int:
         """Bits of the implementation paths taken (_lib.PATH_*)."""

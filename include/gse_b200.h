@@ -46,9 +46,14 @@ typedef enum gse_status {
   GSE_ERR_TIMEOUT = 5,           /* a bounded device-side wait gave up */
   GSE_ERR_NOT_READY = 6,         /* stage called out of order (e.g. energy before solve) */
   GSE_ERR_UNSUPPORTED = 7,       /* no GPU, wrong architecture, or feature not built */
-  GSE_ERR_NONFINITE = 8          /* a position or charge is NaN/Inf: returned by the call
+  GSE_ERR_NONFINITE = 8,         /* a position or charge is NaN/Inf: returned by the call
                                     that saw it when its outputs are host memory, else by
                                     the next gse_synchronize (results are then undefined) */
+  GSE_ERR_RANGE = 9              /* mixed form: the charge of one 16^3-cell brick exceeds
+                                    the int32 tile's fixed-point range: sum over the brick
+                                    of |q| (2 pi sigma1^2)^-1.5 above 2^19 (~1.7e7 e at
+                                    sigma1 1.26) or one charge's above 2^11 (~6.5e4 e);
+                                    reported like GSE_ERR_NONFINITE, results undefined */
 } gse_status_t;
 
 typedef enum gse_precision {
@@ -337,15 +342,21 @@ gse_status_t gse_get_paths(gse_context_t* ctx, int* flags);
  * only owner of device memory, or a time-step loop that cannot take the
  * synchronisation of cudaMalloc/cudaFree.
  *
- *  - xyzq (n float4 records) and rho_out (size_x*size_y*size_z floats) must
- *    be device memory of the current device; the call is asynchronous on
- *    `stream` (a cudaStream_t, NULL = legacy default stream).
+ *  - xyzq (n float4 records, 16-byte aligned) and rho_out
+ *    (size_x*size_y*size_z floats) must be device memory of the current
+ *    device; the call is asynchronous on `stream` (a cudaStream_t, NULL =
+ *    legacy default stream).
  *  - The int64 accumulation grid lives in a fixed device array of
  *    GSE_NOALLOC_MAX_GRID_POINTS values (8 MiB) that every GPU loading the
  *    library holds until the process exits; larger grids are rejected with
  *    GSE_ERR_INVALID_ARG.
- *  - The first call on a device looks up that array's device address; make
- *    the first call on each device before any stream capture begins.
+ *  - The first call on a device looks up that array's device address, and
+ *    again the first call in each further CUDA context on it (a caller that
+ *    drives its own driver-API contexts has one copy of the array per
+ *    context); make the first call on each device (and context) before any
+ *    stream capture begins.  A cudaDeviceReset invalidates the address the
+ *    library keeps: do not call this entry point after resetting a device
+ *    that it has already run on.
  *  - All calls on a device share the one array and each call clears it
  *    first, so calls whose work overlaps on the GPU (different streams, no
  *    ordering between them) race and corrupt each other's results. */

@@ -64,3 +64,22 @@ def oracle_lib():
     import oracle
     oracle.build(with_reference=os.path.isdir("/root/reference"))
     return oracle
+
+
+REF_CONFIGS = ("water_262143_L140_M144", "water_48000_L78.4_M80")
+
+
+def load_ref_config(name):
+    """A benchmark-configuration box (make_ref_configs.py): the input
+    regenerated from its seed as float32 [n, 4] (checked against the stored
+    sha256 of its float64 widening) and the compiled reference's outputs."""
+    import hashlib
+    from gse_b200 import workloads as W
+    system = {"water_262143_L140_M144": W.config_water_262k,
+              "water_48000_L78.4_M80": W.config_water_48k}[name]()
+    z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
+    z = {k: z[k] for k in z.files}
+    x64 = system.xyzq.astype(np.float64)
+    if hashlib.sha256(x64.tobytes()).digest() != z["xyzq_sha"].tobytes():
+        raise AssertionError(f"{name}: the seeded generator no longer gives the golden's input")
+    return system, z

@@ -142,3 +142,92 @@ def test_nonfinite_input_is_reported(precision):
         ctx.synchronize()
     assert ei.value.status == 8
     ctx.synchronize()  # reported once
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_misaligned_device_pointers_are_refused_on_the_host(precision):
+    """Device pointers that a kernel would read or write in place must be
+    aligned to the width it accesses them with: position records 16 (mixed)
+    or 32 (FP64) bytes, forces 8 bytes, spectra 16 bytes.  A view a few bytes
+    into an allocation is refused with GSE_ERR_INVALID_ARG before any work is
+    queued, and the context stays usable."""
+    import ctypes
+    import torch
+    from gse_b200 import _lib
+    from gse_b200.gse import Context
+    L = _lib.load()
+    M, box, n = 16, 16.0, 30
+    ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, box, box, box, precision=precision)
+    dt = torch.float32 if precision == "mixed" else torch.float64
+    rec = 16 if precision == "mixed" else 32
+    from gse_b200 import workloads as W
+    x = torch.zeros(4 * n + 8, dtype=dt, device="cuda")
+    x[:4 * n] = torch.from_numpy(W.triplets(n, box, 3).reshape(-1)).to(dt)
+    f = torch.zeros(3, n + 1, dtype=torch.float64, device="cuda")
+    e = ctypes.c_double()
+    h = ctx.h
+
+    def status(call):
+        st = call()
+        return st, L.gse_last_error().decode()
+
+    off = x.element_size()  # one element in: 4 or 8 bytes
+    st, msg = status(lambda: L.gse_forward(h, n, x.data_ptr() + off, ctypes.addressof(e),
+                                           f[0].data_ptr(), f[1].data_ptr(), f[2].data_ptr()))
+    assert st == 1 and f"{rec}-byte aligned" in msg, msg
+    st, msg = status(lambda: L.gse_spread_charge(h, n, x.data_ptr() + off))
+    assert st == 1 and "xyzq" in msg, msg
+    st, msg = status(lambda: L.gse_forward(h, n, x.data_ptr(), ctypes.addressof(e),
+                                           f[0].data_ptr() + 4, f[1].data_ptr(),
+                                           f[2].data_ptr()))
+    assert st == 1 and "8-byte aligned" in msg, msg
+    k = torch.zeros(2 * (M // 2 + 1) * M * M + 4, dtype=dt, device="cuda")
+    st, msg = status(lambda: L.gse_green_mul(h, 2.0, box, box, box, k.data_ptr() + 4))
+    assert st == 1 and "16-byte aligned" in msg, msg
+    # aligned pointers still work on the same context
+    st = L.gse_forward(h, n, x.data_ptr(), ctypes.addressof(e), f[0].data_ptr(),
+                       f[1].data_ptr(), f[2].data_ptr())
+    assert st == 0, L.gse_last_error().decode()
+    torch.cuda.synchronize()
+    assert np.isfinite(e.value) and torch.isfinite(f).all()
+    ctx.close()
+
+
+def test_ewald_refuses_misaligned_device_records():
+    import torch
+    from gse_b200 import _lib
+    import ctypes
+    L = _lib.load()
+    x = torch.zeros(4 * 10 + 4, dtype=torch.float64, device="cuda")
+    e = ctypes.c_double()
+    st = L.gse_ewald_recip(0, None, 2.0, 8, 10.0, 10.0, 10.0, 332.0716, 10, x.data_ptr() + 16,
+                           ctypes.addressof(e), None, None, None)
+    assert st == 1 and "32-byte aligned" in L.gse_last_error().decode()
+    st = L.gse_ewald_direct(0, None, 2.0, 4.0, 10.0, 10.0, 10.0, 332.0716, 10,
+                            x.data_ptr() + 8, 0, None, None, ctypes.addressof(e), None, None,
+                            None)
+    assert st == 1 and "32-byte aligned" in L.gse_last_error().decode()
+
+
+def test_mixed_range_overflow_is_reported():
+    """The mixed form accumulates each 16^3-cell brick in an int32 tile at a
+    power-of-two scale; a charge so large that even the coarsest scale leaves
+    no headroom (one charge above ~6.5e4 e at sigma1 1.26) makes the call
+    return GSE_ERR_RANGE instead of a wrapped grid.  The FP64 form has no such
+    limit, and the mixed context works again afterwards."""
+    from gse_b200._lib import GseError
+    from gse_b200.gse import Context
+    L, M = 24.0, 24
+    x = waters(900, L, 12)
+    n = x.shape[0]
+    f = [np.zeros(n) for _ in range(3)]
+    big = x.copy()
+    big[10, 3] = 1.0e5
+    ctx = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    with pytest.raises(GseError) as ei:
+        ctx.forward(n, big.astype(np.float32), *f)
+    assert ei.value.status == 9 and "fixed-point range" in str(ei.value)
+    E = ctx.forward(n, x.astype(np.float32), *f)
+    assert np.isfinite(E)
+    c64 = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="fp64")
+    assert np.isfinite(c64.forward(n, big, *f))

@@ -360,3 +360,27 @@ def test_field_at_atoms_is_force_per_unit_charge(precision, tol):
     E0 = [np.zeros(n) for _ in range(3)]
     g.interpolateField(n, x0.astype(ct), *E0)
     assert np.array_equal(np.stack(E0, 1), E)
+
+
+@pytest.mark.parametrize("name", ["water_48000_L78.4_M80", "water_262143_L140_M144"])
+def test_benchmark_boxes_match_reference(name):
+    """The two large benchmark boxes against the compiled reference's
+    CpuGSEk<double,double> (make_ref_configs.py): the 262,143-charge box the
+    force-evaluation rate is quoted on (L 140, M 144) and the 48,000-charge box
+    of the differentiation configuration (L 78.4, M 80), both sigma 2.0.  FP64
+    form: energy, 4096 sampled forces (Erms) and sum |F|^2 within 1e-12.  Mixed
+    form (the same FP32 positions the reference reads widened): within 1e-5."""
+    from conftest import load_ref_config
+    system, z = load_ref_config(name)
+    g = {"M": np.array(system.grid), "box": np.array(system.boxes), "sigma": system.sigma,
+         "xyzq": system.xyzq.astype(np.float64)}
+    idx = z["idx"]
+    for prec, tol in (("fp64", FP64_TOL), ("mixed", MIXED_TOL)):
+        _, E, F = run_gsek(g, prec)
+        f2 = float((F * F).sum())
+        print(name, prec, "E", rel(E, float(z["E"])), "F", rms(F[idx], z["F"]), "F2",
+              rel(f2, float(z["F2sum"])))
+        assert rel(E, float(z["E"])) <= tol
+        assert rms(F[idx], z["F"]) <= tol
+        assert rel(f2, float(z["F2sum"])) <= 2 * tol
+        assert np.abs(F.sum(axis=0) - z["Fsum"]).max() <= 10 * tol * np.sqrt(float(z["F2sum"]))

@@ -84,3 +84,56 @@ def test_wrappers_hand_valid_arrays_to_the_abi_and_refuse_bad_ones():
         with pytest.raises(GseError):
             bad_call()
     assert len(ctx._L.calls) == 7  # refused before any call
+
+
+class _FakeCudaTensor:
+    """Stands in for a CUDA tensor view that starts `offset` bytes into an
+    allocation (no GPU needed): only the attributes the binding inspects."""
+
+    def __init__(self, dtype, numel, offset):
+        self.dtype, self._numel, self._offset = dtype, numel, offset
+        self.is_cuda = True
+
+    def data_ptr(self):
+        return 0x7f0000000000 + self._offset
+
+    def is_contiguous(self):
+        return True
+
+    def numel(self):
+        return self._numel
+
+
+@pytest.mark.parametrize("precision,dtype,offset,align", [
+    ("mixed", torch.float32, 4, 16), ("mixed", torch.float32, 8, 16),
+    ("fp64", torch.float64, 16, 32), ("fp64", torch.float64, 8, 32)])
+def test_misaligned_device_positions_are_refused_before_the_abi(precision, dtype, offset, align):
+    """Positions are read on the GPU as float4/double4 records: a CUDA view
+    whose start is not 16/32-byte aligned is refused by every wrapper that
+    takes positions, and nothing reaches the library (the library checks the
+    same on the host for callers of the C ABI)."""
+    n = 5
+    ctx = _fake_context()
+    ctx.precision, ctx.dtype = precision, (np.float32 if precision == "mixed" else np.float64)
+    x = _FakeCudaTensor(dtype, 4 * n, offset)
+    f = [np.zeros(n) for _ in range(3)]
+    for call in (lambda: ctx.forward(n, x, *f), lambda: ctx.spread_charge(n, x),
+                 lambda: ctx.interpolate_force(n, x, *f), lambda: ctx.interpolate_field(n, x, *f),
+                 lambda: ctx.adjoint(n, x, 1.0, None, None, None, *f, np.zeros(n))):
+        with pytest.raises(GseError) as ei:
+            call()
+        assert ei.value.status == 1 and f"{align}-byte aligned" in str(ei.value)
+    assert ctx._L.calls == []
+    ok = _FakeCudaTensor(dtype, 4 * n, 2 * align)  # aligned view: passes to the ABI
+    ctx.spread_charge(n, ok)
+    assert ctx._L.calls[0][1][2] == ok.data_ptr()
+
+
+def test_positions_of_the_wrong_type_are_refused():
+    n = 4
+    ctx = _fake_context()  # mixed: float32 records
+    with pytest.raises(GseError):
+        ctx.spread_charge(n, np.zeros((n, 4), np.float64))
+    with pytest.raises(GseError):
+        ctx.spread_charge(n, np.zeros((n - 1, 4), np.float32))
+    assert ctx._L.calls == []

@@ -193,3 +193,18 @@ def test_restatement_matches_reference_at_other_splittings(oracle_lib, kappa, la
                                          lambda_sigma1=lam)
     assert e1 == e2
     assert np.array_equal(f1, f2)
+
+
+@pytest.mark.parametrize("name", ["water_48000_L78.4_M80", "water_262143_L140_M144"])
+def test_restatement_equals_reference_on_benchmark_boxes(oracle_lib, name):
+    """The restatement reproduces the compiled reference's CpuGSEk<double,double>
+    bit for bit on the two large benchmark boxes (make_ref_configs.py): energy,
+    4096 sampled forces and the force moments over every atom."""
+    from conftest import load_ref_config
+    system, z = load_ref_config(name)
+    E, F = oracle_lib.gsek_forward(system.grid, system.boxes, system.sigma,
+                                   system.xyzq.astype(np.float64))
+    assert E == float(z["E"])
+    assert np.array_equal(F[z["idx"]], z["F"])
+    assert (F * F).sum() == float(z["F2sum"])
+    assert np.array_equal(F.sum(axis=0), z["Fsum"])

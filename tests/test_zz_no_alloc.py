@@ -48,6 +48,9 @@ def test_noalloc_spread_matches_existing_entry_point_twice():
         got = out.cpu().numpy().reshape(M[2], M[1], M[0])
         want = _existing_spread(M, box, s1, rc, x)
         assert np.abs(got - want).max() <= TOL * np.abs(want).max()
+        # and against the CPU restatement of the reference's spread in double
+        ref = oracle.spread(M, box, s1, rc, x.astype(np.float64))
+        assert np.abs(got - ref).max() <= TOL * np.abs(ref).max()
 
 
 def test_noalloc_spread_rejects_oversized_grid_and_host_memory():
@@ -62,3 +65,16 @@ def test_noalloc_spread_rejects_oversized_grid_and_host_memory():
     st = L.gse_spread_mixed_noalloc(2, 2, 2, 1.26, 5.4, 0, None, 2.0, 2.0, 2.0,
                                     host.ctypes.data, None)
     assert st == 1 and "device memory" in L.gse_last_error().decode()
+
+
+def test_noalloc_spread_rejects_a_misaligned_record_array():
+    """Positions are read as 16-byte records: a device pointer 4 bytes into an
+    allocation is refused on the host, before anything runs on the GPU."""
+    import torch
+    from gse_b200 import _lib
+    L = _lib.load()
+    x = torch.zeros(4 * 10 + 1, dtype=torch.float32, device="cuda")
+    out = torch.empty(8 * 8 * 8, dtype=torch.float32, device="cuda")
+    st = L.gse_spread_mixed_noalloc(8, 8, 8, 1.26, 5.4, 10, x.data_ptr() + 4, 8.0, 8.0, 8.0,
+                                    out.data_ptr(), None)
+    assert st == 1 and "16-byte aligned" in L.gse_last_error().decode()
