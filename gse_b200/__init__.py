@@ -9,7 +9,6 @@ include/gse_b200.h).  Modules:
   gse_b200.torch_binding  a torch.autograd.Function over a Context
   gse_b200.multi          several GPUs: partitioned batches, max over ranks
   gse_b200.workloads      seeded synthetic systems of the benchmark shapes
-  gse_b200.profile_cases  small self-ending cases to run under a profiler
   gse_b200.build          the in-tree build of the library and the C++ check program
 """
 from ._lib import GseError  # noqa: F401

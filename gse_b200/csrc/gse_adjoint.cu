@@ -796,7 +796,7 @@ cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int nto
                                     const double* gfx, const double* gfy, const double* gfz,
                                     float* lambda, cudaStream_t st) {
   if (ntot <= 0) return cudaSuccess;
-  k_batch_adj_source<<<148 * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, gfx, gfy,
+  k_batch_adj_source<<<sm_count() * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, gfx, gfy,
                                                gfz, lambda);
   return cudaGetLastError();
 }
@@ -808,7 +808,7 @@ cudaError_t launch_batch_adj_gather(const float4* xyzq, const int* perm, int nto
                                     double* dq, double* dx, double* dy, double* dz,
                                     cudaStream_t st) {
   if (ntot <= 0) return cudaSuccess;
-  k_batch_adj_gather<<<148 * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, dLdE, psi,
+  k_batch_adj_gather<<<sm_count() * 16, 256, 0, st>>>(xyzq, perm, ntot, sys, first, nsys, c, dLdE, psi,
                                                phi, gfx, gfy, gfz, dq, dx, dy, dz);
   return cudaGetLastError();
 }
@@ -818,7 +818,7 @@ cudaError_t launch_adj_source(const typename Vec4<CT>::type* xyzq, const int* pe
                               const Stencil<CT>& s, double c, const double* gfx,
                               const double* gfy, const double* gfz, CT* lambda, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  const int blocks = (int)std::min<long long>(148 * 16, (n + 7) / 8);
+  const int blocks = (int)std::min<long long>(sm_count() * 16, (n + 7) / 8);
   k_adj_source<CT><<<blocks, 256, 0, st>>>(xyzq, perm, n, s, c, gfx, gfy, gfz, lambda);
   return cudaGetLastError();
 }
@@ -830,7 +830,7 @@ cudaError_t launch_adj_gather(const typename Vec4<CT>::type* xyzq, const int* pe
                               const double* gfy, const double* gfz, double* dq, double* dx,
                               double* dy, double* dz, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  const int blocks = (int)std::min<long long>(148 * 16, (n + 7) / 8);
+  const int blocks = (int)std::min<long long>(sm_count() * 16, (n + 7) / 8);
   k_adj_gather<CT><<<blocks, 256, 0, st>>>(xyzq, perm, n, sp, sg, c, gE_ch3, psi, phi, gfx, gfy,
                                            gfz, dq, dx, dy, dz);
   return cudaGetLastError();

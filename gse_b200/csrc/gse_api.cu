@@ -66,8 +66,9 @@ gse_status_t fail(gse_status_t s, const char* fmt, ...) {
     if (_s != GSE_OK) return _s;                                                            \
   } while (0)
 
-constexpr int kEnergyPartials = 148 * 16;  // blocks of the energy reductions (+1 counter slot)
-constexpr int kBrick = 4;
+// capacity of the reductions' per-block partial sums (+1 counter slot); the
+// reductions launch at most this many blocks
+constexpr int kEnergyPartials = 2368;
 
 bool is_device_ptr(const void* p) {
   if (!p) return false;
@@ -150,13 +151,7 @@ struct gse_context {
   void* d_xyzq = nullptr;
   void* d_sorted = nullptr;
   int* d_perm = nullptr;
-  int* d_keys = nullptr;
-  int* d_slots = nullptr;
   size_t atom_cap = 0;
-  int* d_counts = nullptr;
-  int* d_offsets = nullptr;
-  BinGeom bg{};
-  int nbins = 0;
   // binning of the tiled kernels (stable sort by z cell, y cell, x bin)
   BinLayout bl{};
   int nbins2 = 0;
@@ -311,13 +306,11 @@ gse_status_t ensure_atoms(gse_context_t* c, int n) {
   cudaFree(c->d_xyzq);
   cudaFree(c->d_sorted);
   cudaFree(c->d_perm);
-  cudaFree(c->d_keys);
-  cudaFree(c->d_slots);
   cudaFree(c->d_force);
   cudaFree(c->d_bkey);
   cudaFree(c->d_btmp);
   c->d_xyzq = c->d_sorted = nullptr;
-  c->d_perm = c->d_keys = c->d_slots = nullptr;
+  c->d_perm = nullptr;
   c->d_force = nullptr;
   c->d_bkey = c->d_btmp = nullptr;
   c->atom_cap = 0;
@@ -325,8 +318,6 @@ gse_status_t ensure_atoms(gse_context_t* c, int n) {
   CU(cudaMalloc(&c->d_xyzq, cap * rec));
   CU(cudaMalloc(&c->d_sorted, cap * rec));
   CU(cudaMalloc(&c->d_perm, cap * sizeof(int)));
-  CU(cudaMalloc(&c->d_keys, cap * sizeof(int)));
-  CU(cudaMalloc(&c->d_slots, cap * sizeof(int)));
   CU(cudaMalloc(&c->d_force, 3 * cap * sizeof(double)));
   CU(cudaMalloc(&c->d_bkey, cap * sizeof(int)));
   CU(cudaMalloc(&c->d_btmp, cap * sizeof(int)));
@@ -826,12 +817,6 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
     return st;
   }
   const int M[3] = {p.size_x, p.size_y, p.size_z};
-  for (int d = 0; d < 3; d++) {
-    c->bg.M[d] = M[d];
-    c->bg.B[d] = kBrick;
-    c->bg.nb[d] = (M[d] + kBrick - 1) / kBrick;
-  }
-  c->nbins = c->bg.nb[0] * c->bg.nb[1] * c->bg.nb[2];
 
   auto bail = [&](gse_status_t s) {
     gse_destroy(c);
@@ -856,14 +841,12 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
       c->own_fft = true;
     }
   }
-  CUC(cudaMalloc(&c->d_counts, sizeof(int) * c->nbins));
   c->bl = make_bin_layout(M, c->fp64 ? kBinX64 : kBinX32);
   c->nbins2 = bin_count(c->bl);
   CUC(cudaMalloc(&c->d_bcounts, sizeof(int) * c->nbins2));
   CUC(cudaMalloc(&c->d_bstart, sizeof(int) * (c->nbins2 + 1)));
   CUC(cudaMalloc(&c->d_btiles, sizeof(int) * (c->nbins2 / 4096 + 2)));
   CUC(cudaMalloc(&c->d_qmax, sizeof(unsigned)));
-  CUC(cudaMalloc(&c->d_offsets, sizeof(int) * (c->nbins + 1)));
   CUC(cudaMalloc(&c->d_partials, sizeof(double) * (kEnergyPartials + 1)));
   CUC(cudaMemset(c->d_partials, 0, sizeof(double) * (kEnergyPartials + 1)));
   CUC(cudaMalloc(&c->d_scalars, sizeof(double) * 16));
@@ -910,11 +893,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_xyzq);
   cudaFree(c->d_sorted);
   cudaFree(c->d_perm);
-  cudaFree(c->d_keys);
-  cudaFree(c->d_slots);
   cudaFree(c->d_force);
-  cudaFree(c->d_counts);
-  cudaFree(c->d_offsets);
   cudaFree(c->d_bkey);
   cudaFree(c->d_btmp);
   cudaFree(c->d_bcounts);
@@ -1458,8 +1437,7 @@ gse_status_t gse_virial(gse_context_t* c, double* virial) {
     c->gtab_valid = true;
   }
   TRY(fft_forward(c, c->d_rho, c->d_rhok));
-  const int nb = 148 * 2;
-  static_assert(6 * 148 * 2 <= kEnergyPartials, "virial partials fit the energy partials");
+  const int nb = std::min(sm_count() * 2, kEnergyPartials / 6);
   unsigned* done = reinterpret_cast<unsigned*>(c->d_partials + kEnergyPartials);
   const double hs2 = 0.5 * c->p.sigma * c->p.sigma;
   double* out = c->d_scalars + 8;

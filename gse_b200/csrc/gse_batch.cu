@@ -440,8 +440,7 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
             CUFFT_SUCCESS)
       return bail(set_error(GSE_ERR_CUDA, "cufftPlanMany failed"));
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
+  const int sms = sm_count();
   b->scat_ctas = 2 * sms;
   b->gath_ctas = 2 * sms;
   b->agath_ctas = 2 * sms;
@@ -643,8 +642,7 @@ gse_status_t gse_batch_autotune(gse_batch_t* b, const char* cache_path, int use_
       }
     }
   }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
+  const int sms = sm_count();
   cudaEvent_t e0, e1;
   BCU(cudaEventCreate(&e0));
   BCU(cudaEventCreate(&e1));

@@ -178,7 +178,7 @@ cudaError_t launch_ewald_direct(const double4* xyzq, int n, const EwdGeom& g, Ew
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(w.done, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
-  const int gb = n > 0 ? (int)std::min<long long>(148 * 8, (n + 255) / 256) : 1;
+  const int gb = n > 0 ? (int)std::min<long long>(sm_count() * 8, (n + 255) / 256) : 1;
   if (n > 0) k_ewd_cell_count<<<gb, 256, 0, st>>>(xyzq, n, g, w.key, w.counts);
   BinScratch b;
   b.key = w.key;

@@ -364,7 +364,7 @@ template <typename CT>
 cudaError_t launch_dipole(const CT* rho, const int M[3], const CT h[3], double* partials,
                           unsigned* done, double* out, cudaStream_t st) {
   const long long rows = (long long)M[1] * M[2];
-  const int nb = (int)std::min<long long>(rows, kDipoleBlocks);
+  const int nb = (int)std::min<long long>(rows, std::min(kDipoleBlocks, sm_count() * 4));
   k_dipole<CT><<<nb, 256, 0, st>>>(rho, M[0], M[1], M[2], h[0], h[1], h[2], partials, done, out);
   return cudaGetLastError();
 }

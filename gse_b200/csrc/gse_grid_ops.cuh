@@ -33,7 +33,7 @@ cudaError_t launch_efield(const CT* phi, CT* ex, CT* ey, CT* ez, const int M[3],
 // Dipole sum of a charge grid (CpuGaussCharge.cpp:188-226): out[0..2] =
 // sum_p (double)((rho_p hx hy hz) * (h_d i_d)).  partials holds 3 * kDipoleBlocks
 // doubles; done is a zeroed counter that the last block resets.
-constexpr int kDipoleBlocks = 148 * 4;
+constexpr int kDipoleBlocks = 592;  // capacity; launches use up to 4 per SM
 template <typename CT>
 cudaError_t launch_dipole(const CT* rho, const int M[3], const CT h[3], double* partials,
                           unsigned* done, double* out, cudaStream_t st);

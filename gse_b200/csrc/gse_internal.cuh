@@ -4,9 +4,30 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cmath>
 
 namespace gse {
+
+// Streaming multiprocessors of the current device (148 on a B200), looked up
+// once per device; grid-stride kernels size their grids as multiples of it.
+inline int sm_count() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 148;
+  }
+  int v = cache[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    cache[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
 
 constexpr double kPi = 3.14159265358979323846;  // pi_dbl, TypesGSE.h:24
 constexpr int kMaxStencil = 64;                  // max 2n+1 per axis

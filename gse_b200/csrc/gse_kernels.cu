@@ -1,7 +1,6 @@
 // gse_kernels.cu -- CUDA kernels of the GSE-k path (sm_100a).
 //
 // Stage map (reference = ap-hynninen/GSE):
-//   k_bin_*          cell binning of atoms (locality for the gather)
 //   k_spread_atomic  CpuGaussCharge::spreadChargeToGrid  (CpuGaussCharge.cpp:235-384)
 //   k_fixed_to_real  int64 fixed-point grid -> CT grid (mixed form)
 //   k_green_energy   CpuGreensFuncGSE::mul (CpuGreensFuncGSE.cpp:9-57) fused with
@@ -14,69 +13,6 @@
 #include "gse_reduce.cuh"
 
 namespace gse {
-
-// ---------------------------------------------------------------------------
-// Binning: atoms are keyed by the brick holding their stencil centre
-// round(x/h) (mod M).  Order inside a brick is not specified.
-// ---------------------------------------------------------------------------
-template <typename CT>
-__global__ void k_bin_keys(const typename Vec4<CT>::type* __restrict__ xyzq, int n, BinGeom bg,
-                           CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ keys,
-                           int* __restrict__ slots, int* __restrict__ counts,
-                           int* __restrict__ bad) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const auto a = xyzq[i];
-    if (!(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(a.w))) {
-      atomicExch(bad, 1);
-      keys[i] = 0;
-      slots[i] = atomicAdd(&counts[0], 1);
-      continue;
-    }
-    const int cx = pmod(round_to_int(mul_rn(a.x, inv_hx)), bg.M[0]);
-    const int cy = pmod(round_to_int(mul_rn(a.y, inv_hy)), bg.M[1]);
-    const int cz = pmod(round_to_int(mul_rn(a.z, inv_hz)), bg.M[2]);
-    const int b = (cz / bg.B[2] * bg.nb[1] + cy / bg.B[1]) * bg.nb[0] + cx / bg.B[0];
-    keys[i] = b;
-    slots[i] = atomicAdd(&counts[b], 1);
-  }
-}
-
-// Exclusive scan of counts[0..nb) into offsets[0..nb], single block.
-__global__ void k_bin_scan(const int* __restrict__ counts, int nb, int* __restrict__ offsets) {
-  __shared__ int part[1024];
-  const int t = threadIdx.x, T = blockDim.x;
-  const int chunk = (nb + T - 1) / T;
-  const int lo = min(nb, t * chunk), hi = min(nb, lo + chunk);
-  int s = 0;
-  for (int i = lo; i < hi; i++) s += counts[i];
-  part[t] = s;
-  __syncthreads();
-  for (int o = 1; o < T; o <<= 1) {
-    const int v = (t >= o) ? part[t - o] : 0;
-    __syncthreads();
-    part[t] += v;
-    __syncthreads();
-  }
-  int run = part[t] - s;
-  for (int i = lo; i < hi; i++) {
-    offsets[i] = run;
-    run += counts[i];
-  }
-  if (t == T - 1) offsets[nb] = part[t];
-}
-
-template <typename CT>
-__global__ void k_bin_scatter(const typename Vec4<CT>::type* __restrict__ xyzq, int n,
-                              const int* __restrict__ keys, const int* __restrict__ slots,
-                              const int* __restrict__ offsets,
-                              typename Vec4<CT>::type* __restrict__ sorted,
-                              int* __restrict__ perm) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int d = offsets[keys[i]] + slots[i];
-    sorted[d] = xyzq[i];
-    perm[d] = i;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Spread: one warp per atom.  The three 1-D weight rows are computed once per
@@ -393,7 +329,7 @@ template <typename CT>
 cudaError_t launch_unit_charges(const typename Vec4<CT>::type* in, typename Vec4<CT>::type* out,
                                 int n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_unit_charges<CT><<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(in, out, n);
+  k_unit_charges<CT><<<std::min((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(in, out, n);
   return cudaGetLastError();
 }
 template cudaError_t launch_unit_charges<double>(const double4*, double4*, int, cudaStream_t);
@@ -570,21 +506,6 @@ static int blocks_for(long long work, int per_block, int cap) {
 }
 
 template <typename CT>
-cudaError_t launch_bin(const typename Vec4<CT>::type* xyzq, int n, const BinGeom& bg, CT inv_hx,
-                       CT inv_hy, CT inv_hz, int* keys, int* slots, int* counts, int* offsets,
-                       typename Vec4<CT>::type* sorted, int* perm, int* bad, cudaStream_t st) {
-  const int nb = bg.nb[0] * bg.nb[1] * bg.nb[2];
-  cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * nb, st);
-  if (e != cudaSuccess) return e;
-  const int gb = blocks_for(n, 256, 148 * 8);
-  k_bin_keys<CT><<<gb, 256, 0, st>>>(xyzq, n, bg, inv_hx, inv_hy, inv_hz, keys, slots, counts,
-                                     bad);
-  k_bin_scan<<<1, 1024, 0, st>>>(counts, nb, offsets);
-  k_bin_scatter<CT><<<gb, 256, 0, st>>>(xyzq, n, keys, slots, offsets, sorted, perm);
-  return cudaGetLastError();
-}
-
-template <typename CT>
 cudaError_t launch_spread(const typename Vec4<CT>::type* xyzq, int n, const Stencil<CT>& s,
                           CT* grid, long long* fixed_grid, cudaStream_t st) {
   const long long size = (long long)s.M[0] * s.M[1] * s.M[2];
@@ -595,7 +516,7 @@ cudaError_t launch_spread(const typename Vec4<CT>::type* xyzq, int n, const Sten
     e = cudaMemsetAsync(grid, 0, sizeof(CT) * size, st);
   if (e != cudaSuccess) return e;
   if (n > 0) {
-    const int gb = blocks_for(n, 8, 148 * 16);
+    const int gb = blocks_for(n, 8, sm_count() * 16);
     if (fixed_grid)
       k_spread_atomic<CT, true><<<gb, 256, 0, st>>>(xyzq, n, s, grid,
                                                     (unsigned long long*)fixed_grid);
@@ -603,7 +524,7 @@ cudaError_t launch_spread(const typename Vec4<CT>::type* xyzq, int n, const Sten
       k_spread_atomic<CT, false><<<gb, 256, 0, st>>>(xyzq, n, s, grid, nullptr);
   }
   if (fixed_grid) {
-    k_fixed_to_real<CT><<<blocks_for(size, 256, 148 * 16), 256, 0, st>>>(
+    k_fixed_to_real<CT><<<blocks_for(size, 256, sm_count() * 16), 256, 0, st>>>(
         fixed_grid, size, 1.0 / s.fixed_scale, grid);
   }
   return cudaGetLastError();
@@ -620,7 +541,7 @@ cudaError_t launch_green_energy(typename Cplx<CT>::type* rhok, const GreenGeom& 
 
 template <typename CT>
 cudaError_t launch_green_table(const GreenGeom& g, CT* tab, cudaStream_t st) {
-  k_green_table<CT><<<148 * 8, 256, 0, st>>>(g, tab);
+  k_green_table<CT><<<sm_count() * 8, 256, 0, st>>>(g, tab);
   return cudaGetLastError();
 }
 
@@ -637,7 +558,7 @@ cudaError_t launch_dot_energy(const CT* a, const CT* b, long long size, double* 
                               double factor, double* energy_out, cudaStream_t st) {
   // fewer, fuller blocks than the other energy kernels; the counter stays in
   // the slot after np partials that they use
-  k_dot<CT><<<std::min(np, 148 * 4), 256, 0, st>>>(
+  k_dot<CT><<<std::min(np, sm_count() * 4), 256, 0, st>>>(
       a, b, size, partials, reinterpret_cast<unsigned*>(partials + np), factor, energy_out);
   return cudaGetLastError();
 }
@@ -647,16 +568,13 @@ cudaError_t launch_gather(const typename Vec4<CT>::type* xyzq, const int* perm, 
                           const Stencil<CT>& s, const CT* phi, double outscale, double* fx,
                           double* fy, double* fz, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  const int gb = blocks_for(n, 8, 148 * 16);
+  const int gb = blocks_for(n, 8, sm_count() * 16);
   typedef typename std::conditional<sizeof(CT) == 8, double, float>::type ACC;
   k_gather<CT, ACC><<<gb, 256, 0, st>>>(xyzq, perm, n, s, phi, outscale, fx, fy, fz);
   return cudaGetLastError();
 }
 
 #define GSE_INSTANTIATE(CT)                                                                    \
-  template cudaError_t launch_bin<CT>(const Vec4<CT>::type*, int, const BinGeom&, CT, CT, CT,  \
-                                      int*, int*, int*, int*, Vec4<CT>::type*, int*, int*,     \
-                                      cudaStream_t);                                           \
   template cudaError_t launch_spread<CT>(const Vec4<CT>::type*, int, const Stencil<CT>&, CT*,  \
                                          long long*, cudaStream_t);                            \
   template cudaError_t launch_green_energy<CT>(Cplx<CT>::type*, const GreenGeom&, double*,     \

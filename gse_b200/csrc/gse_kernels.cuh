@@ -7,13 +7,6 @@
 
 namespace gse {
 
-// Brick binning geometry: bricks of B cells per axis, nb bricks per axis.
-struct BinGeom {
-  int M[3];
-  int B[3];
-  int nb[3];
-};
-
 // Green's-function geometry (CpuGreensFuncGSE.cpp:14-28), FP64 constants.
 struct GreenGeom {
   int nfft[3];
@@ -25,11 +18,6 @@ struct GreenGeom {
   double fourpi_vol;  // 4 pi / (nx ny nz): the c2r normalisation folded in
   double sigmafac;    // sigma^2 / 2
 };
-
-template <typename CT>
-cudaError_t launch_bin(const typename Vec4<CT>::type* xyzq, int n, const BinGeom& bg, CT inv_hx,
-                       CT inv_hy, CT inv_hz, int* keys, int* slots, int* counts, int* offsets,
-                       typename Vec4<CT>::type* sorted, int* perm, int* bad, cudaStream_t st);
 
 template <typename CT>
 cudaError_t launch_spread(const typename Vec4<CT>::type* xyzq, int n, const Stencil<CT>& s,

@@ -820,7 +820,7 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
     e = cudaMemsetAsync(qmax, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
   }
-  const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
+  const int gb = (int)std::min<long long>(sm_count() * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
                                         qmax, w.bad);
@@ -837,7 +837,7 @@ cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, in
   const int ntiles = (nb + kScanTile - 1) / kScanTile;
   if (ntiles > kScanTile) return cudaErrorInvalidValue;
   cudaError_t e;
-  const int gb = (int)std::min<long long>(148 * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
+  const int gb = (int)std::min<long long>(sm_count() * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.start, w.tile_sums);
   k_scan_sums<<<1, kScanThreads, 0, st>>>(w.tile_sums, ntiles, w.start, nb);
   k_scan_add<<<(nb + 255) / 256, 256, 0, st>>>(w.start, nb, w.tile_sums);
@@ -925,7 +925,7 @@ cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int
 
 cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float* out,
                                   cudaStream_t st) {
-  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, out);
+  k_grid64_to_real<<<sm_count() * 8, 256, 0, st>>>(grid64, size, out);
   return cudaGetLastError();
 }
 
@@ -953,7 +953,7 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
   k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(sorted, start, b,
                                                                               s, grid64);
   // rho == nullptr: the caller converts the int64 grid itself (the own FFT)
-  if (rho) k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, size, rho);
+  if (rho) k_grid64_to_real<<<sm_count() * 8, 256, 0, st>>>(grid64, size, rho);
   return cudaGetLastError();
 }
 
@@ -1118,7 +1118,7 @@ cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, 
                              cudaStream_t st) {
   const cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nbins, st);
   if (e != cudaSuccess) return e;
-  const int gb = (int)std::min<long long>(148 * 8, (ntot + 255) / 256 > 0 ? (ntot + 255) / 256 : 1);
+  const int gb = (int)std::min<long long>(sm_count() * 8, (ntot + 255) / 256 > 0 ? (ntot + 255) / 256 : 1);
   if (ntot > 0)
     k_batch_bin_count<<<gb, 256, 0, st>>>(xyzq, ntot, sys, first, nsys, w.key, w.counts);
   return launch_bin_scan_place<float>(xyzq, ntot, nbins, w, sorted, perm, st);
@@ -1142,14 +1142,14 @@ cudaError_t launch_batch_spread(const float4* sorted, const int* start, const Ba
     }
     if (e != cudaSuccess) return e;
   }
-  k_grid64_to_real<<<148 * 8, 256, 0, st>>>(grid64, gsize, rho);
+  k_grid64_to_real<<<sm_count() * 8, 256, 0, st>>>(grid64, gsize, rho);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_green(float2* rhok, const float* tab, long long ktot, const BatchSys* sys,
                                const long long* kfirst, const int* ksys, int nsys, double* energy,
                                cudaStream_t st) {
-  k_batch_green_apply<<<148 * 8, 256, 0, st>>>(rhok, tab, ktot, sys, kfirst, ksys, nsys, energy);
+  k_batch_green_apply<<<sm_count() * 8, 256, 0, st>>>(rhok, tab, ktot, sys, kfirst, ksys, nsys, energy);
   return cudaGetLastError();
 }
 

@@ -38,10 +38,27 @@ _lib = None
 _ref = None
 
 
+# Where the reference sources are read from when oracle/_ref is built: the
+# GSE_REFERENCE_DIR environment variable, else the build container's checkout.
+DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
+def reference_dir() -> Optional[str]:
+    """The reference source tree, or None where it is absent (a GPU box uses
+    the prebuilt oracle/_ref)."""
+    d = os.environ.get("GSE_REFERENCE_DIR", DEFAULT_REFERENCE_DIR)
+    return d if os.path.isfile(os.path.join(d, "CpuGSEk.cpp")) else None
+
+
 def build(with_reference: bool = False) -> None:
-    """Compile the restatement (and, if asked, the reference build)."""
-    target = "ref" if with_reference else "all"
-    subprocess.run(["make", "-s", "-C", _HERE, target], check=True)
+    """Compile the restatement (and, if asked, the reference build from
+    reference_dir())."""
+    cmd = ["make", "-s", "-C", _HERE]
+    if with_reference and reference_dir():
+        cmd += ["ref", f"REF={reference_dir()}"]
+    else:
+        cmd += ["all"]
+    subprocess.run(cmd, check=True)
 
 
 def _ptr(a: Optional[np.ndarray], kind=_dp):

@@ -1,11 +1,11 @@
 """Small, self-ending GPU cases to run under a profiler (ncu), one GPU.
 
-  python -m gse_b200.profile_cases forward [--evals 3] [--precision mixed|fp64]
+  python profile_cases.py forward [--evals 3] [--precision mixed|fp64]
       the benchmark workload (262,143 water-like charges, M = 144, sigma 2):
       one context, `evals` forward evaluations on device buffers (the first
       builds the Green's table and records the key, the next ones run
       directly and then replay a CUDA graph), no L2-flush buffer
-  python -m gse_b200.profile_cases gridops [--steps 5] [--warmup 2]
+  python profile_cases.py gridops [--steps 5] [--warmup 2]
       the bench's grid-operation leg (on-grid convolution and field of a 144^3
       grid, both calculation types)
 
@@ -19,13 +19,17 @@ import json
 import os
 import sys
 
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
 
 def forward(evals: int, precision: str) -> None:
     import numpy as np
     import torch
 
-    from . import workloads as W
-    from .gse import Context
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
     s = W.config_water_262k()
     n = s.n
     ctx = Context(s.M, s.M, s.M, s.sigma, s.kappa, s.lambda_sigma, s.lambda_sigma1, s.box, s.box,
@@ -43,8 +47,6 @@ def forward(evals: int, precision: str) -> None:
 
 def gridops(steps: int, warmup: int) -> None:
     import torch
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    sys.path.insert(0, root)
     import bench
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     peak, _ = bench.hbm_peak()
@@ -52,7 +54,7 @@ def gridops(steps: int, warmup: int) -> None:
 
 
 def main(argv=None) -> None:
-    ap = argparse.ArgumentParser(prog="python -m gse_b200.profile_cases")
+    ap = argparse.ArgumentParser(prog="python profile_cases.py")
     sub = ap.add_subparsers(dest="case", required=True)
     fw = sub.add_parser("forward")
     fw.add_argument("--evals", type=int, default=3)

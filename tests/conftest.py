@@ -62,7 +62,7 @@ def ref48k():
 @pytest.fixture(scope="session")
 def oracle_lib():
     import oracle
-    oracle.build(with_reference=os.path.isdir("/root/reference"))
+    oracle.build(with_reference=oracle.reference_dir() is not None)
     return oracle
 
 

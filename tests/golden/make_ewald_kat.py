@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import oracle  # noqa: E402
 
-REF_DATA = "/root/reference/data/xyzq_48k.txt"
+REF_DATA = os.path.join(os.environ.get("GSE_REFERENCE_DIR", "/root/reference"), "data",
+                        "xyzq_48k.txt")
 
 
 def main():

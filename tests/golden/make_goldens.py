@@ -16,7 +16,6 @@ Output: tests/golden/gse_goldens.npz (+ water_23559.npz for the 23,559-charge
 water box, energy and forces only).
 """
 import os
-import subprocess
 import sys
 
 import numpy as np
@@ -47,7 +46,7 @@ def cases():
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    oracle.build(with_reference=True)
     data = {}
     for name, xyzq, M, box, sigma in cases():
         xyzq = np.ascontiguousarray(xyzq, dtype=np.float64)

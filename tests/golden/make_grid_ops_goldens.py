@@ -16,7 +16,6 @@ sigma2 (CpuGSEr.cpp:39-42).  The potential fed to the field is the input grid.
 Output: tests/golden/grid_ops_goldens.npz.
 """
 import os
-import subprocess
 import sys
 
 import numpy as np
@@ -45,7 +44,7 @@ def cases():
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    oracle.build(with_reference=True)
     data = {}
     for name, M, box, sigma, rho in cases():
         rcut = 3.0 * np.sqrt(2.0) * sigma

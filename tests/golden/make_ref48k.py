@@ -17,7 +17,6 @@ Runs in the container that holds the reference sources.  Writes
 import hashlib
 import lzma
 import os
-import subprocess
 import sys
 
 import numpy as np
@@ -28,7 +27,8 @@ sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
 
-REF_DATA = "/root/reference/data/xyzq_48k.txt"
+REF_DATA = os.path.join(os.environ.get("GSE_REFERENCE_DIR", "/root/reference"), "data",
+                        "xyzq_48k.txt")
 SIGMA, BOX, GRID = 2.12132034355964, 80.0, 80
 
 
@@ -39,7 +39,7 @@ def load_xz(path):
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    oracle.build(with_reference=True)
     text = open(REF_DATA, "rb").read()
     xz = os.path.join(HERE, "xyzq_48k.txt.xz")
     with lzma.open(xz, "wb", preset=9) as f:

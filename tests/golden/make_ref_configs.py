@@ -20,7 +20,6 @@ ref_<name>.npz with E; the forces of 4096 atoms (a seeded sample, indices in
 """
 import hashlib
 import os
-import subprocess
 import sys
 import time
 
@@ -57,9 +56,9 @@ def make(system, seed: int) -> None:
 
 
 def main():
-    ref_dir = os.environ.get("GSE_REFERENCE_DIR", "/root/reference")
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={ref_dir}"],
-                   check=True)
+    if oracle.reference_dir() is None:
+        sys.exit("the reference sources are needed (set GSE_REFERENCE_DIR)")
+    oracle.build(with_reference=True)
     make(W.config_water_262k(), 262)
     make(W.config_water_48k(), 48)
 
