@@ -401,10 +401,15 @@ def main():
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         barrier()
         torch.cuda.synchronize()
+        t_busy = None
         if clocks is not None:
-            # the sampler needs a moment to start: keep the GPU busy meanwhile
+            # the sampler needs a moment to start: keep the GPU busy with the
+            # same evaluation meanwhile; a timed region of a few ms may fall
+            # between two samples, so the clock record spans this busy period
+            # and the timed region (same work, back to back)
             clocks.start()
-            t_end = time.time() + 0.5
+            t_busy = time.time()
+            t_end = t_busy + 1.0
             while time.time() < t_end:
                 ctx.forward(n, x, f[0], f[1], f[2], energy_out=e)
                 torch.cuda.synchronize()
@@ -420,7 +425,7 @@ def main():
         launches = ctx.launch_count() - launches0
         clock_info = None
         if clocks is not None:
-            clocks.mark(t0, t1)
+            clocks.mark(t_busy, t1)
             clock_info = clocks.stop()
         barrier()
         ctx.set_timing(False)

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "gse_dropin.h"
@@ -79,6 +80,22 @@ int run(int M[3], double L[3], double sigma, const std::vector<double>& raw) {
              (double)phi.getDataPointer()[i], (double)rhoS.getDataPointer()[i],
              (double)Ex.getDataPointer()[i], (double)Ey.getDataPointer()[i],
              (double)Ez.getDataPointer()[i]);
+  }
+  // the reference's third instance, CpuGaussCharge<float,float>
+  // (CpuGaussCharge.cpp:524-526): the same spread, then the gather from the
+  // solved potential with float force arrays
+  if constexpr (std::is_same<CT, float>::value) {
+    if (getenv("GSE_CHECK_FLOAT_FLOAT")) {
+      CpuGaussCharge<float, float> gff(M[0], M[1], M[2]);
+      CpuGrid<float> rff(M[0], M[1], M[2]);
+      gff.spreadChargeToGrid(sigma1, rcut, n, xyzq.data(), L[0], L[1], L[2], rff);
+      for (int i = 0; i < rff.getSize(); i++) printf("RFF %.9g\n", rff.getDataPointer()[i]);
+      std::vector<float> gx(n), gy(n), gz(n);
+      gff.interpolateForce(sigma1, rcut, n, xyzq.data(), L[0], L[1], L[2], phi, gx.data(),
+                           gy.data(), gz.data());
+      for (int i = 0; i < n; i++) printf("FFF %.9g %.9g %.9g\n", gx[i], gy[i], gz[i]);
+      for (int i = 0; i < phi.getSize(); i++) printf("PHI %.9g\n", phi.getDataPointer()[i]);
+    }
   }
   // the FP64 Ewald references of the same charges (the sequence of
   // cpu_gse.cpp:555-560), with the water exclusions of rigid 3-site molecules

@@ -148,6 +148,8 @@ def ref():
         R.ref_ewald_direct.argtypes = [_d, _d, _d, _d, _d, _d, _i, _dp, _i, _ip, _ip, _dp, _dp,
                                        _dp]
         R.ref_ewald_direct.restype = _d
+        R.ref_grid_save.argtypes = [_i, _i, _i, _i, _vp, ctypes.c_char_p]
+        R.ref_grid_save.restype = _i
         _ref = R
     return _ref
 
@@ -432,3 +434,14 @@ def ref_ewald_direct(sigma, rcut, box, xyzq, ccelec=CCELEC, iblo14=None, inb14=N
     e = ref().ref_ewald_direct(sigma, rcut, box[0], box[1], box[2], ccelec, n, _ptr(a), ne,
                                _ptr(ib, _ip), _ptr(nb, _ip), _ptr(fx), _ptr(fy), _ptr(fz))
     return float(e), np.stack([fx, fy, fz], axis=1)
+
+
+def ref_grid_save(grid: np.ndarray, filename) -> None:
+    """The reference's CpuGrid<T>::save (CpuGrid.h:76-90) of a [z][y][x]
+    float64 or float32 grid into `filename`."""
+    g = np.ascontiguousarray(grid)
+    if g.dtype not in (np.float64, np.float32) or g.ndim != 3:
+        raise ValueError("a 3-D float64 or float32 grid")
+    sz, sy, sx = g.shape
+    ref().ref_grid_save(0 if g.dtype == np.float64 else 1, sx, sy, sz, g.ctypes.data,
+                        os.fsencode(str(filename)))

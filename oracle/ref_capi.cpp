@@ -7,6 +7,8 @@
 // gse_oracle.c, and bench.py times it as the reference CPU baseline.  The
 // product library never links it.
 #include <cstring>
+#include <fstream>
+#include <iostream>
 
 #include "CpuEwaldDirect.h"
 #include "CpuEwaldRecip.h"
@@ -189,6 +191,22 @@ double ref_ewald_direct(double sigma, double rcut, double boxx, double boxy, dou
   CpuEwaldDirect e(sigma, rcut, boxx, boxy, boxz, ccelec);
   if (n_iblo14 > 0) e.setupExclusions(n_iblo14, iblo14, inb14);
   return e.calcForceEnergy(n, reinterpret_cast<const xyzq_t<double>*>(xyzq), fx, fy, fz);
+}
+
+// CpuGrid<T>::save (CpuGrid.h:76-90, header-only): the reference's own grid
+// text writer on a grid holding `data` (x fastest); type 0 = double, 1 = float.
+int ref_grid_save(int type, int sx, int sy, int sz, const void* data, const char* filename) {
+  const size_t size = (size_t)sx * sy * sz;
+  if (type == 0) {
+    CpuGrid<double> g(sx, sy, sz);
+    std::memcpy(g.getDataPointer(), data, size * sizeof(double));
+    static_cast<const CpuGrid<double>&>(g).save(filename);
+  } else {
+    CpuGrid<float> g(sx, sy, sz);
+    std::memcpy(g.getDataPointer(), data, size * sizeof(float));
+    static_cast<const CpuGrid<float>&>(g).save(filename);
+  }
+  return 0;
 }
 
 }  // extern "C"

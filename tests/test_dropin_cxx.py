@@ -224,3 +224,33 @@ def test_reference_instances_compile(tmp_path):
         return
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 3 and out.stdout.startswith("error "), (out.returncode, out.stdout)
+
+
+@pytest.mark.gpu
+def test_dropin_float_float_instance(goldens, tmp_path):
+    """The reference's third instance, CpuGaussCharge<float,float>
+    (CpuGaussCharge.cpp:524-526), through the C++ drop-in on the GPU: its
+    spread and its gather (float force arrays) against the oracle's float
+    restatement of the reference, which equals the compiled reference's float
+    instance bit for bit (test_oracle.py), within 1e-5."""
+    import oracle
+    g = goldens["water300_noncubic"]
+    prog = program()
+    out = run(prog, "mixed", g, tmp_path, env={"GSE_CHECK_FLOAT_FLOAT": "1"})
+    assert out.returncode == 0, out.stderr
+    rows = {"RFF": [], "FFF": [], "PHI": []}
+    for line in out.stdout.splitlines():
+        tag, *vals = line.split()
+        if tag in rows:
+            rows[tag].append([float(v) for v in vals])
+    M = tuple(int(v) for v in g["M"])
+    box = tuple(float(v) for v in g["box"])
+    s1, _, rc = oracle.gse_params(float(g["sigma"]))
+    x32 = np.asarray(g["xyzq"], dtype=np.float32)
+    rho = np.array(rows["RFF"], dtype=np.float32).reshape(M[2], M[1], M[0])
+    phi = np.array(rows["PHI"], dtype=np.float32).reshape(M[2], M[1], M[0])
+    F = np.array(rows["FFF"])
+    want_rho = oracle.spread(M, box, s1, rc, x32, dtype=np.float32)
+    assert np.abs(rho - want_rho).max() <= 1e-5 * np.abs(want_rho).max()
+    want_F = np.stack(oracle.gather(M, box, s1, rc, x32, phi, dtype=np.float32), axis=1)
+    assert F.shape == want_F.shape and rms(F, want_F) <= 1e-5

@@ -87,3 +87,28 @@ def test_erms_is_the_oracle_force_rms():
     R = rng.standard_normal((50, 3))
     F = R + 1e-3 * rng.standard_normal((50, 3))
     assert abs(Erms(50, *R.T, *F.T) - oracle.force_rms(F, R)) <= 1e-15
+
+
+def _grid_values(dtype):
+    rng = np.random.default_rng(11)
+    v = rng.standard_normal(4 * 3 * 5) * 10.0 ** rng.integers(-8, 9, 4 * 3 * 5)
+    v[:9] = VALUES
+    v[9:13] = [1e-5, 1e-4, 99999.95, 100000.5]  # where %g switches notation / rounds up
+    return v.astype(dtype).reshape(5, 3, 4)  # [z][y][x]: sizeX 4, sizeY 3, sizeZ 5
+
+
+def test_grid_save_is_the_reference_writer(tmp_path, oracle_lib):
+    """CpuGrid::save of the Python mirror writes the bytes of the reference's
+    own header-only writer (CpuGrid.h:76-90, compiled into the oracle's
+    reference build), in both calculation types, on a non-cubic grid."""
+    if not oracle_lib.have_reference():
+        import pytest
+        pytest.skip("reference build not present")
+    from gse_b200.gse import CpuGrid
+    for dt in (np.float64, np.float32):
+        v = _grid_values(dt)
+        oracle_lib.ref_grid_save(v, tmp_path / "g_ref.txt")
+        g = CpuGrid(4, 3, 5, dtype=dt)
+        g.data[...] = v
+        g.save(tmp_path / "g_py.txt")
+        assert (tmp_path / "g_py.txt").read_bytes() == (tmp_path / "g_ref.txt").read_bytes(), dt
