@@ -58,6 +58,42 @@ def algorithmic_bytes(stage: str, precision: str) -> float:
     raise ValueError(stage)
 
 
+# algorithmic flops per launch (262,143 charges, M = 144, stencil 13): the
+# spread adds 2197 cube points per atom (multiply and add), the gather visits
+# 704.5 points per atom inside the cut-off sphere on average (8 flops each:
+# the weight, its products with the potential and the three offsets)
+GATHER_POINTS_PER_ATOM = 704.5
+
+
+def algorithmic_flops(stage: str) -> float:
+    if stage == "spread":
+        return N_ATOMS * 13 ** 3 * 2.0
+    if stage == "gather":
+        return N_ATOMS * GATHER_POINTS_PER_ATOM * 8.0
+    raise ValueError(stage)
+
+
+# what limits each kernel, from the committed full ncu capture of the
+# benchmark workload (profiles/spread_gather_water262k_mixed_full.md)
+LIMITER = {
+    "gather": "instruction issue at low occupancy (ncu: 509 warp instructions per atom, "
+              "61% issue-active, 16 warps per SM); FP32 lanes are the arithmetic roofline",
+    "spread": "shared-memory integer atomics and instruction issue (ncu: 440 warp "
+              "instructions per atom, 73% issue-active)",
+}
+
+
+def fp32_peak(device: int):
+    """FP32 fma rate sustained now on this GPU (TFLOP/s), measured by the
+    library's own probe kernel (CUDA events, scalar and packed forms)."""
+    import ctypes
+    from gse_b200 import _lib
+    L = _lib.load()
+    t, tp = ctypes.c_double(), ctypes.c_double()
+    _lib.check(L.gse_measure_fp32_rate(device, None, ctypes.addressof(t), ctypes.addressof(tp)))
+    return max(t.value, tp.value), {"scalar_tflops": t.value, "packed_tflops": tp.value}
+
+
 def hbm_peak():
     try:
         with open(PEAKS_FILE) as f:
@@ -546,6 +582,12 @@ def main():
         dom_ms = stage[dom][0] / max(stage[dom][1], 1)
         ab = algorithmic_bytes(dom, prec)
         achieved = ab / (dom_ms / 1000.0) / 1e9
+        af = algorithmic_flops(dom)
+        achieved_tf = af / (dom_ms / 1000.0) / 1e12
+        try:
+            fpeak, fpeak_forms = fp32_peak(local)
+        except Exception as exc:  # noqa: BLE001
+            fpeak, fpeak_forms = None, {"failed": str(exc)}
         traffic = None
         prof = os.path.join(ROOT, "profiles", "traffic_water262k.txt")
         if os.path.exists(prof):
@@ -594,10 +636,15 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "kernel": dom,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": ab, "launch_ms": dom_ms},
+            "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": fpeak,
+                         "unit": "TFLOP/s", "frac": achieved_tf / fpeak if fpeak else None,
+                         "traffic": traffic, "kernel": dom,
+                         "peak_source": "measured in this run (gse_measure_fp32_rate)",
+                         "peak_forms": fpeak_forms, "algorithmic_flops_per_launch": af,
+                         "launch_ms": dom_ms, "limiter": LIMITER.get(dom),
+                         "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "peak_source": peak_kind,
+                                 "algorithmic_bytes_per_launch": ab}},
             "cpu_baseline": cpu,
             "clocks": clock_info,
             "stage_ms": per_stage,

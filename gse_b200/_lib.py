@@ -102,6 +102,7 @@ SIGNATURES = {
     "gse_ewald_direct": (_i, [_i, _vp, _d, _d, _d, _d, _d, _d, _i, _vp, _i, _vp, _vp, _vp, _vp,
                               _vp, _vp]),
     "gse_get_paths": (_i, [_vp, ctypes.POINTER(_i)]),
+    "gse_measure_fp32_rate": (_i, [_i, _vp, _vp, _vp]),
     "gse_batch_create": (_i, [ctypes.POINTER(gse_params_t), _i, ctypes.POINTER(gse_system_t),
                               ctypes.POINTER(_vp)]),
     "gse_batch_destroy": (_i, [_vp]),

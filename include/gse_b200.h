@@ -300,6 +300,15 @@ gse_status_t gse_set_timing(gse_context_t* ctx, int enable);
  * (arrays of GSE_NUM_STAGES; either may be NULL); reset != 0 zeroes them. */
 gse_status_t gse_get_timing(gse_context_t* ctx, double* ms_total, long long* counts, int reset);
 
+/* The FP32 fused multiply-add rate this GPU sustains now, in TFLOP/s (2 flops
+ * per fma), from a few ms of independent fmas on every SM: *tflops for the
+ * scalar instruction, *tflops_packed (may be NULL) for the packed two-lane
+ * form.  The spread and gather are bound by FP32 arithmetic and instruction
+ * issue rather than by HBM; this is the denominator of their roofline.
+ * Synchronises `stream` (a cudaStream_t on `device`). */
+gse_status_t gse_measure_fp32_rate(int device, void* stream, double* tflops,
+                                   double* tflops_packed);
+
 /* Number of this library's own CUDA kernels the context has launched
  * (library calls such as cuFFT's are not counted). */
 gse_status_t gse_get_launch_count(gse_context_t* ctx, long long* launches);

@@ -19,6 +19,28 @@ def test_algorithmic_bytes():
         bench.algorithmic_bytes("fft", "mixed")
 
 
+def test_algorithmic_flops():
+    """The spread's 13^3 points x 2 flops and the gather's 704.5 in-sphere points
+    x 8 flops per atom (the gather's mean point count, checked here against the
+    reference's sphere test on seeded atom offsets)."""
+    import numpy as np
+    import bench
+    n = 262143
+    assert bench.algorithmic_flops("spread") == n * 2197 * 2
+    assert bench.algorithmic_flops("gather") == n * 704.5 * 8
+    rng = np.random.default_rng(4)
+    h, rc = 140.0 / 144, 3.0 * np.sqrt(2.0) * 2.0 * np.sqrt(0.4)
+    k = np.arange(13) - 6
+    cnt = []
+    for _ in range(300):
+        d = [(k - o) * h for o in rng.uniform(-0.5, 0.5, 3)]
+        r2 = d[0][None, None, :] ** 2 + d[1][None, :, None] ** 2 + d[2][:, None, None] ** 2
+        cnt.append((r2 < rc * rc).sum())
+    assert abs(np.mean(cnt) - bench.GATHER_POINTS_PER_ATOM) < 5.0
+    with pytest.raises(ValueError):
+        bench.algorithmic_flops("fft")
+
+
 def test_traffic_file_has_the_dominant_kernels():
     """bench.py reads 'kernel precision bytes' lines; the gather's cold-cache
     DRAM bytes stay below its algorithmic bytes (nothing re-read)."""
