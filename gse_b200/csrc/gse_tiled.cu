@@ -669,33 +669,44 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   // rcut^2 -- for every atom when n h exceeds rcut by more than rounding
   constexpr int NI = (W - 1) * (W - 1);
   constexpr int NGI = (NI + GL - 1) / GL;  // groups that hold the inner rows
-  int gjy[NG], gjz[NG];
-#pragma unroll
-  for (int g = 0; g < NG; g++) {
-    const int r = g * GL + gl;
+  // (jy, jz) of candidate row r (formed where it is used: a table of them
+  // would hold 2 NG registers through the whole atom loop)
+  auto cand = [&](int r, int& jy, int& jz) {
     if (r < NI) {
-      gjz[g] = 1 + r / (W - 1);
-      gjy[g] = 1 + r % (W - 1);
+      jz = 1 + r / (W - 1);
+      jy = 1 + r % (W - 1);
     } else if (r < NI + W) {
-      gjz[g] = r - NI;
-      gjy[g] = 0;
+      jz = r - NI;
+      jy = 0;
     } else if (r < W * W) {
-      gjz[g] = 0;
-      gjy[g] = r - NI - W + 1;
+      jz = 0;
+      jy = r - NI - W + 1;
     } else {
-      gjz[g] = gjy[g] = 0;
+      jz = jy = 0;
     }
-  }
+  };
   const unsigned gmask = GL == 32 ? 0xffffffffu : ((1u << GL) - 1u);
   for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
     brick_atom_list<kGatherThreads, NR>(rng_a, rng_p, natoms, c0, kGatherList, alist);
     __syncthreads();
     const int nc = min(kGatherList, natoms - c0);
+    // the next atom's record and output slot are loaded one iteration ahead,
+    // so their global-memory latency overlaps the current atom's work
+    int ai_n = 0, o_n = 0;
+    V a_n;
+    auto fetch = [&](int qq0) {
+      const int qq = qq0 + grp;
+      ai_n = alist[qq < nc ? qq : qq0];
+      a_n = sorted[ai_n];
+      o_n = perm[ai_n];
+    };
+    if (APW * warp < nc) fetch(APW * warp);
     for (int q0 = APW * warp; q0 < nc; q0 += APW * NW) {
       const int q = q0 + grp;
       const bool valid = q < nc;  // the last group of a chunk may have no atom
-      const int ai = alist[valid ? q : q0];
-      const V a = sorted[ai];
+      const V a = a_n;
+      const int out_slot = o_n;
+      if (q0 + APW * NW < nc) fetch(q0 + APW * NW);
       const CT pos3[3] = {a.x, a.y, a.z};
       const int org[3] = {x0, y0, z0};
       int loc[3];
@@ -723,12 +734,13 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
       for (int g = 0; g < NG; g++) {
         if (g >= NGI && !edges) break;  // warp-uniform
         const int r = g * GL + gl;
+        int jy, jz;
+        cand(r, jy, jz);
         bool ne = false;
         if (r < W * W)
-          ne = add_rn(tb[(1 * 3 + 1) * kWPad + gjy[g]], tb[(2 * 3 + 1) * kWPad + gjz[g]]) <
-               s.rcut2;
+          ne = add_rn(tb[(1 * 3 + 1) * kWPad + jy], tb[(2 * 3 + 1) * kWPad + jz]) < s.rcut2;
         const unsigned m = (__ballot_sync(0xffffffffu, ne) >> (GL * grp)) & gmask;
-        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = (gjz[g] << 8) | gjy[g];
+        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = (jz << 8) | jy;
         nrow += __popc(m);
       }
       __syncwarp();
@@ -779,11 +791,10 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         az += __shfl_xor_sync(0xffffffffu, az, o);
       }
       if (gl == 0 && valid) {
-        const int o = perm[ai];
         const double f = outscale * (double)(a.w * s.pref);
-        fx[o] = f * ax;
-        fy[o] = f * ay;
-        fz[o] = f * az;
+        fx[out_slot] = f * ax;
+        fy[out_slot] = f * ay;
+        fz[out_slot] = f * az;
       }
       __syncwarp();
     }
