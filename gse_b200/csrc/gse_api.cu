@@ -210,6 +210,9 @@ struct gse_context {
   cudaGraphExec_t fwd_exec = nullptr;
   long long fwd_launches = 0;
   bool fwd_graphs = true;
+  // classification of the pointers of the captured call, for the replay path
+  bool fwd_host_io = false, fwd_e_host = false;
+  const double* fwd_e_raw = nullptr;
   // optional per-stage device timing (gse_set_timing)
   bool timing = false;
   cudaEvent_t ev[GSE_NUM_STAGES][2] = {};
@@ -655,13 +658,16 @@ gse_status_t gather_to(gse_context_t* c, int n, const void* dx, const double box
   if (direct)
     return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz, presorted);
   double* f = c->d_force;
-  const size_t cap = c->atom_cap;
-  TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + cap, f + 2 * cap,
+  // three outputs that are consecutive rows of one [3][n] array take one copy
+  const bool rows = fx && fy == fx + n && fz == fx + 2 * (size_t)n;
+  const size_t stride = rows ? (size_t)n : c->atom_cap;
+  TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + stride, f + 2 * stride,
                     presorted));
   if (n == 0) return GSE_OK;
+  if (rows) return copy_out(c, fx, f, 3 * (size_t)n * sizeof(double), host);
   if (fx) TRY(copy_out(c, fx, f, n * sizeof(double), host));
-  if (fy) TRY(copy_out(c, fy, f + cap, n * sizeof(double), host));
-  if (fz) TRY(copy_out(c, fz, f + 2 * cap, n * sizeof(double), host));
+  if (fy) TRY(copy_out(c, fy, f + stride, n * sizeof(double), host));
+  if (fz) TRY(copy_out(c, fz, f + 2 * stride, n * sizeof(double), host));
   return GSE_OK;
 }
 
@@ -1063,6 +1069,29 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
 gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* energy, double* fx,
                          double* fy, double* fz) {
   TRY(check_ctx(c));
+  // A repeat of the captured call (same count, positions, forces, box and
+  // stream) replays its graph: its pointers were checked and classified when
+  // it was captured.  Only a host energy may change address between calls.
+  const gse_context_t::FwdKey& k = c->fwd_key;
+  if (c->fwd_exec && !c->timing && n == k.n && xyzq == k.x && fx == k.fx && fy == k.fy &&
+      fz == k.fz && c->stream == k.stream && c->p.box_x == k.box[0] && c->p.box_y == k.box[1] &&
+      c->p.box_z == k.box[2]) {
+    bool he = c->fwd_e_host;
+    if (energy != c->fwd_e_raw) {
+      TRY(check_ptr(energy, c->p.device, 1, "energy"));
+      he = energy && !is_device_ptr(energy);
+    }
+    if ((he ? reinterpret_cast<double*>(uintptr_t(1)) : energy) == k.e) {
+      CU(cudaGraphLaunch(c->fwd_exec, c->stream));
+      c->launches += c->fwd_launches;
+      c->rho_valid = c->phi_valid = c->energy_valid = true;
+      c->fwd_e_raw = energy;
+      c->fwd_e_host = he;
+      TRY(finish(c, c->fwd_host_io));
+      if (he) *energy = c->h_pinned[0];
+      return GSE_OK;
+    }
+  }
   TRY(check_ptr(xyzq, c->p.device, 4 * c->ct, "xyzq"));
   TRY(check_ptr(energy, c->p.device, 1, "energy"));
   TRY(check_xyz(c->p.device, fx, fy, fz, "force array"));
@@ -1137,6 +1166,9 @@ gse_status_t gse_forward(gse_context_t* c, int n, const void* xyzq, double* ener
     const cudaError_t ei = cudaGraphInstantiate(&c->fwd_exec, g, 0);
     if (ei == cudaSuccess) {
       c->fwd_launches = c->launches - l0;
+      c->fwd_host_io = host_io;
+      c->fwd_e_host = host_e;
+      c->fwd_e_raw = energy;
       const cudaError_t el = cudaGraphLaunch(c->fwd_exec, c->stream);
       if (el != cudaSuccess) result = fail(GSE_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(el));
     } else {
