@@ -262,7 +262,9 @@ def run_reference_arm(args):
 def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
     """The batching workload: 256 independent triplet systems, N log-uniform in
     [501, 8001], forward + reverse pass replayed from one CUDA graph after the
-    autotuner has picked the persistent-CTA counts and the work order.  With
+    autotuner has picked the launch schedule (per stage or one persistent
+    kernel per direction, CTA counts, lanes per atom, work order); the schedule
+    it did not keep is timed too, for the record.  With
     several ranks the systems are partitioned across them (no collective on the
     data path); every rank times its share, and the rate is the 256 systems over
     the slowest rank's time.  All ranks must call it."""
@@ -289,24 +291,50 @@ def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
     bufs["grad_forces"].copy_(torch.from_numpy(np.ascontiguousarray(G.T)))
     stream = torch.cuda.current_stream()
     b.set_stream(stream.cuda_stream)
-    b.capture(with_adjoint=True)
-    for _ in range(warmup):
-        b.launch()
-    torch.cuda.synchronize()
-    multi.barrier()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    for k in range(steps):
-        flush.zero_()
-        starts[k].record(stream)
-        b.launch()
-        ends[k].record(stream)
-    torch.cuda.synchronize()
-    multi.barrier()
-    ms = multi.max_over_ranks(sum(a.elapsed_time(c) for a, c in zip(starts, ends)) / steps,
-                              device=torch.device("cuda", torch.cuda.current_device()))
+
+    def timed_graph():
+        """Capture forward + reverse into one graph, replay it `steps` times
+        (L2 flushed before each), max over ranks of the mean device time."""
+        b.capture(with_adjoint=True)
+        for _ in range(warmup):
+            b.launch()
+        torch.cuda.synchronize()
+        multi.barrier()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            b.launch()
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        multi.barrier()
+        return multi.max_over_ranks(sum(a.elapsed_time(c) for a, c in zip(starts, ends)) / steps,
+                                    device=torch.device("cuda", torch.cuda.current_device()))
+
+    def schedule(i):
+        if i.fused:
+            return {"launches": "one persistent cooperative kernel per direction",
+                    "graph_kernel_nodes": int(i.graph_kernels),
+                    "gather_lanes_per_atom": int(i.gather_lanes), "ctas": int(i.fused_ctas),
+                    "largest_first": bool(i.largest_first)}
+        return {"launches": "per stage", "graph_kernel_nodes": int(i.graph_kernels),
+                "scatter_ctas": int(i.scatter_ctas), "gather_ctas": int(i.gather_ctas),
+                "largest_first": bool(i.largest_first)}
+
+    ms = timed_graph()
+    i = b.info()  # after capture: the graph's kernel-node count
+    chosen = schedule(i)
+    # the schedule the autotuner did not keep, timed the same way for the record
+    other = None
+    if i.fused_available:
+        if i.fused:
+            b.set_schedule(fused=False)
+        else:
+            b.set_schedule(fused=True, gather_lanes=16, largest_first=bool(i.largest_first))
+        ms_other = timed_graph()
+        other = dict(schedule(b.info()), ms_per_step=ms_other)
     n_all = sum(y.n for y in every)
-    i = b.info()
     out = {"workload": "256 independent triplet systems, N log-uniform in [501, 8001], "
                        "M = nearest multiple of 8 to L, sigma 2.0, mixed form",
            "n_total": n_all, "size_classes": int(i.n_size_classes),
@@ -314,8 +342,7 @@ def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
            "ranks": world, "systems_rank0": len(part[0]),
            "ms_per_step": ms, "systems_per_s": 256 / (ms / 1000.0),
            "charges_per_s": n_all / (ms / 1000.0),
-           "autotuned": {"scatter_ctas": int(i.scatter_ctas), "gather_ctas": int(i.gather_ctas),
-                         "largest_first": bool(i.largest_first)}}
+           "autotuned": chosen, "other_schedule": other}
     b.close()
     return out
 

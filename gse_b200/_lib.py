@@ -58,6 +58,8 @@ class gse_batch_info_t(ctypes.Structure):
         ("largest_first", ctypes.c_int),
         ("xyzq", ctypes.c_void_p), ("energies", ctypes.c_void_p), ("forces", ctypes.c_void_p),
         ("dLdE", ctypes.c_void_p), ("grad_forces", ctypes.c_void_p), ("grad_out", ctypes.c_void_p),
+        ("fused", ctypes.c_int), ("gather_lanes", ctypes.c_int), ("fused_ctas", ctypes.c_int),
+        ("graph_kernels", ctypes.c_int), ("fused_available", ctypes.c_int),
     ]
 
 
@@ -113,6 +115,7 @@ SIGNATURES = {
     "gse_batch_capture": (_i, [_vp, _i]),
     "gse_batch_launch": (_i, [_vp]),
     "gse_batch_autotune": (_i, [_vp, ctypes.c_char_p, _i]),
+    "gse_batch_set_schedule": (_i, [_vp, _i, _i, _i, _i, _i]),
 }
 STAGES = ["bin", "spread", "fft_forward", "green", "fft_backward", "gather"]
 

@@ -346,14 +346,15 @@ __device__ __forceinline__ void adj_scatter_brick(
   brick_flush<W, NT>(tile, b, x0, y0, z0, shift, grid64);
 }
 
-// Shared memory of the reverse-pass gather for stencil width W.
-template <int W>
+// Shared memory of the reverse-pass gather for stencil width W and a block of
+// NT threads.
+template <int W, int NT = kAdjThreads>
 struct AdjGatherGeom {
   static constexpr int n = (W - 1) / 2;
   static constexpr int TX = kAX + 2 * n, TY = kAY + 2 * n, TZ = kAZ + 2 * n;
   static constexpr int TP = TX | 1;
   static constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
-  static constexpr int NW = kAdjThreads / 32;
+  static constexpr int NW = NT / 32;
   static constexpr int APW = 32 / kAdjLanes;  // atoms per warp at a time
   static constexpr size_t bytes =
       sizeof(float) * (2 * TZ * ZP + NW * APW * 9 * kWPad) + sizeof(int) * NW * APW * W * W;
@@ -363,7 +364,7 @@ struct AdjGatherGeom {
 // gE c h^3 phi and phi of the brick plus halo in shared memory; kAdjLanes
 // lanes per atom: the cube rows of Psi (moments e, e u_x) and the sphere rows
 // of phi (moments e, e u_x, e u_x^2), combined into dL/dq and dL/dx.
-template <int W>
+template <int W, int NT = kAdjThreads>
 __device__ __forceinline__ void adj_gather_brick(
     const float4* __restrict__ sorted, const int* __restrict__ perm, const int* __restrict__ start,
     const BinLayout& b, const Stencil<float>& sp, const Stencil<float>& sg, double c,
@@ -372,9 +373,9 @@ __device__ __forceinline__ void adj_gather_brick(
     const double* __restrict__ gfz, double* __restrict__ dq, double* __restrict__ dx,
     double* __restrict__ dy, double* __restrict__ dz, int bxi, int byi, int bzi,
     unsigned char* smem) {
-  typedef AdjGatherGeom<W> AG;
+  typedef AdjGatherGeom<W, NT> AG;
   constexpr int n = AG::n, TX = AG::TX, TY = AG::TY, TZ = AG::TZ, TP = AG::TP, ZP = AG::ZP;
-  constexpr int NW = AG::NW, APW = AG::APW, NT = kAdjThreads, GL = kAdjLanes;
+  constexpr int NW = AG::NW, APW = AG::APW, GL = kAdjLanes;
   constexpr int NR = kAY * kAZ;
   constexpr int NG = (W * W + GL - 1) / GL;
   float* tpsi = (float*)smem;                        // [TZ][ZP]
@@ -789,6 +790,127 @@ cudaError_t launch_batch_adj_gather_tiled(const float4* sorted, const int* perm,
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+
+// ---------------------------------------------------------------------------
+// Reverse pass of a batch in one persistent cooperative launch (grids of at
+// most 64 points, multiples of 8, per side): the adjoint source of every
+// system into the int64 grid, its solve with the Green's function, and the
+// reverse-pass gather.  Reads the forward pass's sorted atoms, bins and
+// potential.
+// ---------------------------------------------------------------------------
+constexpr int kFusedRevThreads = 512;
+static_assert(kFusedRevThreads == kScatterThreads, "the fused kernel runs the scatter bricks");
+
+constexpr size_t cmax_rev(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t fused_rev_smem() {
+  return cmax_rev(
+      cmax_rev(cmax_rev(sizeof(int) * ScatterGeom<9>::words, sizeof(int) * ScatterGeom<11>::words),
+               cmax_rev(sizeof(int) * ScatterGeom<13>::words, sizeof(int) * ScatterGeom<15>::words)),
+      cmax_rev(cmax_rev(cmax_rev(AdjGatherGeom<9, kFusedRevThreads>::bytes,
+                                 AdjGatherGeom<11, kFusedRevThreads>::bytes),
+                        cmax_rev(AdjGatherGeom<13, kFusedRevThreads>::bytes,
+                                 AdjGatherGeom<15, kFusedRevThreads>::bytes)),
+               sizeof(SmallFftTw) + sizeof(int) * 3 * (kSfSmemSystems + 1)));
+}
+
+__global__ void __launch_bounds__(kFusedRevThreads, 1) k_batch_reverse_fused(BatchFused a) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  for (long long i = gtid; i < a.gtot; i += gstride) a.g64[i] = 0;
+  if (gtid < 2) a.qctr[2 + gtid] = 0;
+  cg::this_grid().sync();
+  for (int it = fused_next_item(&a.qctr[2]); it < a.nscat; it = fused_next_item(&a.qctr[2])) {
+    const BatchItem item = a.scat[it];
+    const BatchSys& S = a.sys[item.sys];
+    const int* st = a.w.start + S.bin_off;
+    long long* g = a.g64 + S.grid_off;
+    int* tile = reinterpret_cast<int*>(fsm);
+    const float cA = (float)(a.ccelec * (double)S.sg.pref);
+    switch (S.W) {
+      case 9: adj_scatter_brick<9>(a.sorted, a.perm, st, S.b, S.sg, cA, a.gfx, a.gfy, a.gfz,
+                                   item.bx, item.by, item.bz, tile, g); break;
+      case 11: adj_scatter_brick<11>(a.sorted, a.perm, st, S.b, S.sg, cA, a.gfx, a.gfy, a.gfz,
+                                     item.bx, item.by, item.bz, tile, g); break;
+      case 13: adj_scatter_brick<13>(a.sorted, a.perm, st, S.b, S.sg, cA, a.gfx, a.gfy, a.gfz,
+                                     item.bx, item.by, item.bz, tile, g); break;
+      default: adj_scatter_brick<15>(a.sorted, a.perm, st, S.b, S.sg, cA, a.gfx, a.gfy, a.gfz,
+                                     item.bx, item.by, item.bz, tile, g); break;
+    }
+    __syncthreads();
+  }
+  cg::this_grid().sync();
+  fused_solve(a, a.psi, false, fsm);
+  cg::this_grid().sync();
+  for (int it = fused_next_item(&a.qctr[3]); it < a.nagath; it = fused_next_item(&a.qctr[3])) {
+    const BatchItem item = a.agath[it];
+    const BatchSys& S = a.sys[item.sys];
+    const int* st = a.w.start + S.bin_off;
+    const double gE_ch3 = a.dLdE[item.sys] * a.ccelec * S.h3;
+    const float* ps = a.psi + S.grid_off;
+    const float* ph = a.phi + S.grid_off;
+    switch (S.W) {
+#define GSE_FAG(WW)                                                                          \
+  case WW:                                                                                   \
+    adj_gather_brick<WW, kFusedRevThreads>(a.sorted, a.perm, st, S.b, S.sp, S.sg, a.ccelec,  \
+                                           gE_ch3, ps, ph, a.gfx, a.gfy, a.gfz, a.dq, a.dx,  \
+                                           a.dy, a.dz, item.bx, item.by, item.bz, fsm);      \
+    break;
+      GSE_FAG(9)
+      GSE_FAG(11)
+      GSE_FAG(13)
+      default:
+        adj_gather_brick<15, kFusedRevThreads>(a.sorted, a.perm, st, S.b, S.sp, S.sg, a.ccelec,
+                                               gE_ch3, ps, ph, a.gfx, a.gfy, a.gfz, a.dq, a.dx,
+                                               a.dy, a.dz, item.bx, item.by, item.bz, fsm);
+        break;
+#undef GSE_FAG
+    }
+    __syncthreads();
+  }
+}
+
+int batch_fused_rev_ctas() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 0;
+  }
+  int v = cache[dev].load();
+  if (v == 0) {
+    const size_t smem = fused_rev_smem();
+    int nb = 0;
+    if (cudaFuncSetAttribute(k_batch_reverse_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_reverse_fused,
+                                                      kFusedRevThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      nb = 0;
+    }
+    v = nb > 0 ? nb * sm_count() : -1;
+    cache[dev].store(v);
+  }
+  return v > 0 ? v : 0;
+}
+
+cudaError_t launch_batch_reverse_fused(const BatchFused& a, int ctas, cudaStream_t st) {
+  const int most = batch_fused_rev_ctas();
+  if (most <= 0 || ctas < 1 || ctas > most) return cudaErrorCooperativeLaunchTooLarge;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kFusedRevThreads);
+  cfg.dynamicSmemBytes = fused_rev_smem();
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_batch_reverse_fused, a);
 }
 
 cudaError_t launch_batch_adj_source(const float4* xyzq, const int* perm, int ntot,

@@ -87,6 +87,14 @@ struct gse_batch {
   double* d_gout = nullptr;    // 4 x ntot
   int scat_ctas = 0, gath_ctas = 0, agath_ctas = 0;
   bool largest_first = false;
+  // one persistent cooperative launch per direction (grids that are multiples
+  // of 8 and at most 64 points per side); otherwise the per-stage launches
+  bool fused = false, fused_ok = false;
+  int fused_ctas = 0, gather_lanes = 16;
+  int graph_kernels = 0;  // kernel nodes of the captured graph
+  int* d_line_first = nullptr;  // [3][nsys + 1]: x rows, y columns, z columns
+  int* d_qctr = nullptr;        // [4] work-item counters of the fused launches
+  double* d_epart = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
 };
@@ -199,9 +207,59 @@ gse_status_t upload_items(gse_batch_t* b) {
   return GSE_OK;
 }
 
+// Arguments of the fused launches on the batch's buffers.
+BatchFused fused_args(const gse_batch_t* b) {
+  BatchFused a{};
+  a.xyzq = b->d_xyzq;
+  a.ntot = b->ntot;
+  a.nsys = b->nsys;
+  a.nbins = b->nbins;
+  a.sys = b->d_sys;
+  a.first = b->d_first;
+  a.w = BinScratch{b->d_key, b->d_counts, b->d_start, b->d_tiles, b->d_tmp, b->d_qmax};
+  a.sorted = b->d_sorted;
+  a.perm = b->d_perm;
+  a.scat = b->d_scat;
+  a.nscat = (int)b->scat.size();
+  a.gath = b->d_gath;
+  a.ngath = (int)b->gath.size();
+  a.agath = b->d_agath;
+  a.nagath = (int)b->agath.size();
+  a.g64 = b->d_g64;
+  a.gtot = b->gtot;
+  a.rhok = b->d_rhok;
+  a.gtab = b->d_gtab;
+  a.phi = b->d_phi;
+  a.psi = b->d_lam;
+  a.qctr = b->d_qctr;
+  a.xrow_first = b->d_line_first;
+  a.ycol_first = b->d_line_first + (b->nsys + 1);
+  a.zcol_first = b->d_line_first + 2 * (b->nsys + 1);
+  a.epart = b->d_epart;
+  a.energy = b->d_energy;
+  a.ccelec = b->p.ccelec;
+  a.fx = b->d_forces;
+  a.fy = b->d_forces + b->ntot;
+  a.fz = b->d_forces + 2 * (long long)b->ntot;
+  a.dLdE = b->d_dLdE;
+  const long long nt = b->ntot;
+  a.gfx = b->d_gin;
+  a.gfy = b->d_gin + nt;
+  a.gfz = b->d_gin + 2 * nt;
+  a.dq = b->d_gout;
+  a.dx = b->d_gout + nt;
+  a.dy = b->d_gout + 2 * nt;
+  a.dz = b->d_gout + 3 * nt;
+  return a;
+}
+
 // One batched evaluation on the batch's device buffers (all on b->stream).
 gse_status_t run_forward(gse_batch_t* b) {
   cudaStream_t st = b->stream;
+  if (b->fused) {
+    BCU(launch_batch_forward_fused(fused_args(b), b->fused_ctas, b->gather_lanes, st));
+    return GSE_OK;
+  }
   BinScratch w{b->d_key, b->d_counts, b->d_start, b->d_tiles, b->d_tmp, b->d_qmax};
   BCU(launch_batch_bin(b->d_xyzq, b->ntot, b->d_sys, b->d_first, b->nsys, b->nbins, w,
                        b->d_sorted, b->d_perm, st));
@@ -224,6 +282,10 @@ gse_status_t run_forward(gse_batch_t* b) {
 // Reverse pass after run_forward: uses d_dLdE and d_gin, writes d_gout.
 gse_status_t run_adjoint(gse_batch_t* b) {
   cudaStream_t st = b->stream;
+  if (b->fused) {
+    BCU(launch_batch_reverse_fused(fused_args(b), b->fused_ctas, st));
+    return GSE_OK;
+  }
   const long long nt = b->ntot;
   BCU(launch_batch_adj_scatter(b->d_sorted, b->d_perm, b->d_start, b->d_sys, b->d_scat,
                                b->scat_seg.data(), (int)b->scat_seg.size(), b->scat_ctas,
@@ -266,7 +328,7 @@ std::string tune_key(const gse_batch_t* b) {
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->dev);
   char buf[64];
-  std::string k = "batch";
+  std::string k = b->fused_ok ? "batchf" : "batch";
   snprintf(buf, sizeof(buf), "-n%d-N%d-sm%d", b->nsys, (int)std::log2((double)b->ntot + 1), sms);
   k += buf;
   for (auto& kv : hist) {
@@ -444,6 +506,36 @@ gse_status_t gse_batch_create(const gse_params_t* common, int nsys, const gse_sy
   b->scat_ctas = 2 * sms;
   b->gath_ctas = 2 * sms;
   b->agath_ctas = 2 * sms;
+  // the fused launches are available when every grid side is a multiple of 8
+  // and at most 64 and the cooperative grid can be resident
+  // (GSE_B200_BATCH_FUSED=0 withholds them); the batch starts on the per-stage
+  // launches, the autotuner or gse_batch_set_schedule may switch
+  {
+    const char* env = getenv("GSE_B200_BATCH_FUSED");
+    const bool allowed = !(env && env[0] == '0');
+    const int fc = std::min(batch_fused_ctas(16), batch_fused_rev_ctas());
+    if (allowed && fc > 0 && batch_fused_supported(b->sys.data(), nsys)) {
+      // line counts of the FFT passes: x rows My Mz, y columns Mz Hx, z columns My Hx
+      std::vector<int> lf(3 * (nsys + 1), 0);
+      for (int k = 0; k < nsys; k++) {
+        const int* M = b->sys[k].b.M;
+        const int hx = M[0] / 2 + 1;
+        lf[k + 1] = lf[k] + M[1] * M[2];
+        lf[(nsys + 1) + k + 1] = lf[(nsys + 1) + k] + M[2] * hx;
+        lf[2 * (nsys + 1) + k + 1] = lf[2 * (nsys + 1) + k] + M[1] * hx;
+      }
+      BCUC(cudaMalloc(&b->d_line_first, sizeof(int) * lf.size()));
+      BCUC(cudaMemcpy(b->d_line_first, lf.data(), sizeof(int) * lf.size(),
+                      cudaMemcpyHostToDevice));
+      BCUC(cudaMalloc(&b->d_epart, sizeof(double) * std::max(lf[3 * (nsys + 1) - 1], 1)));
+      BCUC(cudaMalloc(&b->d_qctr, sizeof(int) * 4));
+      BCUC(cudaMemset(b->d_qctr, 0, sizeof(int) * 4));
+      b->fused_ok = true;
+      b->fused_ctas = fc;
+      b->gather_lanes = 16;
+    }
+    cudaGetLastError();
+  }
   order_items(b, true);
   BCUC(cudaMalloc(&b->d_scat, sizeof(BatchItem) * std::max<size_t>(b->scat.size(), 1)));
   BCUC(cudaMalloc(&b->d_gath, sizeof(BatchItem) * std::max<size_t>(b->gath.size(), 1)));
@@ -464,7 +556,8 @@ gse_status_t gse_batch_destroy(gse_batch_t* b) {
     if (c.pf) cufftDestroy(c.pf);
     if (c.pb) cufftDestroy(c.pb);
   }
-  void* ptrs[] = {b->d_sys, b->d_first, b->d_kfirst, b->d_ksys, b->d_scat, b->d_gath, b->d_agath,
+  void* ptrs[] = {b->d_line_first, b->d_epart, b->d_qctr,
+                  b->d_sys, b->d_first, b->d_kfirst, b->d_ksys, b->d_scat, b->d_gath, b->d_agath,
                   b->d_xyzq, b->d_sorted, b->d_perm, b->d_key, b->d_tmp, b->d_counts,
                   b->d_start, b->d_tiles, b->d_qmax, b->d_g64, b->d_rho, b->d_phi, b->d_lam,
                   b->d_rhok, b->d_gtab, b->d_energy, b->d_dLdE, b->d_forces, b->d_gin,
@@ -498,6 +591,11 @@ gse_status_t gse_batch_info(gse_batch_t* b, gse_batch_info_t* info) {
   info->dLdE = b->d_dLdE;
   info->grad_forces = b->d_gin;
   info->grad_out = b->d_gout;
+  info->fused = b->fused ? 1 : 0;
+  info->fused_available = b->fused_ok ? 1 : 0;
+  info->gather_lanes = b->fused ? b->gather_lanes : kGatherLanes;
+  info->fused_ctas = b->fused ? b->fused_ctas : 0;
+  info->graph_kernels = b->gexec ? b->graph_kernels : 0;
   return GSE_OK;
 }
 
@@ -598,6 +696,21 @@ gse_status_t gse_batch_capture(gse_batch_t* b, int with_adjoint) {
     const cudaError_t ei = cudaGraphInstantiate(&b->gexec, g, 0);
     if (ei != cudaSuccess) s = set_error(GSE_ERR_CUDA, cudaGetErrorString(ei));
   }
+  // kernel nodes of the captured graph (library FFT kernels included)
+  b->graph_kernels = 0;
+  if (s == GSE_OK) {
+    size_t nn = 0;
+    if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+        for (size_t i = 0; i < nn; i++) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            b->graph_kernels++;
+        }
+    }
+    cudaGetLastError();
+  }
   b->graph = g;
   if (own) {
     set_stream_all(b, old);
@@ -615,73 +728,104 @@ gse_status_t gse_batch_launch(gse_batch_t* b) {
   return GSE_OK;
 }
 
+gse_status_t gse_batch_set_schedule(gse_batch_t* b, int fused, int gather_lanes,
+                                    int largest_first, int scatter_ctas, int gather_ctas) {
+  if (!b) return set_error(GSE_ERR_INVALID_ARG, "NULL batch");
+  if (fused && !b->fused_ok)
+    return set_error(GSE_ERR_UNSUPPORTED,
+                     "the fused launch needs every grid side a multiple of 8 and at most 64");
+  if (fused && gather_lanes != 8 && gather_lanes != 16)
+    return set_error(GSE_ERR_INVALID_ARG, "gather lanes per atom must be 8 or 16");
+  if (!fused && (scatter_ctas < 1 || gather_ctas < 1))
+    return set_error(GSE_ERR_INVALID_ARG, "persistent CTA counts must be positive");
+  BCU(cudaSetDevice(b->dev));
+  b->fused = fused != 0;
+  if (b->fused) {
+    b->gather_lanes = gather_lanes;
+    b->fused_ctas = std::min(batch_fused_ctas(gather_lanes), batch_fused_rev_ctas());
+  } else {
+    b->scat_ctas = scatter_ctas;
+    b->gath_ctas = gather_ctas;
+    b->agath_ctas = gather_ctas;
+  }
+  order_items(b, largest_first != 0);
+  drop_graph(b);
+  return upload_items(b);
+}
+
 gse_status_t gse_batch_autotune(gse_batch_t* b, const char* cache_path, int use_cache) {
   if (!b) return set_error(GSE_ERR_INVALID_ARG, "NULL batch");
   BCU(cudaSetDevice(b->dev));
   const std::string key = tune_key(b);
-  // cached choice?
+  // cached choice?  One line per key: lf fused gl sc gc ms
   if (use_cache && cache_path) {
     FILE* f = fopen(cache_path, "r");
     if (f) {
       char k[512];
-      int lf, sc, gc;
+      int lf, fu, gl, sc, gc;
       double ms;
       bool found = false;
-      while (fscanf(f, "%511s %d %d %d %lf", k, &lf, &sc, &gc, &ms) == 5) {
-        if (key == k) {
+      while (fscanf(f, "%511s %d %d %d %d %d %lf", k, &lf, &fu, &gl, &sc, &gc, &ms) == 7)
+        if (key == k && (!fu || b->fused_ok)) {
           found = true;
-          b->scat_ctas = sc;
-          b->gath_ctas = gc;
-          order_items(b, lf != 0);
+          BTRY(gse_batch_set_schedule(b, fu, gl, lf, sc, gc));
         }
-      }
       fclose(f);
-      if (found) {
-        drop_graph(b);
-        return upload_items(b);
-      }
+      if (found) return GSE_OK;
     }
   }
+  // every schedule on a forward and a reverse pass of the batch's current
+  // inputs: the per-stage launches (work-item order x persistent CTAs of the
+  // spread and gather kernels) and, where the grids allow it, the fused
+  // launches (work-item order x lanes per atom of the gather)
+  struct Cand {
+    int lf, fused, gl, sc, gc;
+  };
+  std::vector<Cand> cands;
   const int sms = sm_count();
+  for (int lf = 0; lf < 2; lf++) {
+    for (int sc : {sms, 2 * sms})
+      for (int gc : {sms, 2 * sms, 4 * sms}) cands.push_back({lf, 0, kGatherLanes, sc, gc});
+    if (b->fused_ok)
+      for (int gl : {16, 8})
+        if (batch_fused_ctas(gl) > 0) cands.push_back({lf, 1, gl, 2 * sms, 2 * sms});
+  }
   cudaEvent_t e0, e1;
   BCU(cudaEventCreate(&e0));
   BCU(cudaEventCreate(&e1));
   double best = 1e30;
-  int bsc = b->scat_ctas, bgc = b->gath_ctas;
-  bool blf = b->largest_first;
-  for (int lf = 0; lf < 2; lf++) {
-    order_items(b, lf != 0);
-    BTRY(upload_items(b));
-    for (int sc : {sms, 2 * sms})
-      for (int gc : {sms, 2 * sms, 4 * sms}) {
-        b->scat_ctas = sc;
-        b->gath_ctas = gc;
-        BTRY(run_forward(b));  // warm
-        BCU(cudaEventRecord(e0, b->stream));
-        for (int r = 0; r < 3; r++) BTRY(run_forward(b));
-        BCU(cudaEventRecord(e1, b->stream));
-        BCU(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        BCU(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms / 3.0 < best) {
-          best = ms / 3.0;
-          bsc = sc;
-          bgc = gc;
-          blf = lf != 0;
-        }
-      }
+  Cand bc = cands[0];
+  gse_status_t st = GSE_OK;
+  for (const Cand& c : cands) {
+    st = gse_batch_set_schedule(b, c.fused, c.gl, c.lf, c.sc, c.gc);
+    if (st != GSE_OK) break;
+    if ((st = run_forward(b)) != GSE_OK || (st = run_adjoint(b)) != GSE_OK) break;  // warm
+    cudaEventRecord(e0, b->stream);
+    for (int r = 0; r < 3 && st == GSE_OK; r++) {
+      st = run_forward(b);
+      if (st == GSE_OK) st = run_adjoint(b);
+    }
+    cudaEventRecord(e1, b->stream);
+    if (st != GSE_OK) break;
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      st = set_error(GSE_ERR_CUDA, "autotune timing failed");
+      break;
+    }
+    if (ms / 3.0 < best) {
+      best = ms / 3.0;
+      bc = c;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->scat_ctas = bsc;
-  b->gath_ctas = bgc;
-  order_items(b, blf);
-  BTRY(upload_items(b));
-  drop_graph(b);
+  if (st != GSE_OK) return st;
+  BTRY(gse_batch_set_schedule(b, bc.fused, bc.gl, bc.lf, bc.sc, bc.gc));
   if (cache_path) {
     FILE* f = fopen(cache_path, "a");
     if (f) {
-      fprintf(f, "%s %d %d %d %.6f\n", key.c_str(), blf ? 1 : 0, bsc, bgc, best);
+      fprintf(f, "%s %d %d %d %d %d %.6f\n", key.c_str(), bc.lf, bc.fused, bc.gl, bc.sc, bc.gc,
+              best);
       fclose(f);
     }
   }

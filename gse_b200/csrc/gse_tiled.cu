@@ -21,7 +21,10 @@
 #include <atomic>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "gse_internal.cuh"
+#include "gse_smallfft.cuh"
 #include "gse_tiled.cuh"
 #include "gse_tiled_dev.cuh"
 
@@ -593,7 +596,7 @@ __device__ __forceinline__ void row_sums(const CT* row, const CT (&dx2)[W], cons
 // Shared memory of the gather for calculation type CT and stencil width W:
 // the potential tile [TZ][ZP] (rows of pitch TP), per-atom weight tables and
 // per-atom row lists.
-template <typename CT, int W>
+template <typename CT, int W, int NT = kGatherThreads, int GL = kGatherLanes>
 struct GatherGeom {
   static constexpr int n = (W - 1) / 2;
   static constexpr int TX = kGX + 2 * n, TY = kGY + 2 * n, TZ = kGZ + 2 * n;
@@ -601,17 +604,18 @@ struct GatherGeom {
   // plane pitch = W*TP (mod 32): row (jy, jz) starts in bank TP*(jy + W*jz)
   // mod 32, distinct for 32 consecutive (jy, jz)
   static constexpr int ZP = ((TY * TP + 31) / 32) * 32 + ((W * TP) % 32);
-  static constexpr int NW = kGatherThreads / 32;
-  static constexpr int APW = 32 / kGatherLanes;  // atoms per warp at a time
+  static constexpr int NW = NT / 32;
+  static constexpr int APW = 32 / GL;  // atoms per warp at a time
   static constexpr size_t bytes =
       sizeof(CT) * (TZ * ZP + NW * APW * 9 * kWPad) + sizeof(int) * NW * APW * W * W;
 };
 
-// The gather of the atoms of one brick.  kGatherLanes lanes share one atom
-// (two atoms per warp at 16): each group builds its atom's weight tables,
-// compacts the (y, z) rows that meet the sphere and sums them, one row per
-// lane and iteration, in the order of the row list.
-template <typename CT, int W>
+// The gather of the atoms of one brick by a block of NT threads.  kGatherLanes
+// lanes share one atom (two atoms per warp at 16): each group builds its
+// atom's weight tables, compacts the (y, z) rows that meet the sphere and sums
+// them, one row per lane and iteration, in the order of the row list.  GL
+// lanes per atom (16 by default; the batched launch may take 8).
+template <typename CT, int W, int NT = kGatherThreads, int GL = kGatherLanes>
 __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __restrict__ sorted,
                                              const int* __restrict__ perm,
                                              const int* __restrict__ start, const BinLayout& b,
@@ -619,9 +623,9 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
                                              double outscale, double* __restrict__ fx,
                                              double* __restrict__ fy, double* __restrict__ fz,
                                              int bxi, int byi, int bzi, unsigned char* gsm) {
-  typedef GatherGeom<CT, W> GG;
+  typedef GatherGeom<CT, W, NT, GL> GG;
   constexpr int n = GG::n, TX = GG::TX, TY = GG::TY, TZ = GG::TZ, TP = GG::TP, ZP = GG::ZP;
-  constexpr int NW = GG::NW, APW = GG::APW, GL = kGatherLanes;
+  constexpr int NW = GG::NW, APW = GG::APW;
   constexpr int NR = kGY * kGZ;  // cell rows of the brick
   constexpr int NG = (W * W + GL - 1) / GL;
   typedef typename Vec4<CT>::type V;
@@ -687,7 +691,7 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   };
   const unsigned gmask = GL == 32 ? 0xffffffffu : ((1u << GL) - 1u);
   for (int c0 = 0; c0 < natoms; c0 += kGatherList) {
-    brick_atom_list<kGatherThreads, NR>(rng_a, rng_p, natoms, c0, kGatherList, alist);
+    brick_atom_list<NT, NR>(rng_a, rng_p, natoms, c0, kGatherList, alist);
     __syncthreads();
     const int nc = min(kGatherList, natoms - c0);
     // the next atom's record and output slot are loaded one iteration ahead,
@@ -983,15 +987,6 @@ cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const 
 // ===========================================================================
 // Batched systems: persistent kernels over (system, brick) work items
 // ===========================================================================
-__device__ __forceinline__ int batch_sys_of(const int* __restrict__ first, int nsys, int i) {
-  int lo = 0, hi = nsys - 1;  // last s with first[s] <= i
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (first[mid] <= i) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 __global__ void k_batch_bin_count(const float4* __restrict__ xyzq, int ntot,
                                   const BatchSys* __restrict__ sys, const int* __restrict__ first,
                                   int nsys, int* __restrict__ key, int* __restrict__ counts) {
@@ -1183,6 +1178,198 @@ cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+
+// ===========================================================================
+// Batched systems in one persistent cooperative launch
+// ===========================================================================
+constexpr int kFusedThreads = 512;
+static_assert(kFusedThreads == kScatterThreads, "the fused kernel runs the scatter bricks");
+static_assert(kScanTile % kFusedThreads == 0, "scan tile per thread");
+
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+
+template <int GL>
+constexpr size_t fused_fwd_smem() {
+  return cmax(cmax(cmax(sizeof(int) * ScatterGeom<9>::words, sizeof(int) * ScatterGeom<11>::words),
+                   cmax(sizeof(int) * ScatterGeom<13>::words, sizeof(int) * ScatterGeom<15>::words)),
+              cmax(cmax(cmax(GatherGeom<float, 9, kFusedThreads, GL>::bytes,
+                             GatherGeom<float, 11, kFusedThreads, GL>::bytes),
+                        cmax(GatherGeom<float, 13, kFusedThreads, GL>::bytes,
+                             GatherGeom<float, 15, kFusedThreads, GL>::bytes)),
+                   sizeof(SmallFftTw) + sizeof(int) * 3 * (kSfSmemSystems + 1)));
+}
+
+bool batch_fused_supported(const BatchSys* sys, int nsys) {
+  for (int s = 0; s < nsys; s++) {
+    for (int d = 0; d < 3; d++)
+      if (sys[s].b.M[d] % 8 != 0 || sys[s].b.M[d] > kSfMax) return false;
+    if (sys[s].W != 9 && sys[s].W != 11 && sys[s].W != 13 && sys[s].W != 15) return false;
+  }
+  return nsys > 0;
+}
+
+// One tile of kScanTile bin counts: exclusive prefix into start, the tile's
+// sum into tile_sums[t].  All threads of the block.
+__device__ __forceinline__ int fused_scan_tile(const int* __restrict__ counts, int nb,
+                                               int* __restrict__ start, int* __restrict__ sums,
+                                               int t) {
+  constexpr int PER = kScanTile / kFusedThreads;
+  const int base = t * kScanTile + threadIdx.x * PER;
+  int v[PER];
+  int s = 0;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    v[j] = (base + j < nb) ? counts[base + j] : 0;
+    s += v[j];
+  }
+  int total;
+  int run = block_exclusive_scan(s, &total);
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    if (base + j < nb) start[base + j] = run;
+    run += v[j];
+  }
+  if (threadIdx.x == 0) sums[t] = total;
+  return total;
+}
+
+template <int GL>
+__global__ void __launch_bounds__(kFusedThreads, 1) k_batch_forward_fused(BatchFused a) {
+  namespace cg = cooperative_groups;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
+  // clear the bin counts and the int64 grid
+  for (long long i = gtid; i < a.nbins; i += gstride) a.w.counts[i] = 0;
+  for (long long i = gtid; i < a.gtot; i += gstride) a.g64[i] = 0;
+  if (gtid < 2) a.qctr[gtid] = 0;
+  cg::this_grid().sync();
+  // bin keys and counts (the key of k_batch_bin_count)
+  for (long long i = gtid; i < a.ntot; i += gstride) {
+    const float4 p = a.xyzq[i];
+    const BatchSys& S = a.sys[batch_sys_of(a.first, a.nsys, (int)i)];
+    const int cx = wrap1(centre_cell(p.x, S.sp.inv_h[0]), S.b.M[0]);
+    const int cy = wrap1(centre_cell(p.y, S.sp.inv_h[1]), S.b.M[1]);
+    const int cz = wrap1(centre_cell(p.z, S.sp.inv_h[2]), S.b.M[2]);
+    const int k = S.bin_off + (cz * S.b.M[1] + cy) * S.b.nbx + (cx >> S.b.bxs);
+    a.w.key[i] = k;
+    atomicAdd(&a.w.counts[k], 1);
+  }
+  cg::this_grid().sync();
+  // exclusive scan of the counts: tiles, their sums, the offsets
+  const int ntiles = (a.nbins + kScanTile - 1) / kScanTile;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    fused_scan_tile(a.w.counts, a.nbins, a.w.start, a.w.tile_sums, t);
+  cg::this_grid().sync();
+  if (blockIdx.x == 0) {  // tile sums -> tile offsets, in place (ntiles <= kScanTile)
+    const int total = fused_scan_tile(a.w.tile_sums, ntiles, a.w.tile_sums,
+                                      a.w.tile_sums + ntiles, 0);
+    if (threadIdx.x == 0) a.w.start[a.nbins] = total;
+  }
+  cg::this_grid().sync();
+  for (long long i = gtid; i < a.nbins; i += gstride) a.w.start[i] += a.w.tile_sums[i / kScanTile];
+  cg::this_grid().sync();
+  // placement in any order within a bin (the counts return to zero)
+  for (long long i = gtid; i < a.ntot; i += gstride) {
+    const int k = a.w.key[i];
+    const int slot = a.w.start[k] + atomicSub(&a.w.counts[k], 1) - 1;
+    a.sorted[slot] = a.xyzq[i];
+    a.perm[slot] = (int)i;
+  }
+  cg::this_grid().sync();
+  // spread bricks
+  for (int it = fused_next_item(&a.qctr[0]); it < a.nscat; it = fused_next_item(&a.qctr[0])) {
+    const BatchItem item = a.scat[it];
+    const BatchSys& S = a.sys[item.sys];
+    const int* st = a.w.start + S.bin_off;
+    long long* g = a.g64 + S.grid_off;
+    int* tile = reinterpret_cast<int*>(fsm);
+    switch (S.W) {
+      case 9: scatter_brick<9>(a.sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, g); break;
+      case 11: scatter_brick<11>(a.sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, g); break;
+      case 13: scatter_brick<13>(a.sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, g); break;
+      default: scatter_brick<15>(a.sorted, st, S.b, S.sp, item.bx, item.by, item.bz, tile, g); break;
+    }
+    __syncthreads();
+  }
+  cg::this_grid().sync();
+  fused_solve(a, a.phi, true, fsm);
+  cg::this_grid().sync();
+  // gather bricks
+  for (int it = fused_next_item(&a.qctr[1]); it < a.ngath; it = fused_next_item(&a.qctr[1])) {
+    const BatchItem item = a.gath[it];
+    const BatchSys& S = a.sys[item.sys];
+    const int* st = a.w.start + S.bin_off;
+    const float* ph = a.phi + S.grid_off;
+    switch (S.W) {
+      case 9:
+        gather_brick<float, 9, kFusedThreads, GL>(a.sorted, a.perm, st, S.b, S.sg, ph, a.ccelec,
+                                                  a.fx, a.fy, a.fz, item.bx, item.by, item.bz, fsm);
+        break;
+      case 11:
+        gather_brick<float, 11, kFusedThreads, GL>(a.sorted, a.perm, st, S.b, S.sg, ph, a.ccelec,
+                                                   a.fx, a.fy, a.fz, item.bx, item.by, item.bz, fsm);
+        break;
+      case 13:
+        gather_brick<float, 13, kFusedThreads, GL>(a.sorted, a.perm, st, S.b, S.sg, ph, a.ccelec,
+                                                   a.fx, a.fy, a.fz, item.bx, item.by, item.bz, fsm);
+        break;
+      default:
+        gather_brick<float, 15, kFusedThreads, GL>(a.sorted, a.perm, st, S.b, S.sg, ph, a.ccelec,
+                                                   a.fx, a.fy, a.fz, item.bx, item.by, item.bz, fsm);
+        break;
+    }
+    __syncthreads();
+  }
+}
+
+template <int GL>
+static int fused_fwd_ctas() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 0;
+  }
+  int v = cache[dev].load();
+  if (v == 0) {
+    const size_t smem = fused_fwd_smem<GL>();
+    int nb = 0;
+    if (cudaFuncSetAttribute(k_batch_forward_fused<GL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_forward_fused<GL>,
+                                                      kFusedThreads, smem) != cudaSuccess) {
+      cudaGetLastError();
+      nb = 0;
+    }
+    v = nb > 0 ? nb * sm_count() : -1;
+    cache[dev].store(v);
+  }
+  return v > 0 ? v : 0;
+}
+
+int batch_fused_ctas(int gather_lanes) {
+  return gather_lanes == 8 ? fused_fwd_ctas<8>() : fused_fwd_ctas<16>();
+}
+
+cudaError_t launch_batch_forward_fused(const BatchFused& a, int ctas, int gather_lanes,
+                                       cudaStream_t st) {
+  const int most = gather_lanes == 8 ? fused_fwd_ctas<8>() : fused_fwd_ctas<16>();
+  if (most <= 0 || ctas < 1 || ctas > most) return cudaErrorCooperativeLaunchTooLarge;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(kFusedThreads);
+  cfg.dynamicSmemBytes = gather_lanes == 8 ? fused_fwd_smem<8>() : fused_fwd_smem<16>();
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (gather_lanes == 8) return cudaLaunchKernelEx(&cfg, k_batch_forward_fused<8>, a);
+  return cudaLaunchKernelEx(&cfg, k_batch_forward_fused<16>, a);
 }
 
 #define GSE_TILED_INST(CT)                                                                      \

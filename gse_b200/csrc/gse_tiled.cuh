@@ -112,6 +112,53 @@ struct BatchSeg {
   int W, first, count;
 };
 
+// The batched evaluation in one persistent cooperative launch per direction:
+// binning, spread, the small-grid FFT solve with the Green's multiply and
+// energy, and gather (forward), or adjoint source, solve and reverse-pass
+// gather (reverse), separated by grid-wide barriers.  Grids must be multiples
+// of 8 and at most 64 points per side (batch_fused_supported).
+struct BatchFused {
+  const float4* xyzq;
+  int ntot, nsys, nbins;
+  const BatchSys* sys;
+  const int* first;         // [nsys + 1] first atom of each system
+  BinScratch w;
+  float4* sorted;
+  int* perm;
+  const BatchItem* scat;    // spread / adjoint-source bricks
+  int nscat;
+  const BatchItem* gath;    // gather bricks
+  int ngath;
+  const BatchItem* agath;   // reverse-pass gather bricks
+  int nagath;
+  long long* g64;           // int64 accumulation grid (all systems)
+  long long gtot;
+  float2* rhok;             // half spectra
+  const float* gtab;        // Green's tables (half-spectrum layout)
+  float* phi;               // potential
+  float* psi;               // reverse-pass potential of the adjoint source
+  const int* xrow_first;    // [nsys + 1] prefix of the systems' x rows (My Mz)
+  const int* ycol_first;    // [nsys + 1] prefix of their y columns (Mz (Mx/2+1))
+  const int* zcol_first;    // [nsys + 1] prefix of their z columns (My (Mx/2+1))
+  double* epart;            // [zcol_first[nsys]] k-space energy of each z column
+  double* energy;           // [nsys]
+  double ccelec;
+  double *fx, *fy, *fz;     // forces [ntot]
+  const double* dLdE;       // reverse pass inputs
+  const double *gfx, *gfy, *gfz;
+  double *dq, *dx, *dy, *dz;  // reverse pass outputs
+  int* qctr;                // [4] work-item counters: spread, gather, adjoint source,
+                            // reverse-pass gather (each kernel zeroes its own first)
+};
+
+bool batch_fused_supported(const BatchSys* sys, int nsys);
+// Largest cooperative grid of the fused kernels on this device (0: cannot run).
+int batch_fused_ctas(int gather_lanes);
+int batch_fused_rev_ctas();
+cudaError_t launch_batch_forward_fused(const BatchFused& a, int ctas, int gather_lanes,
+                                       cudaStream_t st);
+cudaError_t launch_batch_reverse_fused(const BatchFused& a, int ctas, cudaStream_t st);
+
 cudaError_t launch_batch_bin(const float4* xyzq, int ntot, const BatchSys* sys, const int* first,
                              int nsys, int nbins, BinScratch w, float4* sorted, int* perm,
                              cudaStream_t st);

@@ -2,7 +2,10 @@
 // (gse_tiled.cu) and the tiled reverse-pass kernels (gse_adjoint.cu).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "gse_internal.cuh"
+#include "gse_smallfft.cuh"
 #include "gse_tiled.cuh"
 
 namespace gse {
@@ -214,5 +217,272 @@ __device__ __forceinline__ void stage_tile_async(const CT* __restrict__ src, con
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// Batched systems
+// ---------------------------------------------------------------------------
+// Next work item of a phase for the whole block, from a counter in global
+// memory: blocks take items as they finish the previous one, so a phase ends
+// with the blocks' loads balanced.  All threads of the block must call it.
+__device__ __forceinline__ int fused_next_item(int* ctr) {
+  __shared__ int next;
+  __syncthreads();
+  if (threadIdx.x == 0) next = atomicAdd(ctr, 1);
+  __syncthreads();
+  return next;
+}
+
+// System of item i, given each system's first item in first[0..nsys).
+__device__ __forceinline__ int batch_sys_of(const int* __restrict__ first, int nsys, int i) {
+  int lo = 0, hi = nsys - 1;  // last s with first[s] <= i
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// The small-grid FFT solve of every system (forward: from the int64 spread
+// grid to the potential, with the k-space energy; reverse: the adjoint source
+// to its potential, no energy): five passes of independent lines, one group of
+// 8 lanes per line (gse_smallfft.cuh), separated by grid-wide barriers.  All
+// threads of the cooperative grid call it.
+struct SfLine {
+  int s, r;     // system, line index within the system's pass
+  bool active;  // false for the padding groups past the last line
+};
+
+// Largest system count whose line prefixes the FFT passes stage in shared memory.
+constexpr int kSfSmemSystems = 2047;
+
+__device__ __forceinline__ SfLine sf_line(const int* first, int nsys, int u) {
+  SfLine L;
+  L.active = u < first[nsys];
+  L.s = L.active ? batch_sys_of(first, nsys, u) : 0;
+  L.r = L.active ? u - first[L.s] : 0;
+  return L;
+}
+
+// Group loop over the lines of one pass: every warp of the grid takes eight
+// consecutive lines at a time, two per group (u0 and u1 = u0 + 4), so all its
+// lanes run the shuffles together and each group has two independent lines in
+// flight.
+#define SF_FOR_LINE_PAIRS(total, u0, u1)                                                \
+  for (int sf_w0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 8;                  \
+       sf_w0 < (total); sf_w0 += (gridDim.x * blockDim.x) >> 2)                         \
+    for (int u0 = sf_w0 + ((threadIdx.x & 31) >> 3), u1 = u0 + 4, sf_once = 1; sf_once;  \
+         sf_once = 0)
+
+__device__ __forceinline__ void fused_solve(const BatchFused& a, float* out, bool energy,
+                                            unsigned char* fsm) {
+  namespace cg = cooperative_groups;
+  SmallFftTw& T = *reinterpret_cast<SmallFftTw*>(fsm);
+  sf_build_twiddles(T);
+  // the passes' line prefixes in shared memory: every line looks up its system
+  // by a binary search over them
+  const int* xrow_first = a.xrow_first;
+  const int* ycol_first = a.ycol_first;
+  const int* zcol_first = a.zcol_first;
+  if (a.nsys <= kSfSmemSystems) {
+    int* pre = reinterpret_cast<int*>(fsm + sizeof(SmallFftTw));
+    const int np = a.nsys + 1;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+      pre[i] = a.xrow_first[i];
+      pre[np + i] = a.ycol_first[i];
+      pre[2 * np + i] = a.zcol_first[i];
+    }
+    xrow_first = pre;
+    ycol_first = pre + np;
+    zcol_first = pre + 2 * np;
+  }
+  __syncthreads();
+  const int l = threadIdx.x & 7, k1 = bitrev3(l);
+  const double unscale = exp2(-40.0);
+  // x rows: r2c of the int64 grid
+  SF_FOR_LINE_PAIRS(xrow_first[a.nsys], u0, u1) {
+    SfLine L[2] = {sf_line(xrow_first, a.nsys, u0), sf_line(xrow_first, a.nsys, u1)};
+    float2 v[2][8];
+    int m[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const BatchSys& S = a.sys[L[q].s];
+      const int Mx = S.b.M[0];
+      m[q] = L[q].active ? Mx / 8 : 1;
+      const long long* g = a.g64 + S.grid_off + (long long)L[q].r * Mx;
+#pragma unroll
+      for (int j1 = 0; j1 < 8; j1++)
+        v[q][j1] = (L[q].active && j1 < m[q])
+                       ? make_float2((float)((double)g[m[q] * l + j1] * unscale), 0.f)
+                       : make_float2(0.f, 0.f);
+    }
+    const int mmax = sf_warp_mmax(max(m[0], m[1]));
+    sf8_dft(v[0], m[0], mmax, -1.f, T);
+    sf8_dft(v[1], m[1], mmax, -1.f, T);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const BatchSys& S = a.sys[L[q].s];
+      const int Hx = S.b.M[0] / 2 + 1;
+      float2* o = a.rhok + S.kgrid_off + (long long)L[q].r * Hx;
+#pragma unroll
+      for (int k2 = 0; k2 < 8; k2++)
+        if (L[q].active && k2 < m[q] && k1 + 8 * k2 < Hx) o[k1 + 8 * k2] = v[q][k2];
+    }
+  }
+  cg::this_grid().sync();
+  // y columns, forward then (after the z pass) inverse
+  auto ypass = [&](float dir) {
+    SF_FOR_LINE_PAIRS(ycol_first[a.nsys], u0, u1) {
+      SfLine L[2] = {sf_line(ycol_first, a.nsys, u0), sf_line(ycol_first, a.nsys, u1)};
+      float2 v[2][8];
+      float2* c[2];
+      int m[2];
+      long long hx[2];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const BatchSys& S = a.sys[L[q].s];
+        const int Hx = S.b.M[0] / 2 + 1, My = S.b.M[1];
+        m[q] = L[q].active ? My / 8 : 1;
+        hx[q] = Hx;
+        const int z = L[q].r / Hx, x = L[q].r - z * Hx;
+        c[q] = a.rhok + S.kgrid_off + (long long)z * My * Hx + x;
+#pragma unroll
+        for (int j1 = 0; j1 < 8; j1++)
+          v[q][j1] = (L[q].active && j1 < m[q]) ? c[q][(m[q] * l + j1) * hx[q]]
+                                                : make_float2(0.f, 0.f);
+      }
+      const int mmax = sf_warp_mmax(max(m[0], m[1]));
+      sf8_dft(v[0], m[0], mmax, dir, T);
+      sf8_dft(v[1], m[1], mmax, dir, T);
+#pragma unroll
+      for (int q = 0; q < 2; q++)
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++)
+          if (L[q].active && k2 < m[q]) c[q][(k1 + 8 * k2) * hx[q]] = v[q][k2];
+    }
+  };
+  ypass(-1.f);
+  cg::this_grid().sync();
+  // z columns: forward, Green's multiply (and energy), inverse
+  SF_FOR_LINE_PAIRS(zcol_first[a.nsys], u0, u1) {
+    SfLine L[2] = {sf_line(zcol_first, a.nsys, u0), sf_line(zcol_first, a.nsys, u1)};
+    float2 v[2][8];
+    float2* c[2];
+    const float* gt[2];
+    long long pitch[2];
+    int m[2];
+    double wgt[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const BatchSys& S = a.sys[L[q].s];
+      const int Mx = S.b.M[0], Hx = Mx / 2 + 1, My = S.b.M[1], Mz = S.b.M[2];
+      m[q] = L[q].active ? Mz / 8 : 1;
+      const int y = L[q].r / Hx, x = L[q].r - y * Hx;
+      pitch[q] = (long long)My * Hx;
+      const long long off = S.kgrid_off + (long long)y * Hx + x;
+      c[q] = a.rhok + off;
+      gt[q] = a.gtab + off;
+      wgt[q] = (x == 0 || x == Mx / 2) ? 1.0 : 2.0;
+#pragma unroll
+      for (int j1 = 0; j1 < 8; j1++)
+        v[q][j1] = (L[q].active && j1 < m[q]) ? c[q][(m[q] * l + j1) * pitch[q]]
+                                              : make_float2(0.f, 0.f);
+    }
+    const int mmax = sf_warp_mmax(max(m[0], m[1]));
+    sf8_dft(v[0], m[0], mmax, -1.f, T);
+    sf8_dft(v[1], m[1], mmax, -1.f, T);
+    double e[2] = {0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int k2 = 0; k2 < 8; k2++) {
+        if (L[q].active && k2 < m[q]) {
+          const float f = gt[q][(k1 + 8 * k2) * pitch[q]];
+          const float2 w = v[q][k2];
+          if (energy) e[q] += wgt[q] * (double)f * ((double)w.x * w.x + (double)w.y * w.y);
+          c[q][(k1 + 8 * k2) * pitch[q]] = make_float2(w.x * f, w.y * f);
+        }
+      }
+    __syncwarp();  // the groups' columns, multiplied, back in memory in index order
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int j1 = 0; j1 < 8; j1++)
+        v[q][j1] = (L[q].active && j1 < m[q]) ? c[q][(m[q] * l + j1) * pitch[q]]
+                                              : make_float2(0.f, 0.f);
+    __syncwarp();
+    sf8_dft(v[0], m[0], mmax, 1.f, T);
+    sf8_dft(v[1], m[1], mmax, 1.f, T);
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int k2 = 0; k2 < 8; k2++)
+        if (L[q].active && k2 < m[q]) c[q][(k1 + 8 * k2) * pitch[q]] = v[q][k2];
+    if (energy) {
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        // the group's eight lane sums in a fixed order
+        double t = e[q];
+        t += __shfl_xor_sync(0xffffffffu, t, 1);
+        t += __shfl_xor_sync(0xffffffffu, t, 2);
+        t += __shfl_xor_sync(0xffffffffu, t, 4);
+        if (L[q].active && l == 0) a.epart[q == 0 ? u0 : u1] = t;
+      }
+    }
+  }
+  cg::this_grid().sync();
+  ypass(1.f);
+  cg::this_grid().sync();
+  // x rows: c2r into the real grid
+  SF_FOR_LINE_PAIRS(xrow_first[a.nsys], u0, u1) {
+    SfLine L[2] = {sf_line(xrow_first, a.nsys, u0), sf_line(xrow_first, a.nsys, u1)};
+    float2 v[2][8];
+    int m[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const BatchSys& S = a.sys[L[q].s];
+      const int Mx = S.b.M[0], Hx = Mx / 2 + 1;
+      m[q] = L[q].active ? Mx / 8 : 1;
+      const float2* c = a.rhok + S.kgrid_off + (long long)L[q].r * Hx;
+#pragma unroll
+      for (int j1 = 0; j1 < 8; j1++) {
+        const int j = m[q] * l + j1;
+        float2 t = make_float2(0.f, 0.f);
+        if (L[q].active && j1 < m[q]) {
+          if (j < Hx) {
+            t = c[j];
+            if (j == 0 || j == Mx / 2) t.y = 0.f;  // FFTW's c2r ignores these imaginary parts
+          } else {
+            t = c[Mx - j];
+            t.y = -t.y;
+          }
+        }
+        v[q][j1] = t;
+      }
+    }
+    const int mmax = sf_warp_mmax(max(m[0], m[1]));
+    sf8_dft(v[0], m[0], mmax, 1.f, T);
+    sf8_dft(v[1], m[1], mmax, 1.f, T);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const BatchSys& S = a.sys[L[q].s];
+      const int Mx = S.b.M[0];
+      float* o = out + S.grid_off + (long long)L[q].r * Mx;
+#pragma unroll
+      for (int k2 = 0; k2 < 8; k2++)
+        if (L[q].active && k2 < m[q]) o[k1 + 8 * k2] = v[q][k2].x;
+    }
+  }
+  if (energy) {  // each system's column energies by one warp: lane-strided sums, then a tree
+    const int lane = threadIdx.x & 31;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.nsys;
+         s += (gridDim.x * blockDim.x) >> 5) {
+      double e = 0.0;
+      for (int u = a.zcol_first[s] + lane; u < a.zcol_first[s + 1]; u += 32) e += a.epart[u];
+      e = warp_sum(e);
+      if (lane == 0) a.energy[s] = a.sys[s].efac * e;
+    }
+  }
+}
+#undef SF_FOR_LINE_PAIRS
 
 }  // namespace gse

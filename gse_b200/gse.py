@@ -699,6 +699,14 @@ class Batch:
         check(self._L.gse_batch_autotune(
             self.h, None if cache_path is None else str(cache_path).encode(), 1 if use_cache else 0))
 
+    def set_schedule(self, fused, gather_lanes=16, largest_first=False, scatter_ctas=296,
+                     gather_ctas=296):
+        """Pin the launch schedule (gse_batch_set_schedule): fused=True runs each
+        direction as one persistent cooperative kernel."""
+        check(self._L.gse_batch_set_schedule(self.h, int(bool(fused)), int(gather_lanes),
+                                             int(bool(largest_first)), int(scatter_ctas),
+                                             int(gather_ctas)))
+
     def buffers(self):
         """The batch's device buffers as CUDA torch tensors (views, no copy)."""
         import torch

@@ -408,6 +408,12 @@ typedef struct gse_batch_info {
   double* dLdE;                    /* [n_systems] reverse-pass input */
   double* grad_forces;             /* [3][n_total] reverse-pass input */
   double* grad_out;                /* [4][n_total]: dL/dq, dL/dx, dL/dy, dL/dz */
+  int fused;        /* 1: each direction is one persistent cooperative launch (every grid
+                       side a multiple of 8 and at most 64); 0: one launch per stage */
+  int gather_lanes; /* lanes per atom in the gather (autotuned on the fused path: 16 or 8) */
+  int fused_ctas;   /* persistent CTAs of the fused launches */
+  int graph_kernels; /* kernel nodes of the graph gse_batch_capture recorded (0: none) */
+  int fused_available; /* 1: the fused schedule can run on this batch */
 } gse_batch_info_t;
 
 /* Build a batch: bins, grids grouped by size for strided FFT plans, and the
@@ -439,8 +445,23 @@ gse_status_t gse_batch_adjoint(gse_batch_t* batch, const void* xyzq, const doubl
 gse_status_t gse_batch_capture(gse_batch_t* batch, int with_adjoint);
 gse_status_t gse_batch_launch(gse_batch_t* batch);
 
-/* Time the persistent-CTA counts of spread and gather and the order of the
- * work items on the batch's current positions, keep the fastest.  With
+/* Choose the launch schedule of the batch.  fused != 0: each direction as one
+ * persistent cooperative kernel (binning, spread, the small-grid FFT solve with
+ * the Green's multiply and energy, gather; or adjoint source, solve, reverse
+ * gather, separated by grid-wide barriers), with gather_lanes (8 or 16) lanes
+ * per atom in the gathers; only where every grid side is a multiple of 8 and
+ * at most 64 (GSE_ERR_UNSUPPORTED otherwise).  fused == 0: one launch per
+ * stage, persistent spread and gather kernels of scatter_ctas / gather_ctas
+ * CTAs and cuFFT transforms per grid-size class.  largest_first orders the
+ * work items by system size.  Drops a captured graph. */
+gse_status_t gse_batch_set_schedule(gse_batch_t* batch, int fused, int gather_lanes,
+                                    int largest_first, int scatter_ctas, int gather_ctas);
+
+/* Time the launch schedules on the batch's current positions, each on a
+ * forward and a reverse pass, and keep the fastest: the per-stage launches
+ * (work-item order x persistent-CTA counts of spread and gather) and, where
+ * the batch allows it, the fused launches (work-item order x lanes per atom of
+ * the gathers: 16, two atoms per warp, or 8, four).  With
  * cache_path, the choice is appended to that text file under a key made of
  * the system count, grid-size histogram, atom count and SM count; with
  * use_cache != 0 a cached choice for the same key is taken without timing. */
