@@ -64,10 +64,10 @@ __device__ __forceinline__ void sf_build_twiddles(SmallFftTw& T) {
 
 // In-register DFT of one group of 8 lanes (l = lane & 7): on entry v[j1] =
 // x[m l + j1] for j1 < m, on return v[k2] = X[bitrev3(l) + 8 k2] for k2 < m.
-// mmax >= m is the same in the whole warp (groups of one warp may work on
+// MM >= m is the same in the whole warp (groups of one warp may work on
 // different lengths); every lane of the warp must call it.
-__device__ __forceinline__ void sf8_dft(float2 (&v)[8], int m, int mmax, float dir,
-                                        const SmallFftTw& T) {
+template <int MM>
+__device__ __forceinline__ void sf8_dft_t(float2 (&v)[8], int m, float dir, const SmallFftTw& T) {
   const int l = threadIdx.x & 7;
   const int M = 8 * m;
   const float2* tw = T.tw[m - 1];
@@ -76,36 +76,48 @@ __device__ __forceinline__ void sf8_dft(float2 (&v)[8], int m, int mmax, float d
     const bool upper = (l & h) != 0;
     const float2 w = sf_w(tw, (l & (h - 1)) * (4 / h) * m, dir);  // w_{2h}^(l mod h)
 #pragma unroll
-    for (int j1 = 0; j1 < 8; j1++) {
-      if (j1 < mmax) {
-        float2 p;
-        p.x = __shfl_xor_sync(0xffffffffu, v[j1].x, h);
-        p.y = __shfl_xor_sync(0xffffffffu, v[j1].y, h);
-        v[j1] = upper ? cmul(make_float2(p.x - v[j1].x, p.y - v[j1].y), w)
-                      : make_float2(v[j1].x + p.x, v[j1].y + p.y);
-      }
+    for (int j1 = 0; j1 < MM; j1++) {
+      float2 p;
+      p.x = __shfl_xor_sync(0xffffffffu, v[j1].x, h);
+      p.y = __shfl_xor_sync(0xffffffffu, v[j1].y, h);
+      v[j1] = upper ? cmul(make_float2(p.x - v[j1].x, p.y - v[j1].y), w)
+                    : make_float2(v[j1].x + p.x, v[j1].y + p.y);
     }
   }
   const int k1 = bitrev3(l);
-  float2 t[8];
+  float2 t[MM];
+  int e1 = 0;  // j1 k1 mod M
 #pragma unroll
-  for (int j1 = 0; j1 < 8; j1++)
-    if (j1 < m) t[j1] = cmul(v[j1], sf_w(tw, (j1 * k1) % M, dir));
+  for (int j1 = 0; j1 < MM; j1++) {
+    t[j1] = j1 < m ? cmul(v[j1], sf_w(tw, e1, dir)) : make_float2(0.f, 0.f);
+    e1 += k1;
+    if (e1 >= M) e1 -= M;
+  }
 #pragma unroll
-  for (int k2 = 0; k2 < 8; k2++) {
-    if (k2 < m) {
-      float2 acc = t[0];
-      int e = 0;  // 8 j1 k2 mod M
+  for (int k2 = 0; k2 < MM; k2++) {
+    float2 acc = t[0];
+    int e = 0;  // 8 j1 k2 mod M
 #pragma unroll
-      for (int j1 = 1; j1 < 8; j1++) {
-        if (j1 < m) {
-          e += 8 * k2;
-          if (e >= M) e -= M;
-          acc = cmad(t[j1], sf_w(tw, e, dir), acc);
-        }
-      }
-      v[k2] = acc;
+    for (int j1 = 1; j1 < MM; j1++) {
+      e += 8 * k2;
+      if (e >= M) e -= M;
+      if (j1 < m) acc = cmad(t[j1], sf_w(tw, e, dir), acc);
     }
+    v[k2] = acc;
+  }
+}
+
+__device__ __forceinline__ void sf8_dft(float2 (&v)[8], int m, int mmax, float dir,
+                                        const SmallFftTw& T) {
+  switch (mmax) {
+    case 1: sf8_dft_t<1>(v, m, dir, T); break;
+    case 2: sf8_dft_t<2>(v, m, dir, T); break;
+    case 3: sf8_dft_t<3>(v, m, dir, T); break;
+    case 4: sf8_dft_t<4>(v, m, dir, T); break;
+    case 5: sf8_dft_t<5>(v, m, dir, T); break;
+    case 6: sf8_dft_t<6>(v, m, dir, T); break;
+    case 7: sf8_dft_t<7>(v, m, dir, T); break;
+    default: sf8_dft_t<8>(v, m, dir, T); break;
   }
 }
 
