@@ -159,6 +159,7 @@ struct gse_context {
   int* d_btmp = nullptr;
   int* d_bcounts = nullptr;
   int* d_bstart = nullptr;
+  int* d_blstart = nullptr;  // mixed form: tile-local bin starts of the scan
   int* d_btiles = nullptr;
   unsigned* d_qmax = nullptr;
   // Green's function table of the context's own solve (sigma2, box)
@@ -357,9 +358,14 @@ gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT
   StageTimer tm(c, GSE_STAGE_BIN);
   BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax,
                c->d_badmap};
-  // count, three scan passes, then the placement: one kernel (mixed, any
-  // order within a bin) or two (FP64, stable)
-  c->launches += n > 0 ? (c->fp64 ? 6 : 5) : 3;
+  // mixed: count, a tile-local scan and the placement that applies the tile
+  // offsets (the counts stay zero between calls); FP64: count, three scan
+  // passes and a stable placement in two kernels
+  if (!c->fp64) {
+    w.lstart = c->d_blstart;
+    w.counts_zero = true;
+  }
+  c->launches += c->fp64 ? (n > 0 ? 6 : 3) : (n > 0 ? 3 : 2);
   CU(launch_bin_sorted<CT>((const V*)dx, n, c->bl, s.inv_h[0], s.inv_h[1], s.inv_h[2], w,
                            (V*)c->d_sorted, c->d_perm, c->stream));
   return GSE_OK;
@@ -850,6 +856,8 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   c->bl = make_bin_layout(M, c->fp64 ? kBinX64 : kBinX32);
   c->nbins2 = bin_count(c->bl);
   CUC(cudaMalloc(&c->d_bcounts, sizeof(int) * c->nbins2));
+  CUC(cudaMemset(c->d_bcounts, 0, sizeof(int) * c->nbins2));
+  if (!c->fp64) CUC(cudaMalloc(&c->d_blstart, sizeof(int) * c->nbins2));
   CUC(cudaMalloc(&c->d_bstart, sizeof(int) * (c->nbins2 + 1)));
   CUC(cudaMalloc(&c->d_btiles, sizeof(int) * (c->nbins2 / 4096 + 2)));
   CUC(cudaMalloc(&c->d_qmax, sizeof(unsigned)));
@@ -903,6 +911,7 @@ gse_status_t gse_destroy(gse_context_t* c) {
   cudaFree(c->d_bkey);
   cudaFree(c->d_btmp);
   cudaFree(c->d_bcounts);
+  cudaFree(c->d_blstart);
   cudaFree(c->d_bstart);
   cudaFree(c->d_btiles);
   cudaFree(c->d_qmax);

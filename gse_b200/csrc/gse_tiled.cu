@@ -143,6 +143,45 @@ __global__ void k_bin_place_direct(const typename Vec4<CT>::type* __restrict__ x
   }
 }
 
+// Order-free placement of the mixed form after a tile-local scan: the block's
+// copy of the tile offsets (exclusive prefix of the tile sums) turns the local
+// bin starts into global ones; the atoms are placed (counts[] counts down to
+// zero) and the global starts written for the kernels that read the bins.
+__global__ void __launch_bounds__(256)
+    k_bin_place_final(const float4* __restrict__ xyzq, int n, const int* __restrict__ key,
+                      const int* __restrict__ lstart, const int* __restrict__ tile_sums,
+                      int ntiles, int* __restrict__ counts, float4* __restrict__ sorted,
+                      int* __restrict__ perm, int* __restrict__ start, int nb) {
+  __shared__ int off[kScanTile];
+  constexpr int PER = kScanTile / 256;
+  {
+    const int base = threadIdx.x * PER;
+    int v[PER];
+    int s = 0;
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      v[j] = base + j < ntiles ? tile_sums[base + j] : 0;
+      s += v[j];
+    }
+    int run = block_exclusive_scan(s, nullptr);
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      off[base + j] = run;
+      run += v[j];
+    }
+  }
+  __syncthreads();
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (int i = gtid; i < n; i += gs) {
+    const int k = key[i];
+    const int slot = lstart[k] + off[k / kScanTile] + atomicSub(&counts[k], 1) - 1;
+    sorted[slot] = xyzq[i];
+    perm[slot] = i;
+  }
+  for (int i = gtid; i < nb; i += gs) start[i] = lstart[i] + off[i / kScanTile];
+  if (gtid == 0) start[nb] = off[ntiles - 1] + tile_sums[ntiles - 1];
+}
+
 // Stable placement: an atom's rank in its bin is the number of bin members
 // with a smaller original index.
 template <typename CT>
@@ -827,8 +866,11 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
   const int nb = b.M[1] * b.M[2] * b.nbx;
   const int ntiles = (nb + kScanTile - 1) / kScanTile;
   if (ntiles > kScanTile) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (!(sizeof(CT) == 4 && w.counts_zero)) {
+    e = cudaMemsetAsync(w.counts, 0, sizeof(int) * nb, st);
+    if (e != cudaSuccess) return e;
+  }
   // the largest |q| feeds the FP64 spread's range check only
   unsigned* qmax = sizeof(CT) == 8 ? w.qmax_bits : nullptr;
   if (qmax) {
@@ -853,6 +895,13 @@ cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, in
   if (ntiles > kScanTile) return cudaErrorInvalidValue;
   cudaError_t e;
   const int gb = (int)std::min<long long>(sm_count() * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
+  if (sizeof(CT) == 4 && w.lstart) {
+    // two kernels: tile-local scan, then placement with the tile offsets
+    k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.lstart, w.tile_sums);
+    k_bin_place_final<<<gb, 256, 0, st>>>((const float4*)xyzq, n, w.key, w.lstart, w.tile_sums,
+                                          ntiles, w.counts, (float4*)sorted, perm, w.start, nb);
+    return cudaGetLastError();
+  }
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.start, w.tile_sums);
   k_scan_sums<<<1, kScanThreads, 0, st>>>(w.tile_sums, ntiles, w.start, nb);
   k_scan_add<<<(nb + 255) / 256, 256, 0, st>>>(w.start, nb, w.tile_sums);

@@ -56,6 +56,12 @@ struct BinScratch {
   int* tmp;        // [n]
   unsigned* qmax_bits;  // max |q| over the atoms (float bits), written by the binning
   int* bad = nullptr;   // set to 1 when a position or charge is not finite (may be NULL)
+  // mixed form: the scan's tile-local prefix [nbins] (the placement applies the tile
+  // offsets and writes `start`); NULL: a three-kernel scan writes `start` directly
+  int* lstart = nullptr;
+  // mixed form: `counts` are zero on entry (the order-free placement counts every
+  // bin back down to zero), so the binning does not clear them
+  bool counts_zero = false;
 };
 
 // exp(-2 h^2 / (2 sigma^2)) per axis as an unevaluated sum hi + lo in CT
