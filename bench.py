@@ -334,6 +334,8 @@ def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
             b.set_schedule(fused=True, gather_lanes=16, largest_first=bool(i.largest_first))
         ms_other = timed_graph()
         other = dict(schedule(b.info()), ms_per_step=ms_other)
+    independent = bench_independent(syst, G, min(steps, 5), warmup, flush, stream)
+    independent["batch_ms_per_step"] = ms
     n_all = sum(y.n for y in every)
     out = {"workload": "256 independent triplet systems, N log-uniform in [501, 8001], "
                        "M = nearest multiple of 8 to L, sigma 2.0, mixed form",
@@ -342,9 +344,57 @@ def bench_batch(steps: int, warmup: int, flush, rank: int = 0, world: int = 1):
            "ranks": world, "systems_rank0": len(part[0]),
            "ms_per_step": ms, "systems_per_s": 256 / (ms / 1000.0),
            "charges_per_s": n_all / (ms / 1000.0),
-           "autotuned": chosen, "other_schedule": other}
+           "autotuned": chosen, "other_schedule": other, "independent": independent}
     b.close()
     return out
+
+
+def bench_independent(syst, G, steps: int, warmup: int, flush, stream):
+    """The batch's work done by separate single-system calls: one mixed
+    context per system, its forward (a replayed graph from the second call on)
+    and its reverse pass with dL/dE = 1 and the same dL/dF, all systems in
+    turn on one stream; device time per step (every system once), L2 flushed
+    before each step."""
+    import torch
+    from gse_b200.gse import Context
+    ctxs, args = [], []
+    off = 0
+    for y in syst:
+        c = Context(*y.grid, y.sigma, y.kappa, y.lambda_sigma, y.lambda_sigma1, *y.boxes,
+                    precision="mixed")
+        c.set_stream(stream.cuda_stream)
+        x = torch.from_numpy(np.ascontiguousarray(y.xyzq, dtype=np.float32)).cuda()
+        f = torch.empty((3, y.n), dtype=torch.float64, device="cuda")
+        e = torch.empty(1, dtype=torch.float64, device="cuda")
+        g = torch.from_numpy(np.ascontiguousarray(G[off:off + y.n].T)).cuda()
+        d = torch.empty((4, y.n), dtype=torch.float64, device="cuda")
+        off += y.n
+        ctxs.append(c)
+        args.append((y.n, x, f, e, g, d))
+
+    def one_step():
+        for c, (n, x, f, e, g, d) in zip(ctxs, args):
+            c.forward(n, x, f[0], f[1], f[2], energy_out=e)
+            c.adjoint(n, x, 1.0, g[0], g[1], g[2], d[0], d[1], d[2], d[3])
+
+    for _ in range(max(warmup, 2)):  # the second forward call captures the graph
+        one_step()
+    torch.cuda.synchronize()
+    t = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        one_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        t += a.elapsed_time(b)
+    launches = sum(c.launch_count() for c in ctxs)
+    for c in ctxs:
+        c.close()
+    return {"step": "every system's gse_forward (graph replay) and gse_adjoint, one context "
+                    "per system, one stream", "ms_per_step": t / steps,
+            "contexts": len(ctxs), "library_launches_total": int(launches)}
 
 
 def bench_grid_ops(steps: int, warmup: int, flush, peak: float):
