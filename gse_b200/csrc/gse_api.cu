@@ -383,9 +383,11 @@ bool tiled_ok(const gse_context_t* c, const Stencil<CT>& s) {
 template <typename CT>
 // `defer_rho`: with the own FFT, leave the float grid to the solve that
 // follows (it reads the int64 grid directly and writes rho on the way).
+// `zeroed`: the int64 grid was cleared before the binning that directly
+// precedes this call (forward_body).
 gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
                        double rcut, bool normalize, bool presorted = false,
-                       bool defer_rho = false) {
+                       bool defer_rho = false, bool zeroed = false) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, false, normalize);
   if (!normalize && tiled_ok<CT>(c, s)) {
@@ -399,7 +401,8 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
       const bool defer = defer_rho && c->own_fft;
       c->launches += defer ? 1 : 2;
       CU(launch_spread_scatter((const float4*)c->d_sorted, c->d_bstart, c->bl, s, c->d_fixed,
-                               defer ? nullptr : (float*)c->d_rho, c->stream));
+                               defer ? nullptr : (float*)c->d_rho, zeroed && presorted,
+                               c->stream));
       c->fixed_pending = defer;
     }
   } else {
@@ -414,10 +417,12 @@ gse_status_t do_spread(gse_context_t* c, int n, const void* dx, const double box
   return GSE_OK;
 }
 
+// after_solve: the gather directly follows the own FFT's last kernel on the
+// stream (forward_body), so it may be launched as that kernel's dependent.
 template <typename CT>
 gse_status_t do_gather(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
                        double rcut, const CT* phi, double outscale, double* fx, double* fy,
-                       double* fz, bool presorted = false) {
+                       double* fz, bool presorted = false, bool after_solve = false) {
   typedef typename Vec4<CT>::type V;
   const Stencil<CT> s = stencil_of<CT>(c, box, sigma, rcut, true, false);
   if (n == 0) return GSE_OK;
@@ -426,7 +431,8 @@ gse_status_t do_gather(gse_context_t* c, int n, const void* dx, const double box
   c->launches += 1;
   if (tiled_ok<CT>(c, s))
     CU(launch_gather_tiled<CT>((const V*)c->d_sorted, c->d_perm, c->d_bstart, c->bl, s, phi,
-                               outscale, fx, fy, fz, c->stream));
+                               outscale, fx, fy, fz,
+                               after_solve && presorted && c->own_fft && !c->timing, c->stream));
   else
     CU(launch_gather<CT>((const V*)c->d_sorted, c->d_perm, n, s, phi, outscale, fx, fy, fz,
                          c->stream));
@@ -543,9 +549,13 @@ gse_status_t do_solve_ctx(gse_context_t* c) {
       StageTimer tm(c, GSE_STAGE_FFT_FORWARD);
       c->launches += 1;
       const bool fx = c->fixed_pending;
+      // from a deferred spread (forward_body) the solve follows the spread
+      // kernel directly, and each pass follows the previous one: dependent
+      // launches, unless stage timing puts events between them
       CU(launch_own_fft_xy_forward(M, fx ? c->d_fixed : nullptr, fx ? nullptr : (float*)c->d_rho,
                                    std::exp2(-(double)kFlushBits), fx ? (float*)c->d_rho : nullptr,
-                                   (float2*)c->d_rhok, c->d_fft_tw, c->stream));
+                                   (float2*)c->d_rhok, c->d_fft_tw, c->bl.flags,
+                                   fx && !c->timing, c->stream));
       c->fixed_pending = false;
     }
     {
@@ -554,12 +564,12 @@ gse_status_t do_solve_ctx(gse_context_t* c) {
       CU(launch_own_fft_z_green(M, (float2*)c->d_rhok, (const float*)c->d_gtab, c->d_fft_tw,
                                 c->d_partials,
                                 reinterpret_cast<unsigned*>(c->d_partials + kEnergyPartials),
-                                energy_factor(c), c->d_scalars, c->stream));
+                                energy_factor(c), c->d_scalars, !c->timing, c->stream));
     }
     StageTimer tm(c, GSE_STAGE_FFT_BACKWARD);
     c->launches += 1;
     CU(launch_own_fft_xy_inverse(M, (const float2*)c->d_rhok, (float*)c->d_phi, c->d_fft_tw,
-                                 c->stream));
+                                 c->bl.flags, !c->timing, c->stream));
     return GSE_OK;
   }
   if (!c->green_cb_tried && c->size >= kGreenCallbackMinPoints) {
@@ -636,6 +646,8 @@ gse_status_t check_finite(gse_context_t* c) {
   if (c->h_bad && *c->h_bad) {
     const int f = *c->h_bad;
     *c->h_bad = 0;
+    if (f == kFlagStall)
+      return fail(GSE_ERR_TIMEOUT, "a bounded wait for a staged copy in the FFT gave up");
     if (f == kFlagRange)
       return fail(GSE_ERR_RANGE,
                   "the charge in one 16^3-cell brick exceeds the mixed form's fixed-point range "
@@ -659,16 +671,17 @@ gse_status_t finish(gse_context_t* c, bool host_outputs) {
 template <typename CT>
 gse_status_t gather_to(gse_context_t* c, int n, const void* dx, const double box[3], double sigma,
                        double rcut, const CT* phi, double outscale, double* fx, double* fy,
-                       double* fz, bool* host, bool presorted = false) {
+                       double* fz, bool* host, bool presorted = false, bool after_solve = false) {
   const bool direct = fx && fy && fz && is_device_ptr(fx) && is_device_ptr(fy) && is_device_ptr(fz);
   if (direct)
-    return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz, presorted);
+    return do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, fx, fy, fz, presorted,
+                         after_solve);
   double* f = c->d_force;
   // three outputs that are consecutive rows of one [3][n] array take one copy
   const bool rows = fx && fy == fx + n && fz == fx + 2 * (size_t)n;
   const size_t stride = rows ? (size_t)n : c->atom_cap;
   TRY(do_gather<CT>(c, n, dx, box, sigma, rcut, phi, outscale, f, f + stride, f + 2 * stride,
-                    presorted));
+                    presorted, after_solve));
   if (n == 0) return GSE_OK;
   if (rows) return copy_out(c, fx, f, 3 * (size_t)n * sizeof(double), host);
   if (fx) TRY(copy_out(c, fx, f, n * sizeof(double), host));
@@ -1052,15 +1065,22 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
   const void* dx = nullptr;
   TRY(stage_atoms(c, n, xyzq, &dx));
   const Box3 box = ctx_box(c);
-  // one stable sort serves the spread and the gather
-  if (c->fp64)
+  // one stable sort serves the spread and the gather; the mixed form clears
+  // its int64 grid first, so that the spread follows the binning directly
+  // (kept inside the spread stage when stages are timed)
+  bool zeroed = false;
+  if (c->fp64) {
     TRY(bin_atoms<double>(c, n, dx, stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false)));
-  else
-    TRY(bin_atoms<float>(c, n, dx, stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false)));
+  } else {
+    const Stencil<float> s = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false);
+    zeroed = !c->timing && tiled_ok<float>(c, s);
+    if (zeroed) CU(cudaMemsetAsync(c->d_fixed, 0, sizeof(long long) * c->size, c->stream));
+    TRY(bin_atoms<float>(c, n, dx, s));
+  }
   if (c->fp64)
     TRY(do_spread<double>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));
   else
-    TRY(do_spread<float>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true, true));
+    TRY(do_spread<float>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true, true, zeroed));
   TRY(do_solve_ctx(c));
   c->phi_valid = true;
   c->energy_valid = true;
@@ -1070,7 +1090,7 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
                             c->p.ccelec, fx, fy, fz, host, true));
     else
       TRY(gather_to<float>(c, n, dx, box.v, c->sigma1, c->rcut1, (const float*)c->d_phi,
-                           c->p.ccelec, fx, fy, fz, host, true));
+                           c->p.ccelec, fx, fy, fz, host, true, true));
   }
   return energy_out(c, energy, host);
 }

@@ -26,6 +26,8 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdint>
+#include <type_traits>
 #include <vector>
 
 #include "gse_reduce.cuh"
@@ -219,8 +221,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
   float2* S = fsm + M * X;  // [kHalfWarps][M]
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  pdl_trigger();
   LaneTw<N2> lt;
   lt.load(tw, l);
+  pdl_wait();
   const long long plane = (long long)M * M;
   const long long z0 = (long long)blockIdx.x * plane;
   float2* Z = S + hw * M;
@@ -286,8 +290,10 @@ __global__ void __launch_bounds__(kColThreads, z_blocks(N2))
   __shared__ float G[M][17];
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  pdl_trigger();
   LaneTw<N2> lt;
   lt.load(tw, l);
+  pdl_wait();
   const int xt = blockIdx.x % NXT, y = blockIdx.x / NXT;
   const int x0 = xt * 16, nx = min(16, X - x0);
   const long long zs = (long long)M * X;
@@ -359,8 +365,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
   float* S = reinterpret_cast<float*>(fsm + M * X);    // [kHalfWarps][2M]
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
   const unsigned mask = 0xFFFFu << (tid & 16);
+  pdl_trigger();
   LaneTw<N2> lt;
   lt.load(tw, l);
+  pdl_wait();
   copy_in(P, rhok + (long long)blockIdx.x * M * X, M * X);
   __syncthreads();
   // inverse y: each x' column in place
@@ -377,6 +385,252 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
   // c2r x: the half spectra A (row 2p) and B (row 2p+1), extended by
   // Hermitian symmetry, combined as A + iB; one inverse transform gives row
   // 2p in the real and row 2p+1 in the imaginary part
+  float* T = S + hw * 2 * M;
+  float* out = phi + (long long)blockIdx.x * M * M;
+  for (int pr = hw; pr < M / 2; pr += kHalfWarps) {
+    const float2* Pa = P + (2 * pr) * X;
+    const float2* Pb = Pa + X;
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) {
+      const int k = l + 16 * j;
+      float2 A, B;
+      if (2 * k <= M) {
+        A = Pa[k];
+        B = Pb[k];
+        if (k == 0 || 2 * k == M) {
+          A.y = 0.f;
+          B.y = 0.f;
+        }
+      } else {
+        A = Pa[M - k];
+        B = Pb[M - k];
+        A.y = -A.y;
+        B.y = -B.y;
+      }
+      v[j] = make_float2(A.x - B.y, A.y + B.x);
+    }
+    fft16<N2, true>(v, l, mask, lt);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) {
+      T[k2 + N2 * k1] = v[k2].x;
+      T[M + k2 + N2 * k1] = v[k2].y;
+    }
+    __syncwarp(mask);
+    float* ra = out + (long long)(2 * pr) * M;
+    for (int i = l; i < M; i += 16) {
+      ra[i] = T[i];
+      ra[M + i] = T[M + i];
+    }
+    __syncwarp(mask);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plane passes with the plane staged by bulk copies
+// ---------------------------------------------------------------------------
+// The same transforms, the plane brought into shared memory by the copy
+// engine (cp.async.bulk, completion counted on an mbarrier) instead of by
+// each lane's loads: the forward pass stages its input in one copy per round
+// of x transforms (2 kHalfWarps rows), so a round starts as soon as its rows
+// have arrived, and writes the half spectrum over rows it has consumed; the
+// inverse pass stages the whole half spectrum in one copy.  Used where the
+// plane and the scratch rows fit in shared memory (M <= 144 from the int64
+// grid).  Every wait is bounded: past kStageWaitCycles the CTA sets
+// kFlagStall in `flags` and returns without writing.
+constexpr long long kStageWaitCycles = 2000000000LL;  // about a second
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void stage_bulk(void* dst, const void* src, unsigned bytes,
+                                           unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Wait for phase 0 of `bar`; false when kStageWaitCycles pass first.
+__device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_u32(bar))
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kStageWaitCycles) return false;
+  }
+}
+
+// Byte layout of the forward pass's shared memory for input element In:
+// region A holds the staged input plane at offset `in_off` and, as the
+// rounds consume it, the half spectrum P [M][X] from offset 0 (P's rows of
+// a round end before the input rows of the next round start); then the
+// scratch rows [kHalfWarps][M] complex.
+template <int N2, typename In>
+struct StagedFwd {
+  static constexpr int M = 16 * N2, X = M / 2 + 1;
+  static constexpr int kRows = 2 * kHalfWarps;  // rows per round
+  static constexpr int kRounds = (M + kRows - 1) / kRows;
+  static constexpr long long p_pair = 2LL * X * sizeof(float2), in_pair = 2LL * M * sizeof(In);
+  static constexpr long long lag = p_pair > in_pair ? (p_pair - in_pair) * kHalfWarps : 0;
+  static constexpr size_t in_off = (size_t)(lag * (kRounds - 1) + 15) / 16 * 16;
+  static constexpr size_t in_bytes = sizeof(In) * (size_t)M * M;
+  static constexpr size_t p_bytes = sizeof(float2) * (size_t)M * X;
+  static constexpr size_t a_bytes =
+      ((in_off + in_bytes > p_bytes ? in_off + in_bytes : p_bytes) + 15) / 16 * 16;
+  static constexpr size_t bytes = a_bytes + sizeof(float2) * kHalfWarps * (size_t)M;
+  static_assert(kRounds <= 3, "three staging barriers");
+};
+
+template <int N2, bool FIXED>
+__global__ void __launch_bounds__(kPlaneThreads, 1)
+    k_own_fft_xy_fwd_staged(const long long* __restrict__ g64, const float* __restrict__ rho,
+                            double unscale, float* __restrict__ rho_out,
+                            float2* __restrict__ rhok, const float2* __restrict__ tw,
+                            int* __restrict__ flags) {
+  typedef typename std::conditional<FIXED, long long, float>::type In;
+  typedef StagedFwd<N2, In> L;
+  constexpr int M = L::M, X = L::X;
+  extern __shared__ __align__(16) unsigned char smb[];
+  __shared__ unsigned long long bars[3];
+  float2* P = reinterpret_cast<float2*>(smb);                           // [M][X]
+  const In* stg = reinterpret_cast<const In*>(smb + L::in_off);        // [M][M]
+  float2* S = reinterpret_cast<float2*>(smb + L::a_bytes);              // [kHalfWarps][M]
+  const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
+  const unsigned mask = 0xFFFFu << (tid & 16);
+  const long long plane = (long long)M * M;
+  const In* src = (FIXED ? reinterpret_cast<const In*>(g64) : reinterpret_cast<const In*>(rho)) +
+                  (long long)blockIdx.x * plane;
+  pdl_trigger();
+  if (tid == 0) {
+#pragma unroll
+    for (int r = 0; r < L::kRounds; r++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[r])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  LaneTw<N2> lt;
+  lt.load(tw, l);
+  pdl_wait();
+  if (tid == 0) {
+#pragma unroll
+    for (int r = 0; r < L::kRounds; r++) {
+      const int r0 = r * L::kRows, nr = min(L::kRows, M - r0);
+      stage_bulk(smb + L::in_off + sizeof(In) * (size_t)r0 * M, src + (long long)r0 * M,
+                 (unsigned)(sizeof(In) * nr * M), &bars[r]);
+    }
+  }
+  __syncthreads();  // barriers initialised before anyone waits on them
+  float2* Z = S + hw * M;
+  const long long z0 = (long long)blockIdx.x * plane;
+#pragma unroll 1
+  for (int r = 0; r < L::kRounds; r++) {
+    const bool ok = __syncthreads_and(stage_wait(&bars[r]));
+    if (!ok) {
+      if (tid == 0 && flags) *flags = kFlagStall;
+      return;
+    }
+    const int pr = r * kHalfWarps + hw;
+    const bool has = pr < M / 2;
+    float2 v[N2];
+    if (has) {
+      const In* ra = stg + (2 * pr) * M;
+#pragma unroll
+      for (int j = 0; j < N2; j++) {
+        const int x = l + 16 * j;
+        float a, b;
+        if (FIXED) {
+          a = (float)((double)ra[x] * unscale);
+          b = (float)((double)ra[M + x] * unscale);
+          if (rho_out) {
+            rho_out[z0 + (2 * pr) * M + x] = a;
+            rho_out[z0 + (2 * pr + 1) * M + x] = b;
+          }
+        } else {
+          a = ra[x];
+          b = ra[M + x];
+        }
+        v[j] = make_float2(a, b);
+      }
+    }
+    __syncthreads();  // the round's rows are read before P is written over them
+    if (has) {
+      fft16<N2, false>(v, l, mask, lt);
+      const int k1 = brev4(l);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; k2++) Z[k2 + N2 * k1] = v[k2];
+      __syncwarp(mask);
+      float2* Pa = P + (2 * pr) * X;
+      float2* Pb = Pa + X;
+      for (int k = l; k < X; k += 16) {
+        const float2 zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
+        Pa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        Pb[k] = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+      }
+      __syncwarp(mask);
+    }
+  }
+  __syncthreads();
+  for (int col = hw; col < X; col += kHalfWarps) {
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
+    fft16<N2, false>(v, l, mask, lt);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
+  }
+  __syncthreads();
+  float2* out = rhok + (long long)blockIdx.x * M * X;
+  for (int i = tid; i < M * X; i += kPlaneThreads) out[i] = P[i];
+}
+
+template <int N2>
+__global__ void __launch_bounds__(kPlaneThreads, 1)
+    k_own_fft_xy_inv_staged(const float2* __restrict__ rhok, float* __restrict__ phi,
+                            const float2* __restrict__ tw, int* __restrict__ flags) {
+  constexpr int M = 16 * N2, X = M / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smb[];
+  __shared__ unsigned long long bar;
+  float2* P = reinterpret_cast<float2*>(smb);                                  // [M][X]
+  float* S = reinterpret_cast<float*>(smb + sizeof(float2) * (size_t)M * X);   // [kHalfWarps][2M]
+  const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
+  const unsigned mask = 0xFFFFu << (tid & 16);
+  pdl_trigger();
+  LaneTw<N2> lt;
+  lt.load(tw, l);
+  pdl_wait();
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    stage_bulk(P, rhok + (long long)blockIdx.x * M * X, (unsigned)(sizeof(float2) * M * X), &bar);
+  }
+  __syncthreads();
+  if (!__syncthreads_and(stage_wait(&bar))) {
+    if (tid == 0 && flags) *flags = kFlagStall;
+    return;
+  }
+  for (int col = hw; col < X; col += kHalfWarps) {
+    float2 v[N2];
+#pragma unroll
+    for (int j = 0; j < N2; j++) v[j] = P[(l + 16 * j) * X + col];
+    fft16<N2, true>(v, l, mask, lt);
+    const int k1 = brev4(l);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; k2++) P[(k2 + N2 * k1) * X + col] = v[k2];
+  }
+  __syncthreads();
   float* T = S + hw * 2 * M;
   float* out = phi + (long long)blockIdx.x * M * M;
   for (int pr = hw; pr < M / 2; pr += kHalfWarps) {
@@ -466,44 +720,91 @@ cudaError_t allow_smem(K kernel, size_t bytes, std::atomic<bool> (&done)[64]) {
   return cudaSuccess;
 }
 
+// Largest dynamic shared memory a block may opt in to on the current device.
+size_t optin_smem() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  int v = cache[dev].load();
+  if (v == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+      return 0;
+    cache[dev] = v;
+  }
+  return (size_t)v;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 template <int N2>
 cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float* rho_out,
-                   float2* rhok, const float2* tw, cudaStream_t st) {
+                   float2* rhok, const float2* tw, int* flags, bool pdl, cudaStream_t st) {
   constexpr int M = 16 * N2;
   constexpr size_t smem = plane_smem<N2>();
-  static std::atomic<bool> fx[64], fl[64];
+  static std::atomic<bool> fx[64], fl[64], sx[64], sl[64];
+  if (aligned16(g64 ? (const void*)g64 : (const void*)rho)) {
+    if (g64 && StagedFwd<N2, long long>::bytes <= optin_smem()) {
+      constexpr size_t sm = StagedFwd<N2, long long>::bytes;
+      cudaError_t e = allow_smem(k_own_fft_xy_fwd_staged<N2, true>, sm, sx);
+      if (e != cudaSuccess) return e;
+      e = launch_dependent(pdl, k_own_fft_xy_fwd_staged<N2, true>, dim3(M), dim3(kPlaneThreads),
+                           sm, st, g64, rho, unscale, rho_out, rhok, tw, flags);
+      return e != cudaSuccess ? e : cudaGetLastError();
+    }
+    if (!g64 && StagedFwd<N2, float>::bytes <= optin_smem()) {
+      constexpr size_t sm = StagedFwd<N2, float>::bytes;
+      cudaError_t e = allow_smem(k_own_fft_xy_fwd_staged<N2, false>, sm, sl);
+      if (e != cudaSuccess) return e;
+      e = launch_dependent(pdl, k_own_fft_xy_fwd_staged<N2, false>, dim3(M),
+                           dim3(kPlaneThreads), sm, st, g64, rho, unscale, rho_out, rhok, tw,
+                           flags);
+      return e != cudaSuccess ? e : cudaGetLastError();
+    }
+  }
   if (g64) {
     cudaError_t e = allow_smem(k_own_fft_xy_fwd<N2, true>, smem, fx);
     if (e != cudaSuccess) return e;
-    k_own_fft_xy_fwd<N2, true><<<M, kPlaneThreads, smem, st>>>(g64, rho, unscale, rho_out, rhok,
-                                                               tw);
+    e = launch_dependent(pdl, k_own_fft_xy_fwd<N2, true>, dim3(M), dim3(kPlaneThreads), smem,
+                         st, g64, rho, unscale, rho_out, rhok, tw);
+    if (e != cudaSuccess) return e;
   } else {
     cudaError_t e = allow_smem(k_own_fft_xy_fwd<N2, false>, smem, fl);
     if (e != cudaSuccess) return e;
-    k_own_fft_xy_fwd<N2, false><<<M, kPlaneThreads, smem, st>>>(g64, rho, unscale, rho_out,
-                                                                rhok, tw);
+    e = launch_dependent(pdl, k_own_fft_xy_fwd<N2, false>, dim3(M), dim3(kPlaneThreads), smem,
+                         st, g64, rho, unscale, rho_out, rhok, tw);
+    if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();
 }
 
 template <int N2>
 cudaError_t z_n2(float2* rhok, const float* tab, const float2* tw, double* partials,
-                 unsigned* done, double factor, double* out, cudaStream_t st) {
+                 unsigned* done, double factor, double* out, bool pdl, cudaStream_t st) {
   constexpr int M = 16 * N2, X = M / 2 + 1, NXT = (X + 15) / 16;
-  k_own_fft_z_green<N2><<<NXT * M, kColThreads, 0, st>>>(rhok, tab, tw, partials, done, factor,
-                                                          out);
-  return cudaGetLastError();
+  const cudaError_t e = launch_dependent(pdl, k_own_fft_z_green<N2>, dim3(NXT * M),
+                                         dim3(kColThreads), 0, st, rhok, tab, tw, partials, done,
+                                         factor, out);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int N2>
-cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, cudaStream_t st) {
+cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, int* flags, bool pdl,
+                   cudaStream_t st) {
   constexpr int M = 16 * N2;
   constexpr size_t smem = plane_smem<N2>();
-  static std::atomic<bool> fi[64];
+  static std::atomic<bool> fi[64], si[64];
+  if (aligned16(rhok) && smem <= optin_smem()) {
+    cudaError_t e = allow_smem(k_own_fft_xy_inv_staged<N2>, smem, si);
+    if (e != cudaSuccess) return e;
+    e = launch_dependent(pdl, k_own_fft_xy_inv_staged<N2>, dim3(M), dim3(kPlaneThreads), smem,
+                         st, rhok, phi, tw, flags);
+    return e != cudaSuccess ? e : cudaGetLastError();
+  }
   cudaError_t e = allow_smem(k_own_fft_xy_inv<N2>, smem, fi);
   if (e != cudaSuccess) return e;
-  k_own_fft_xy_inv<N2><<<M, kPlaneThreads, smem, st>>>(rhok, phi, tw);
-  return cudaGetLastError();
+  e = launch_dependent(pdl, k_own_fft_xy_inv<N2>, dim3(M), dim3(kPlaneThreads), smem, st, rhok,
+                       phi, tw);
+  return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace
@@ -524,26 +825,26 @@ cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, cudaStream_
 
 cudaError_t launch_own_fft_xy_forward(int M, const long long* g64, const float* rho,
                                       double unscale, float* rho_out, float2* rhok,
-                                      const float2* tw, cudaStream_t st) {
+                                      const float2* tw, int* flags, bool pdl, cudaStream_t st) {
   if (M % 16) return cudaErrorInvalidValue;
-#define CALL_FWD(N) fwd_n2<N>(g64, rho, unscale, rho_out, rhok, tw, st)
+#define CALL_FWD(N) fwd_n2<N>(g64, rho, unscale, rho_out, rhok, tw, flags, pdl, st)
   GSE_FFT_SWITCH(CALL_FWD)
 #undef CALL_FWD
 }
 
 cudaError_t launch_own_fft_z_green(int M, float2* rhok, const float* tab, const float2* tw,
                                    double* partials, unsigned* done, double factor,
-                                   double* energy_out, cudaStream_t st) {
+                                   double* energy_out, bool pdl, cudaStream_t st) {
   if (M % 16) return cudaErrorInvalidValue;
-#define CALL_Z(N) z_n2<N>(rhok, tab, tw, partials, done, factor, energy_out, st)
+#define CALL_Z(N) z_n2<N>(rhok, tab, tw, partials, done, factor, energy_out, pdl, st)
   GSE_FFT_SWITCH(CALL_Z)
 #undef CALL_Z
 }
 
 cudaError_t launch_own_fft_xy_inverse(int M, const float2* rhok, float* phi, const float2* tw,
-                                      cudaStream_t st) {
+                                      int* flags, bool pdl, cudaStream_t st) {
   if (M % 16) return cudaErrorInvalidValue;
-#define CALL_INV(N) inv_n2<N>(rhok, phi, tw, st)
+#define CALL_INV(N) inv_n2<N>(rhok, phi, tw, flags, pdl, st)
   GSE_FFT_SWITCH(CALL_INV)
 #undef CALL_INV
 }

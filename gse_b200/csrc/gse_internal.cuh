@@ -9,6 +9,37 @@
 
 namespace gse {
 
+// Programmatic dependent launch between consecutive kernels of this library
+// on one stream: a kernel launched by launch_dependent() may be scheduled
+// while its predecessor is still running; it runs its own set-up, then
+// pdl_wait() returns once the predecessor has completed and its writes are
+// visible.  Every kernel so launched calls pdl_wait() on every path before
+// it reads a predecessor's output or exits, so completion carries down the
+// chain.  pdl_trigger() lets the successor be scheduled once every block of
+// the current kernel has started.  Both are no-ops for a normal launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch `kernel` on `st` after the kernel before it on the stream, with
+// programmatic serialisation when `pdl` (the kernel must call pdl_wait()).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                             size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Streaming multiprocessors of the current device (148 on a B200), looked up
 // once per device; grid-stride kernels size their grids as multiples of it.
 inline int sm_count() {
@@ -43,6 +74,12 @@ template <> struct Cplx<float> { typedef float2 type; };
 // Stencil constants of one spread or gather call, derived on the host exactly
 // as CpuGaussCharge computes them (CpuGaussCharge.cpp:114-128 and :244-258):
 // the spacing and its inverse in double, then cast to CT.
+// Values of a context's status flag (a host-mapped int that kernels set and the
+// host reads after a synchronisation).
+constexpr int kFlagNonFinite = 1;  // a position or charge is NaN or infinite
+constexpr int kFlagRange = 2;      // a brick's charge overflows the mixed form's tile range
+constexpr int kFlagStall = 4;      // a bounded wait in a kernel gave up
+
 template <typename CT>
 struct Stencil {
   int M[3];      // grid sizes
@@ -111,6 +148,12 @@ __device__ __forceinline__ int round_to_int(float v) { return (int)roundf(v); }
 
 __device__ __forceinline__ double gexp(double v) { return exp(v); }
 __device__ __forceinline__ float gexp(float v) { return expf(v); }
+// Stencil weights of the forward spread and gather: exp in the FP64 form; in
+// the mixed form the hardware exponential (__expf: ex2.approx of x log2 e),
+// within about 1e-6 relative for the exponents of these stencils (|x| < 40),
+// which moves the mixed forces against the FP64 reference by less than 1e-7.
+__device__ __forceinline__ double wexp(double v) { return exp(v); }
+__device__ __forceinline__ float wexp(float v) { return __expf(v); }
 
 __device__ __forceinline__ int pmod(int a, int m) {
   int r = a % m;

@@ -38,6 +38,7 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
                             CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
                             int* __restrict__ counts, unsigned* __restrict__ qmax_bits,
                             int* __restrict__ bad) {
+  pdl_trigger();
   float qm = 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const auto a = xyzq[i];
@@ -74,6 +75,8 @@ constexpr int kScanTile = kScanPer * kScanThreads;
 __global__ void __launch_bounds__(kScanThreads)
     k_scan_tiles(const int* __restrict__ counts, int nb, int* __restrict__ start,
                  int* __restrict__ tile_sums) {
+  pdl_trigger();
+  pdl_wait();
   const int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
   int v[kScanPer];
   int s = 0;
@@ -152,6 +155,8 @@ __global__ void __launch_bounds__(256)
                       const int* __restrict__ lstart, const int* __restrict__ tile_sums,
                       int ntiles, int* __restrict__ counts, float4* __restrict__ sorted,
                       int* __restrict__ perm, int* __restrict__ start, int nb) {
+  pdl_trigger();
+  pdl_wait();
   __shared__ int off[kScanTile];
   constexpr int PER = kScanTile / 256;
   {
@@ -531,7 +536,7 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
         const int c = centre_cell(pos3[d], s.inv_h[d]);
         loc[d] = wrap1(c, s.M[d]) - org[d];  // window start in tile coordinates
         const float dd = sub_rn(mul_rn((float)(c - n + lane), s.h[d]), pos3[d]);
-        wl[d] = (lane < W) ? expf(mul_rn(mul_rn(-dd, dd), s.inv_2s2)) : 0.f;
+        wl[d] = (lane < W) ? wexp(mul_rn(mul_rn(-dd, dd), s.inv_2s2)) : 0.f;
       }
       float wy[W];
 #pragma unroll
@@ -581,6 +586,8 @@ template <int W>
 __global__ void __launch_bounds__(kScatterThreads)
     k_spread_scatter(const float4* __restrict__ sorted, const int* __restrict__ start,
                      BinLayout b, Stencil<float> s, long long* __restrict__ grid64) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ int tile[];
   scatter_brick<W>(sorted, start, b, s, blockIdx.x, blockIdx.y, blockIdx.z, tile, grid64);
 }
@@ -762,7 +769,7 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
           const CT d2 = mul_rn(dd, dd);
           tb[(d * 3 + 0) * kWPad + j] = dd;
           tb[(d * 3 + 1) * kWPad + j] = d2;
-          tb[(d * 3 + 2) * kWPad + j] = gexp(mul_rn(-d2, s.inv_2s2));
+          tb[(d * 3 + 2) * kWPad + j] = wexp(mul_rn(-d2, s.inv_2s2));
         }
       }
       __syncwarp();
@@ -851,6 +858,7 @@ __global__ void __launch_bounds__(kGatherThreads, sizeof(CT) == 4 ? 2 : 1)
                    const int* __restrict__ perm, const int* __restrict__ start, BinLayout b,
                    Stencil<CT> s, const CT* __restrict__ phi, double outscale,
                    double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz) {
+  pdl_wait();
   extern __shared__ __align__(16) unsigned char gsm[];
   gather_brick<CT, W>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, blockIdx.x,
                       blockIdx.y, blockIdx.z, gsm);
@@ -897,9 +905,16 @@ cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, in
   const int gb = (int)std::min<long long>(sm_count() * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (sizeof(CT) == 4 && w.lstart) {
     // two kernels: tile-local scan, then placement with the tile offsets
-    k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.lstart, w.tile_sums);
-    k_bin_place_final<<<gb, 256, 0, st>>>((const float4*)xyzq, n, w.key, w.lstart, w.tile_sums,
-                                          ntiles, w.counts, (float4*)sorted, perm, w.start, nb);
+    // each kernel follows the previous one of the binning on the stream
+    // (the counts, when there are atoms)
+    e = launch_dependent(n > 0, k_scan_tiles, dim3(ntiles), dim3(kScanThreads), 0, st, w.counts,
+                         nb, w.lstart, w.tile_sums);
+    if (e != cudaSuccess) return e;
+    e = launch_dependent(true, k_bin_place_final, dim3(gb), dim3(256), 0, st,
+                         (const float4*)xyzq, n, (const int*)w.key, (const int*)w.lstart,
+                         (const int*)w.tile_sums, ntiles, w.counts, (float4*)sorted, perm,
+                         w.start, nb);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
   }
   k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(w.counts, nb, w.start, w.tile_sums);
@@ -955,7 +970,7 @@ template <typename CT, int W>
 static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* perm,
                             const int* start, const BinLayout& b, const Stencil<CT>& s,
                             const CT* phi, double outscale, double* fx, double* fy, double* fz,
-                            cudaStream_t st) {
+                            bool pdl, cudaStream_t st) {
   const size_t smem = GatherGeom<CT, W>::bytes;
   static std::atomic<bool> attr[64];
   int dev = 0;
@@ -968,8 +983,10 @@ static cudaError_t gather_w(const typename Vec4<CT>::type* sorted, const int* pe
     attr[dev] = true;
   }
   dim3 grd((b.M[0] + kGX - 1) / kGX, (b.M[1] + kGY - 1) / kGY, (b.M[2] + kGZ - 1) / kGZ);
-  k_gather_tiled<CT, W><<<grd, kGatherThreads, smem, st>>>(sorted, perm, start, b, s, phi,
-                                                          outscale, fx, fy, fz);
+  const cudaError_t e = launch_dependent(pdl, k_gather_tiled<CT, W>, grd, dim3(kGatherThreads),
+                                         smem, st, sorted, perm, start, b, s, phi, outscale, fx,
+                                         fy, fz);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
@@ -977,12 +994,15 @@ template <typename CT>
 cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int* perm,
                                 const int* start, const BinLayout& b, const Stencil<CT>& s,
                                 const CT* phi, double outscale, double* fx, double* fy,
-                                double* fz, cudaStream_t st) {
+                                double* fz, bool pdl, cudaStream_t st) {
   switch (2 * s.nst[0] + 1) {
-    case 9: return gather_w<CT, 9>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
-    case 11: return gather_w<CT, 11>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
-    case 13: return gather_w<CT, 13>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
-    case 15: return gather_w<CT, 15>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, st);
+    case 9: return gather_w<CT, 9>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, pdl, st);
+    case 11:
+      return gather_w<CT, 11>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, pdl, st);
+    case 13:
+      return gather_w<CT, 13>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, pdl, st);
+    case 15:
+      return gather_w<CT, 15>(sorted, perm, start, b, s, phi, outscale, fx, fy, fz, pdl, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -995,7 +1015,7 @@ cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float
 
 template <int W>
 static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLayout& b,
-                             const Stencil<float>& s, long long* grid64, float* rho,
+                             const Stencil<float>& s, long long* grid64, float* rho, bool zeroed,
                              cudaStream_t st) {
   typedef ScatterGeom<W> G;
   const size_t smem = sizeof(int) * G::words;
@@ -1010,12 +1030,15 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
     attr[dev] = true;
   }
   const long long size = (long long)b.M[0] * b.M[1] * b.M[2];
-  cudaError_t e = cudaMemsetAsync(grid64, 0, sizeof(long long) * size, st);
+  cudaError_t e = cudaSuccess;
+  if (!zeroed) e = cudaMemsetAsync(grid64, 0, sizeof(long long) * size, st);
   if (e != cudaSuccess) return e;
   const int nb[3] = {(b.M[0] + kSB - 1) / kSB, (b.M[1] + kSB - 1) / kSB,
                      (b.M[2] + kSB - 1) / kSB};
-  k_spread_scatter<W><<<dim3(nb[0], nb[1], nb[2]), kScatterThreads, smem, st>>>(sorted, start, b,
-                                                                              s, grid64);
+  // with the grid cleared earlier the spread follows the binning's last kernel
+  e = launch_dependent(zeroed, k_spread_scatter<W>, dim3(nb[0], nb[1], nb[2]),
+                       dim3(kScatterThreads), smem, st, sorted, start, b, s, grid64);
+  if (e != cudaSuccess) return e;
   // rho == nullptr: the caller converts the int64 grid itself (the own FFT)
   if (rho) k_grid64_to_real<<<sm_count() * 8, 256, 0, st>>>(grid64, size, rho);
   return cudaGetLastError();
@@ -1023,12 +1046,12 @@ static cudaError_t scatter_w(const float4* sorted, const int* start, const BinLa
 
 cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
                                   const Stencil<float>& s, long long* grid64, float* rho,
-                                  cudaStream_t st) {
+                                  bool zeroed, cudaStream_t st) {
   switch (2 * s.nst[0] + 1) {
-    case 9: return scatter_w<9>(sorted, start, b, s, grid64, rho, st);
-    case 11: return scatter_w<11>(sorted, start, b, s, grid64, rho, st);
-    case 13: return scatter_w<13>(sorted, start, b, s, grid64, rho, st);
-    case 15: return scatter_w<15>(sorted, start, b, s, grid64, rho, st);
+    case 9: return scatter_w<9>(sorted, start, b, s, grid64, rho, zeroed, st);
+    case 11: return scatter_w<11>(sorted, start, b, s, grid64, rho, zeroed, st);
+    case 13: return scatter_w<13>(sorted, start, b, s, grid64, rho, zeroed, st);
+    case 15: return scatter_w<15>(sorted, start, b, s, grid64, rho, zeroed, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -1433,7 +1456,8 @@ cudaError_t launch_batch_forward_fused(const BatchFused& a, int ctas, int gather
                                                const Stencil<CT>&, CT*, cudaStream_t);          \
   template cudaError_t launch_gather_tiled<CT>(const Vec4<CT>::type*, const int*, const int*,   \
                                                const BinLayout&, const Stencil<CT>&, const CT*, \
-                                               double, double*, double*, double*, cudaStream_t);
+                                               double, double*, double*, double*, bool,         \
+                                               cudaStream_t);
 
 GSE_TILED_INST(double)
 GSE_TILED_INST(float)

@@ -44,9 +44,6 @@ struct BinLayout {
   // fixed-point range of its int32 tile (may be NULL: not reported)
   int* flags = nullptr;
 };
-// Values of the context's status flag (host-mapped int, read after a sync).
-constexpr int kFlagNonFinite = 1;  // a position or charge is NaN or infinite
-constexpr int kFlagRange = 2;      // a brick's charge overflows the mixed form's tile range
 
 struct BinScratch {
   int* key;        // [n]
@@ -183,11 +180,14 @@ cudaError_t launch_batch_gather(const float4* sorted, const int* perm, const int
 cudaError_t launch_grid64_to_real(const long long* grid64, long long size, float* out,
                                   cudaStream_t st);
 
-// Mixed-form spread: brick tiles added into the int64 grid `grid64` (cleared
-// here) at 2^40, then converted into the float grid `rho`.
+// Mixed-form spread: brick tiles added into the int64 grid `grid64` at 2^40,
+// then converted into the float grid `rho` (NULL: left to the caller).  The
+// grid is cleared here unless `zeroed`: the caller cleared it before the
+// binning, and the spread then launches as the dependent of the binning's
+// last kernel, which directly precedes it on `st`.
 cudaError_t launch_spread_scatter(const float4* sorted, const int* start, const BinLayout& b,
                                   const Stencil<float>& s, long long* grid64, float* rho,
-                                  cudaStream_t st);
+                                  bool zeroed, cudaStream_t st);
 
 template <typename CT>
 cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const BinLayout& b,
@@ -207,10 +207,12 @@ cudaError_t launch_spread_tiled(const typename Vec4<CT>::type* sorted, const int
                                 const unsigned* qmax_bits, const BinLayout& b,
                                 const Stencil<CT>& s, CT* grid, cudaStream_t st);
 
+// pdl: the launch follows a kernel of this library directly on `st` and may
+// overlap its end (programmatic dependent launch).
 template <typename CT>
 cudaError_t launch_gather_tiled(const typename Vec4<CT>::type* sorted, const int* perm,
                                 const int* start, const BinLayout& b, const Stencil<CT>& s,
                                 const CT* phi, double outscale, double* fx, double* fy,
-                                double* fz, cudaStream_t st);
+                                double* fz, bool pdl, cudaStream_t st);
 
 }  // namespace gse
