@@ -192,6 +192,10 @@ struct gse_context {
   // whether the float rho grid still has to be made from the int64 grid
   float2* d_fft_tw = nullptr;
   bool own_fft = false;
+  // GSE_B200_TEST_FFT_STALL=1 at creation: the staged forward plane pass's
+  // first copy wait runs out (about a millisecond), a test of the
+  // GSE_ERR_TIMEOUT report
+  bool fft_stall_test = false;
   bool fixed_pending = false;
   bool rho_valid = false, phi_valid = false, energy_valid = false;
   // replay of repeated gse_forward calls with device inputs and outputs: the
@@ -555,7 +559,7 @@ gse_status_t do_solve_ctx(gse_context_t* c) {
       CU(launch_own_fft_xy_forward(M, fx ? c->d_fixed : nullptr, fx ? nullptr : (float*)c->d_rho,
                                    std::exp2(-(double)kFlushBits), fx ? (float*)c->d_rho : nullptr,
                                    (float2*)c->d_rhok, c->d_fft_tw, c->bl.flags,
-                                   fx && !c->timing, c->stream));
+                                   fx && !c->timing, c->fft_stall_test, c->stream));
       c->fixed_pending = false;
     }
     {
@@ -865,6 +869,8 @@ gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
       CUC(make_fft_twiddles(M[0], &c->d_fft_tw));
       c->own_fft = true;
     }
+    const char* stall = std::getenv("GSE_B200_TEST_FFT_STALL");
+    c->fft_stall_test = stall && stall[0] == '1';
   }
   c->bl = make_bin_layout(M, c->fp64 ? kBinX64 : kBinX32);
   c->nbins2 = bin_count(c->bl);

@@ -437,9 +437,11 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
 // have arrived, and writes the half spectrum over rows it has consumed; the
 // inverse pass stages the whole half spectrum in one copy.  Used where the
 // plane and the scratch rows fit in shared memory (M <= 144 from the int64
-// grid).  Every wait is bounded: past kStageWaitCycles the CTA sets
-// kFlagStall in `flags` and returns without writing.
-constexpr long long kStageWaitCycles = 2000000000LL;  // about a second
+// grid).  Every wait is bounded: past `wait_cycles` (kStageWaitCycles, about a
+// second) the CTA sets kFlagStall in `flags` and returns without writing.  A
+// test makes the forward pass's first wait run out by expecting `extra_tx`
+// bytes more than its copies bring (every copy still completes).
+constexpr long long kStageWaitCycles = 2000000000LL;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -457,8 +459,8 @@ __device__ __forceinline__ void stage_bulk(void* dst, const void* src, unsigned 
       : "memory");
 }
 
-// Wait for phase 0 of `bar`; false when kStageWaitCycles pass first.
-__device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
+// Wait for phase 0 of `bar`; false when `limit` clock cycles pass first.
+__device__ __forceinline__ bool stage_wait(unsigned long long* bar, long long limit) {
   const long long t0 = clock64();
   for (;;) {
     unsigned done;
@@ -469,7 +471,7 @@ __device__ __forceinline__ bool stage_wait(unsigned long long* bar) {
         : "r"(smem_u32(bar))
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > kStageWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
     k_own_fft_xy_fwd_staged(const long long* __restrict__ g64, const float* __restrict__ rho,
                             double unscale, float* __restrict__ rho_out,
                             float2* __restrict__ rhok, const float2* __restrict__ tw,
-                            int* __restrict__ flags) {
+                            int* __restrict__ flags, unsigned extra_tx, long long wait_cycles) {
   typedef typename std::conditional<FIXED, long long, float>::type In;
   typedef StagedFwd<N2, In> L;
   constexpr int M = L::M, X = L::X;
@@ -527,6 +529,10 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
 #pragma unroll
     for (int r = 0; r < L::kRounds; r++) {
       const int r0 = r * L::kRows, nr = min(L::kRows, M - r0);
+      if (r == 0 && extra_tx)
+        asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[0])),
+                     "r"(extra_tx)
+                     : "memory");
       stage_bulk(smb + L::in_off + sizeof(In) * (size_t)r0 * M, src + (long long)r0 * M,
                  (unsigned)(sizeof(In) * nr * M), &bars[r]);
     }
@@ -536,7 +542,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
   const long long z0 = (long long)blockIdx.x * plane;
 #pragma unroll 1
   for (int r = 0; r < L::kRounds; r++) {
-    const bool ok = __syncthreads_and(stage_wait(&bars[r]));
+    const bool ok = __syncthreads_and(stage_wait(&bars[r], wait_cycles));
     if (!ok) {
       if (tid == 0 && flags) *flags = kFlagStall;
       return;
@@ -617,7 +623,7 @@ __global__ void __launch_bounds__(kPlaneThreads, 1)
     stage_bulk(P, rhok + (long long)blockIdx.x * M * X, (unsigned)(sizeof(float2) * M * X), &bar);
   }
   __syncthreads();
-  if (!__syncthreads_and(stage_wait(&bar))) {
+  if (!__syncthreads_and(stage_wait(&bar, kStageWaitCycles))) {
     if (tid == 0 && flags) *flags = kFlagStall;
     return;
   }
@@ -738,7 +744,10 @@ bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 template <int N2>
 cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float* rho_out,
-                   float2* rhok, const float2* tw, int* flags, bool pdl, cudaStream_t st) {
+                   float2* rhok, const float2* tw, int* flags, bool pdl, bool stall_test,
+                   cudaStream_t st) {
+  const unsigned extra = stall_test ? 16u : 0u;
+  const long long cycles = stall_test ? 2000000LL : kStageWaitCycles;
   constexpr int M = 16 * N2;
   constexpr size_t smem = plane_smem<N2>();
   static std::atomic<bool> fx[64], fl[64], sx[64], sl[64];
@@ -748,7 +757,7 @@ cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float
       cudaError_t e = allow_smem(k_own_fft_xy_fwd_staged<N2, true>, sm, sx);
       if (e != cudaSuccess) return e;
       e = launch_dependent(pdl, k_own_fft_xy_fwd_staged<N2, true>, dim3(M), dim3(kPlaneThreads),
-                           sm, st, g64, rho, unscale, rho_out, rhok, tw, flags);
+                           sm, st, g64, rho, unscale, rho_out, rhok, tw, flags, extra, cycles);
       return e != cudaSuccess ? e : cudaGetLastError();
     }
     if (!g64 && StagedFwd<N2, float>::bytes <= optin_smem()) {
@@ -757,7 +766,7 @@ cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float
       if (e != cudaSuccess) return e;
       e = launch_dependent(pdl, k_own_fft_xy_fwd_staged<N2, false>, dim3(M),
                            dim3(kPlaneThreads), sm, st, g64, rho, unscale, rho_out, rhok, tw,
-                           flags);
+                           flags, extra, cycles);
       return e != cudaSuccess ? e : cudaGetLastError();
     }
   }
@@ -825,9 +834,10 @@ cudaError_t inv_n2(const float2* rhok, float* phi, const float2* tw, int* flags,
 
 cudaError_t launch_own_fft_xy_forward(int M, const long long* g64, const float* rho,
                                       double unscale, float* rho_out, float2* rhok,
-                                      const float2* tw, int* flags, bool pdl, cudaStream_t st) {
+                                      const float2* tw, int* flags, bool pdl, bool stall_test,
+                                      cudaStream_t st) {
   if (M % 16) return cudaErrorInvalidValue;
-#define CALL_FWD(N) fwd_n2<N>(g64, rho, unscale, rho_out, rhok, tw, flags, pdl, st)
+#define CALL_FWD(N) fwd_n2<N>(g64, rho, unscale, rho_out, rhok, tw, flags, pdl, stall_test, st)
   GSE_FFT_SWITCH(CALL_FWD)
 #undef CALL_FWD
 }

@@ -29,10 +29,13 @@ cudaError_t make_fft_twiddles(int M, float2** out);
 // grid, rho_out (if not null) receives the float grid exactly as
 // k_grid64_to_real writes it.  Where the plane fits in shared memory it is
 // staged there by bulk copies; a copy wait that gives up sets kFlagStall in
-// `flags` (may be NULL: not reported).
+// `flags` (may be NULL: not reported).  stall_test: the staged pass expects
+// 16 bytes more than its first copy brings and waits about a millisecond, so
+// that its first wait runs out (a test of that report; every copy completes).
 cudaError_t launch_own_fft_xy_forward(int M, const long long* g64, const float* rho,
                                       double unscale, float* rho_out, float2* rhok,
-                                      const float2* tw, int* flags, bool pdl, cudaStream_t st);
+                                      const float2* tw, int* flags, bool pdl, bool stall_test,
+                                      cudaStream_t st);
 
 // In place on rho^: the z transform of every (y, x') column, the multiply by
 // the Green's table `tab` (same layout) with the k-space energy

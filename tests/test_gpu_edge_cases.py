@@ -231,3 +231,37 @@ def test_mixed_range_overflow_is_reported():
     assert np.isfinite(E)
     c64 = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="fp64")
     assert np.isfinite(c64.forward(n, big, *f))
+
+
+def test_staged_copy_wait_that_runs_out_is_reported(monkeypatch):
+    """The FFT's staged plane copies are awaited with a bounded wait.  With
+    GSE_B200_TEST_FFT_STALL=1 at context creation the forward plane pass
+    expects 16 bytes more than its first copy brings (every copy still
+    completes), so its first wait runs out after about a millisecond: the
+    CTAs set the stall flag and return, and the call reports
+    GSE_ERR_TIMEOUT.  The GPU stays usable: a context made afterwards
+    without the variable evaluates normally."""
+    from gse_b200 import GseError
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
+    M, L = 64, 62.0
+    x = W.triplets(600, L, 5).astype(np.float32)
+    n = x.shape[0]
+    monkeypatch.setenv("GSE_B200_TEST_FFT_STALL", "1")
+    a = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    assert a.paths() & 8
+    f = [np.zeros(n) for _ in range(3)]
+    with pytest.raises(GseError) as ei:
+        a.forward(n, x, *f)
+    assert ei.value.name == "GSE_ERR_TIMEOUT"
+    a.close()
+    monkeypatch.delenv("GSE_B200_TEST_FFT_STALL")
+    b = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    g = [np.zeros(n) for _ in range(3)]
+    E = b.forward(n, x, *g)
+    c = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    h = [np.zeros(n) for _ in range(3)]
+    assert c.forward(n, x, *h) == E
+    assert all(np.array_equal(u, v) for u, v in zip(g, h))
+    b.close()
+    c.close()

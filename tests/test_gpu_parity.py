@@ -384,3 +384,35 @@ def test_benchmark_boxes_match_reference(name):
         assert rms(F[idx], z["F"]) <= tol
         assert rel(f2, float(z["F2sum"])) <= 2 * tol
         assert np.abs(F.sum(axis=0) - z["Fsum"]).max() <= 10 * tol * np.sqrt(float(z["F2sum"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n2", [4, 9, 12])
+def test_split_calls_equal_forward_on_own_fft(n2):
+    """The four separate calls (spread, solve, energy, gather) on a mixed
+    context equal one forward call bit for bit: the solve then starts from
+    the float grid the spread converted, which is exactly the conversion the
+    forward call's solve applies to the int64 grid as it reads it.  M = 64 and
+    144 stage both kinds of plane in shared memory; at M = 192 only the float
+    plane fits, and the int64 plane is read by the lanes' own loads."""
+    from gse_b200 import workloads as W
+    from gse_b200.gse import Context
+    M = 16 * n2
+    L = 0.97 * M
+    x = W.triplets(3000, L, 40 + n2).astype(np.float32)
+    n = x.shape[0]
+    a = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    fa = [np.zeros(n) for _ in range(3)]
+    Ea = a.forward(n, x, *fa)
+    assert a.paths() & 8
+    b = Context(M, M, M, 2.0, 0.4, 3.0, 3.0, L, L, L, precision="mixed")
+    b.spread_charge(n, x)
+    b.solve_poisson()
+    Eb = b.calculate_energy()
+    fb = [np.zeros(n) for _ in range(3)]
+    b.interpolate_force(n, x, *fb)
+    a.close()
+    b.close()
+    assert Ea == Eb
+    for u, v in zip(fa, fb):
+        assert np.array_equal(u, v)
