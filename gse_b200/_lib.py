@@ -116,6 +116,7 @@ SIGNATURES = {
     "gse_batch_launch": (_i, [_vp]),
     "gse_batch_autotune": (_i, [_vp, ctypes.c_char_p, _i]),
     "gse_batch_set_schedule": (_i, [_vp, _i, _i, _i, _i, _i]),
+    "gse_build_info": (ctypes.c_char_p, []),
 }
 STAGES = ["bin", "spread", "fft_forward", "green", "fft_backward", "gather"]
 
@@ -126,11 +127,13 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB_PATH):
+    from . import build
+    fresh = build.built_hash(LIB_PATH) == build.source_hash()
+    if not fresh:
+        # missing, or built from other sources than the ones beside it
         if not build_if_missing:
-            raise GseError(7, f"{LIB_PATH} is not built")
-        from . import build
-        build.build_lib()
+            raise GseError(7, f"{LIB_PATH} is not built from the current sources")
+        build.build_lib(force=True)
     L = ctypes.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
         f = getattr(L, name)

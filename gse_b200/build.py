@@ -4,6 +4,7 @@ output."""
 from __future__ import annotations
 
 import glob
+import hashlib
 import os
 import shutil
 import subprocess
@@ -53,15 +54,50 @@ def build_callbacks(verbose: bool = False) -> None:
     os.replace(CB_HEADER + ".tmp", CB_HEADER)
 
 
+HASH_MARK = b"gse-b200-sources:"
+
+
+def source_hash() -> str:
+    """First 16 hex digits of a SHA-256 over the library's sources (the .cu
+    and .cuh files, the public header, the cuFFT callback source), by path
+    and content; compiled into the library as its build stamp."""
+    h = hashlib.sha256()
+    files = sorted(_sources() + glob.glob(os.path.join(CSRC, "*.cuh")) +
+                   glob.glob(os.path.join(INCLUDE, "*.h")) + [CB_SRC])
+    for f in files:
+        h.update(os.path.relpath(f, ROOT).encode())
+        h.update(b"\0")
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def built_hash(path: str = LIB):
+    """The source hash stamped into a library file at its build (None when
+    the file or the stamp is missing); read from the file, not loaded."""
+    if not os.path.exists(path):
+        return None
+    with open(path, "rb") as fh:
+        data = fh.read()
+    i = data.find(HASH_MARK)
+    if i < 0:
+        return None
+    return data[i + len(HASH_MARK):i + len(HASH_MARK) + 16].decode("ascii", "replace")
+
+
 def _stale(target, deps):
     if not os.path.exists(target):
         return True
     t = os.path.getmtime(target)
-    return any(os.path.getmtime(d) > t for d in deps)
+    if any(os.path.getmtime(d) > t for d in deps):
+        return True
+    # file times can be lost in a copy; the stamp says which sources it came from
+    return target == LIB and built_hash(target) != source_hash()
 
 
 def nvcc_cmd(out=LIB):
-    return ([NVCC] + ARCH + NVCC_FLAGS + ["-shared", "-I", INCLUDE, "-I", CSRC, "-I", GEN] +
+    return ([NVCC] + ARCH + NVCC_FLAGS + [f'-DGSE_SOURCE_HASH="{source_hash()}"'] +
+            ["-shared", "-I", INCLUDE, "-I", CSRC, "-I", GEN] +
             _sources() +
             ["-o", out, "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft",
              "-Xlinker", "-rpath=" + os.path.join(CUDA_HOME, "lib64")])

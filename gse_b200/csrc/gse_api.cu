@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -801,6 +802,24 @@ const char* gse_status_string(gse_status_t s) {
 const char* gse_last_error(void) { return g_last_error.c_str(); }
 
 int gse_abi_version(void) { return GSE_B200_ABI_VERSION; }
+
+#ifndef GSE_SOURCE_HASH
+#define GSE_SOURCE_HASH "unstamped-build"
+#endif
+// The source hash as a marked string in the library file, where the loader
+// reads it without loading the library.
+extern "C" __attribute__((used)) const char gse_build_stamp[] =
+    "gse-b200-sources:" GSE_SOURCE_HASH;
+
+const char* gse_build_info(void) {
+  static char info[128];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    snprintf(info, sizeof(info), "sources %s, nvcc %d.%d.%d, sm_100a", GSE_SOURCE_HASH,
+             __CUDACC_VER_MAJOR__, __CUDACC_VER_MINOR__, __CUDACC_VER_BUILD__);
+  });
+  return info;
+}
 
 gse_status_t gse_create(const gse_params_t* params, gse_context_t** out) {
   g_last_error.clear();

@@ -96,6 +96,12 @@ const char* gse_last_error(void);
 
 int gse_abi_version(void);
 
+/* Build record of the loaded library: "sources <hash>, nvcc <version>,
+ * sm_100a", <hash> the first 16 hex digits of a SHA-256 over the sources it
+ * was compiled from (the loader rebuilds a library whose hash differs from
+ * the sources beside it). */
+const char* gse_build_info(void);
+
 /* ---- context lifetime ------------------------------------------------- */
 
 /* Replaces the constructors CpuGSE(...) / CpuGSEk(...) (CpuGSE.cpp:11-19,

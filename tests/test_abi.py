@@ -152,3 +152,14 @@ def test_support_size_matches_reference_formula():
                 dx, dy, dz = (np.float32(abs(t) - 1) * np.float32(h) for t in (tx, ty, tz))
                 cnt32 += (dx * dx + dy * dy) + dz * dz < rc2
     assert g.calcSupportSize(rcut, 20.0, 20.0, 20.0) == cnt32
+
+
+def test_library_is_stamped_with_its_sources():
+    """The library carries the hash of the sources it was built from; the
+    loader rebuilds a library whose stamp differs from the sources beside it,
+    and gse_build_info reports the stamp."""
+    from gse_b200 import _lib, build
+    h = build.source_hash()
+    assert len(h) == 16 and build.built_hash() == h
+    info = _lib.load().gse_build_info().decode()
+    assert info.startswith(f"sources {h}, nvcc ") and info.endswith("sm_100a")
