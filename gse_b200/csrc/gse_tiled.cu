@@ -674,6 +674,7 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
   constexpr int NW = GG::NW, APW = GG::APW;
   constexpr int NR = kGY * kGZ;  // cell rows of the brick
   constexpr int NG = (W * W + GL - 1) / GL;
+  static_assert(TZ * ZP < (1 << 23), "tile offsets fit the row list entries");
   typedef typename Vec4<CT>::type V;
   CT* tile = (CT*)gsm;                                   // [TZ][ZP]
   CT* tabs = tile + TZ * ZP;                             // [NW][APW][axis][d, d^2, w][kWPad]
@@ -790,7 +791,8 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         if (r < W * W)
           ne = add_rn(tb[(1 * 3 + 1) * kWPad + jy], tb[(2 * 3 + 1) * kWPad + jz]) < s.rcut2;
         const unsigned m = (__ballot_sync(0xffffffffu, ne) >> (GL * grp)) & gmask;
-        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = (jz << 8) | jy;
+        // the row's tile offset with its (jz, jy): bits 8+ offset, 4-7 jz, 0-3 jy
+        if (ne) rl[nrow + __popc(m & ((1u << gl) - 1u))] = ((jz * ZP + jy * TP) << 8) | (jz << 4) | jy;
         nrow += __popc(m);
       }
       __syncwarp();
@@ -804,6 +806,7 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
       // each row's 2n+1 terms and a lane's rows (about rows/16 of them) in CT, the
       // lanes' sums in double (the reference's AT)
       CT lx = 0, ly = 0, lz = 0;
+      const CT* abase = tile + loc[2] * ZP + loc[1] * TP + loc[0];  // the atom's first row
       // an end point of the rows lies outside the sphere for every row when
       // dx^2 >= rcut^2 there (rem <= rcut^2): the rows are then summed
       // without it, the same terms in the same order.  The first point is
@@ -815,10 +818,10 @@ __device__ __forceinline__ void gather_brick(const typename Vec4<CT>::type* __re
         constexpr int K1 = decltype(k1)::value;
         for (int i = gl; i < nrow; i += GL) {
           const int r = rl[i];
-          const int jz = r >> 8, jy = r & 255;
+          const int jz = (r >> 4) & 15, jy = r & 15;
           const CT dy2 = tb[(1 * 3 + 1) * kWPad + jy], dz2 = tb[(2 * 3 + 1) * kWPad + jz];
           const CT rem = s.rcut2 - (dy2 + dz2);
-          const CT* row = tile + (loc[2] + jz) * ZP + (loc[1] + jy) * TP + loc[0];
+          const CT* row = abase + (r >> 8);
           CT s0, s1;
           row_sums<CT, W, K0, K1>(row, dx2, wx, wdx, dy2, dz2, rem, s.rcut2, s0, s1);
           const CT wyz = tb[(1 * 3 + 2) * kWPad + jy] * tb[(2 * 3 + 2) * kWPad + jz];
