@@ -357,8 +357,10 @@ gse_status_t stage_atoms(gse_context_t* c, int n, const void* xyzq, const void**
 // Stable counting sort of the atoms into c->d_sorted / c->d_perm by
 // (z cell, y cell, x bin) of their stencil centres; c->d_bstart holds the bin
 // offsets afterwards.
+// clear_fixed: the counting kernel also clears the mixed form's int64 grid.
 template <typename CT>
-gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s) {
+gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT>& s,
+                       bool clear_fixed = false) {
   typedef typename Vec4<CT>::type V;
   StageTimer tm(c, GSE_STAGE_BIN);
   BinScratch w{c->d_bkey, c->d_bcounts, c->d_bstart, c->d_btiles, c->d_btmp, c->d_qmax,
@@ -369,6 +371,10 @@ gse_status_t bin_atoms(gse_context_t* c, int n, const void* dx, const Stencil<CT
   if (!c->fp64) {
     w.lstart = c->d_blstart;
     w.counts_zero = true;
+    if (clear_fixed) {
+      w.clear = c->d_fixed;
+      w.clear_n = c->size;
+    }
   }
   c->launches += c->fp64 ? (n > 0 ? 6 : 3) : (n > 0 ? 3 : 2);
   CU(launch_bin_sorted<CT>((const V*)dx, n, c->bl, s.inv_h[0], s.inv_h[1], s.inv_h[2], w,
@@ -1090,17 +1096,17 @@ gse_status_t forward_body(gse_context_t* c, int n, const void* xyzq, double* ene
   const void* dx = nullptr;
   TRY(stage_atoms(c, n, xyzq, &dx));
   const Box3 box = ctx_box(c);
-  // one stable sort serves the spread and the gather; the mixed form clears
-  // its int64 grid first, so that the spread follows the binning directly
-  // (kept inside the spread stage when stages are timed)
+  // one stable sort serves the spread and the gather; the mixed form's
+  // counting kernel clears the int64 grid on the way, so that the spread
+  // follows the binning directly (a memset in the spread stage when stages
+  // are timed)
   bool zeroed = false;
   if (c->fp64) {
     TRY(bin_atoms<double>(c, n, dx, stencil_of<double>(c, box.v, c->sigma1, c->rcut1, false, false)));
   } else {
     const Stencil<float> s = stencil_of<float>(c, box.v, c->sigma1, c->rcut1, false, false);
     zeroed = !c->timing && tiled_ok<float>(c, s);
-    if (zeroed) CU(cudaMemsetAsync(c->d_fixed, 0, sizeof(long long) * c->size, c->stream));
-    TRY(bin_atoms<float>(c, n, dx, s));
+    TRY(bin_atoms<float>(c, n, dx, s, zeroed));
   }
   if (c->fp64)
     TRY(do_spread<double>(c, n, dx, box.v, c->sigma1, c->rcut1, false, true));

@@ -37,8 +37,16 @@ template <typename CT>
 __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, int n, BinLayout b,
                             CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
                             int* __restrict__ counts, unsigned* __restrict__ qmax_bits,
-                            int* __restrict__ bad) {
+                            int* __restrict__ bad, long long* __restrict__ clear,
+                            long long clear_n) {
   pdl_trigger();
+  if (clear) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (long long i = first; i < clear_n / 2; i += stride)
+      reinterpret_cast<int4*>(clear)[i] = make_int4(0, 0, 0, 0);
+    if ((clear_n & 1) && first == 0) clear[clear_n - 1] = 0;
+  }
   float qm = 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const auto a = xyzq[i];
@@ -888,10 +896,16 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
     e = cudaMemsetAsync(qmax, 0, sizeof(unsigned), st);
     if (e != cudaSuccess) return e;
   }
-  const int gb = (int)std::min<long long>(sm_count() * 8, (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
+  // a grid to clear takes every SM; the atoms alone, one thread each up to that
+  const int gb = w.clear ? sm_count() * 8
+                         : (int)std::min<long long>(sm_count() * 8,
+                                                    (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
-                                        qmax, w.bad);
+                                        qmax, w.bad, w.clear, w.clear_n);
+  else if (w.clear)
+    e = cudaMemsetAsync(w.clear, 0, sizeof(long long) * w.clear_n, st);
+  if (e != cudaSuccess) return e;
   return launch_bin_scan_place<CT>(xyzq, n, nb, w, sorted, perm, st);
 }
 

@@ -59,6 +59,10 @@ struct BinScratch {
   // mixed form: `counts` are zero on entry (the order-free placement counts every
   // bin back down to zero), so the binning does not clear them
   bool counts_zero = false;
+  // an int64 array of clear_n elements (16-byte aligned) that the counting
+  // kernel clears on the way (the mixed form's spread grid); NULL: none
+  long long* clear = nullptr;
+  long long clear_n = 0;
 };
 
 // exp(-2 h^2 / (2 sigma^2)) per axis as an unevaluated sum hi + lo in CT
