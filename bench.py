@@ -590,6 +590,30 @@ def main():
     e2e_value = world * e2e_steps / (float(t.item()) / 1000.0)
     h2d = n * 4 * np.dtype(ct).itemsize
     d2h = 3 * n * 8 + 8
+    # the same two copies alone, on this box's link, to explain e2e (which
+    # varies from box to box with the host link while the device time does not)
+    dx = torch.empty(hx.shape, dtype=hx.dtype, device="cuda")
+    df = torch.empty(hf.shape, dtype=hf.dtype, device="cuda")
+
+    def copy_ms(fn):
+        a = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+        b = [torch.cuda.Event(enable_timing=True) for _ in range(e2e_steps)]
+        for k in range(e2e_steps):
+            a[k].record(stream)
+            fn()
+            b[k].record(stream)
+        torch.cuda.synchronize()
+        return sorted(x.elapsed_time(y) for x, y in zip(a, b))[e2e_steps // 2]
+
+    ms_h2d = copy_ms(lambda: dx.copy_(hx, non_blocking=True))
+    ms_d2h = copy_ms(lambda: hf.copy_(df, non_blocking=True))
+    pcie = {"what": "the evaluation's position upload and force download alone, pinned host "
+                    "memory, median of the e2e step count",
+            "h2d_ms": ms_h2d, "d2h_ms": ms_d2h,
+            "h2d_gbs": hx.numel() * hx.element_size() / (ms_h2d * 1e6),
+            "d2h_gbs": hf.numel() * hf.element_size() / (ms_d2h * 1e6),
+            "device_ms_plus_copies": ms_max / args.steps + ms_h2d + ms_d2h,
+            "e2e_ms": float(t.item()) / e2e_steps}
 
     # ---- the other precision, for the mixed-vs-FP64 comparison ----------
     other = "fp64" if prec == "mixed" else "mixed"
@@ -712,6 +736,7 @@ def main():
                        "l2": "flushed between timed evaluations (256 MiB write)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
+            "pcie": pcie,
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp32", "achieved": achieved_tf, "peak": fpeak,
                          "unit": "TFLOP/s", "frac": achieved_tf / fpeak if fpeak else None,
