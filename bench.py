@@ -76,10 +76,11 @@ def algorithmic_flops(stage: str) -> float:
 # what limits each kernel, from the committed full ncu capture of the
 # benchmark workload (profiles/spread_gather_water262k_mixed_full.md)
 LIMITER = {
-    "gather": "instruction issue at low occupancy (ncu: 509 warp instructions per atom, "
-              "61% issue-active, 16 warps per SM); FP32 lanes are the arithmetic roofline",
-    "spread": "shared-memory integer atomics and instruction issue (ncu: 440 warp "
-              "instructions per atom, 73% issue-active)",
+    "gather": "latency and instruction issue at low occupancy (ncu: 500 warp instructions "
+              "per atom, 64% issue-active, 16 warps per SM); FP32 lanes are the arithmetic "
+              "roofline",
+    "spread": "shared-memory integer reductions and instruction issue (ncu: 428 warp "
+              "instructions per atom, 71% issue-active, LSU pipe 74% busy)",
 }
 
 
