@@ -38,7 +38,7 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
                             CT inv_hx, CT inv_hy, CT inv_hz, int* __restrict__ key,
                             int* __restrict__ counts, unsigned* __restrict__ qmax_bits,
                             int* __restrict__ bad, long long* __restrict__ clear,
-                            long long clear_n) {
+                            long long clear_n, int* __restrict__ rank) {
   pdl_trigger();
   if (clear) {
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -58,7 +58,10 @@ __global__ void k_bin_count(const typename Vec4<CT>::type* __restrict__ xyzq, in
     const int cz = wrap1(centre_cell(a.z, inv_hz), b.M[2]);
     const int k = (cz * b.M[1] + cy) * b.nbx + (cx >> b.bxs);
     key[i] = k;
-    atomicAdd(&counts[k], 1);
+    // rank: the atom's place among its bin's atoms (counting order; the mixed
+    // form's consumers are order-free), so the placement needs no atomics
+    const int r = atomicAdd(&counts[k], 1);
+    if (rank) rank[i] = r;
   }
   if (!qmax_bits) return;  // uniform
   // block maximum first: one atomic per block, not per warp, on the single
@@ -156,13 +159,15 @@ __global__ void k_bin_place_direct(const typename Vec4<CT>::type* __restrict__ x
 
 // Order-free placement of the mixed form after a tile-local scan: the block's
 // copy of the tile offsets (exclusive prefix of the tile sums) turns the local
-// bin starts into global ones; the atoms are placed (counts[] counts down to
-// zero) and the global starts written for the kernels that read the bins.
+// bin starts into global ones; each atom goes to its bin's start plus the rank
+// the counting kernel gave it, the global starts are written for the kernels
+// that read the bins, and counts[] is cleared for the next call.
 __global__ void __launch_bounds__(256)
     k_bin_place_final(const float4* __restrict__ xyzq, int n, const int* __restrict__ key,
                       const int* __restrict__ lstart, const int* __restrict__ tile_sums,
                       int ntiles, int* __restrict__ counts, float4* __restrict__ sorted,
-                      int* __restrict__ perm, int* __restrict__ start, int nb) {
+                      int* __restrict__ perm, int* __restrict__ start, int nb,
+                      const int* __restrict__ rank) {
   pdl_trigger();
   pdl_wait();
   __shared__ int off[kScanTile];
@@ -187,11 +192,14 @@ __global__ void __launch_bounds__(256)
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   for (int i = gtid; i < n; i += gs) {
     const int k = key[i];
-    const int slot = lstart[k] + off[k / kScanTile] + atomicSub(&counts[k], 1) - 1;
+    const int slot = lstart[k] + off[k / kScanTile] + rank[i];
     sorted[slot] = xyzq[i];
     perm[slot] = i;
   }
-  for (int i = gtid; i < nb; i += gs) start[i] = lstart[i] + off[i / kScanTile];
+  for (int i = gtid; i < nb; i += gs) {
+    start[i] = lstart[i] + off[i / kScanTile];
+    counts[i] = 0;  // zero for the next call's counting
+  }
   if (gtid == 0) start[nb] = off[ntiles - 1] + tile_sums[ntiles - 1];
 }
 
@@ -902,7 +910,8 @@ cudaError_t launch_bin_sorted(const typename Vec4<CT>::type* xyzq, int n, const 
                                                     (n + 255) / 256 > 0 ? (n + 255) / 256 : 1);
   if (n > 0)
     k_bin_count<CT><<<gb, 256, 0, st>>>(xyzq, n, b, inv_hx, inv_hy, inv_hz, w.key, w.counts,
-                                        qmax, w.bad, w.clear, w.clear_n);
+                                        qmax, w.bad, w.clear, w.clear_n,
+                                        (sizeof(CT) == 4 && w.lstart) ? w.tmp : nullptr);
   else if (w.clear)
     e = cudaMemsetAsync(w.clear, 0, sizeof(long long) * w.clear_n, st);
   if (e != cudaSuccess) return e;
@@ -930,7 +939,7 @@ cudaError_t launch_bin_scan_place(const typename Vec4<CT>::type* xyzq, int n, in
     e = launch_dependent(true, k_bin_place_final, dim3(gb), dim3(256), 0, st,
                          (const float4*)xyzq, n, (const int*)w.key, (const int*)w.lstart,
                          (const int*)w.tile_sums, ntiles, w.counts, (float4*)sorted, perm,
-                         w.start, nb);
+                         w.start, nb, (const int*)w.tmp);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
   }

@@ -50,7 +50,7 @@ struct BinScratch {
   int* counts;     // [nbins]
   int* start;      // [nbins + 1]
   int* tile_sums;  // [ceil(nbins / 4096)]
-  int* tmp;        // [n]
+  int* tmp;        // [n]: the FP64 stable placement's scratch; the mixed form's ranks in bin
   unsigned* qmax_bits;  // max |q| over the atoms (float bits), written by the binning
   int* bad = nullptr;   // set to 1 when a position or charge is not finite (may be NULL)
   // mixed form: the scan's tile-local prefix [nbins] (the placement applies the tile
