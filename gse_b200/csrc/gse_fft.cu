@@ -4,7 +4,7 @@
 //   k_own_fft_xy_fwd   one CTA per z plane: int64 (or float) plane -> x r2c of
 //                      two real rows per half-warp complex transform -> y
 //                      transform of each x' column in shared memory -> rho^
-//   k_own_fft_z_green  a CTA per (y, 16 x' columns): z transform, Green's
+//   k_own_fft_z_green  a CTA per 16 (y, x') columns: z transform, Green's
 //                      multiply and k-space energy, inverse z transform
 //   k_own_fft_xy_inv   one CTA per z plane: inverse y, then the c2r x transform
 //                      of two rows per half-warp complex transform -> phi
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kColThreads, z_blocks(N2))
     k_own_fft_z_green(float2* __restrict__ rhok, const float* __restrict__ tab,
                       const float2* __restrict__ tw, double* __restrict__ partials,
                       unsigned* __restrict__ done, double factor, double* __restrict__ out) {
-  constexpr int M = 16 * N2, X = M / 2 + 1, NXT = (X + 15) / 16;
+  constexpr int M = 16 * N2, X = M / 2 + 1;
   __shared__ float2 Q[M][17];
   __shared__ float G[M][17];
   const int tid = threadIdx.x, hw = tid >> 4, l = tid & 15;
@@ -294,10 +294,11 @@ __global__ void __launch_bounds__(kColThreads, z_blocks(N2))
   LaneTw<N2> lt;
   lt.load(tw, l);
   pdl_wait();
-  const int xt = blockIdx.x % NXT, y = blockIdx.x / NXT;
-  const int x0 = xt * 16, nx = min(16, X - x0);
+  // 16 consecutive (y, x') columns, y X + x' in the flattened plane, which is
+  // contiguous in every z plane: full tiles across row ends (M X / 16 CTAs)
+  const int c0 = blockIdx.x * 16, nx = min(16, M * X - c0);
   const long long zs = (long long)M * X;
-  const long long base = (long long)y * X + x0;
+  const long long base = c0;
   // M * 16 / kColThreads = N2 elements per thread, all loads issued first
   {
     float2 q[N2];
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kColThreads, z_blocks(N2))
     for (int j = 0; j < N2; j++) v[j] = Q[l + 16 * j][hw];
     fft16<N2, false>(v, l, mask, lt);
     const int k1 = brev4(l);
-    const int xg = x0 + hw;
+    const int xg = (c0 + hw) % X;
     const double wgt = (xg == 0 || 2 * xg == M) ? 1.0 : 2.0;
 #pragma unroll
     for (int k2 = 0; k2 < N2; k2++) {
@@ -789,8 +790,8 @@ cudaError_t fwd_n2(const long long* g64, const float* rho, double unscale, float
 template <int N2>
 cudaError_t z_n2(float2* rhok, const float* tab, const float2* tw, double* partials,
                  unsigned* done, double factor, double* out, bool pdl, cudaStream_t st) {
-  constexpr int M = 16 * N2, X = M / 2 + 1, NXT = (X + 15) / 16;
-  const cudaError_t e = launch_dependent(pdl, k_own_fft_z_green<N2>, dim3(NXT * M),
+  constexpr int M = 16 * N2, X = M / 2 + 1;
+  const cudaError_t e = launch_dependent(pdl, k_own_fft_z_green<N2>, dim3((M * X + 15) / 16),
                                          dim3(kColThreads), 0, st, rhok, tab, tw, partials, done,
                                          factor, out);
   return e != cudaSuccess ? e : cudaGetLastError();
