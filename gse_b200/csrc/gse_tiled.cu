@@ -516,6 +516,7 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
   constexpr int NPASS = (W * W + 31) / 32;
   __shared__ int rng_a[kSB * kSB], rng_p[kSB * kSB];
   __shared__ int alist[kScatterList];
+  __shared__ __align__(16) float wys[NW][16];  // each warp's atom's y weights
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int x0 = bxi * kSB, y0 = byi * kSB, z0 = bzi * kSB;
@@ -554,9 +555,25 @@ __device__ __forceinline__ void scatter_brick(const float4* __restrict__ sorted,
         const float dd = sub_rn(mul_rn((float)(c - n + lane), s.h[d]), pos3[d]);
         wl[d] = (lane < W) ? wexp(mul_rn(mul_rn(-dd, dd), s.inv_2s2)) : 0.f;
       }
+      // every lane needs all W y weights: stored once by the lanes that formed
+      // them and read back by four 16-byte broadcast loads (13 shuffles took
+      // the shared-memory pipe the reductions wait for; the x and z weights,
+      // one each per pass, stay shuffles: per-lane loads of them were slower)
       float wy[W];
+      {
+        __syncwarp();  // the warp's previous atom has read its weights
+        if (lane < 16) wys[warp][lane] = wl[1];
+        __syncwarp();
+        const float4* v = reinterpret_cast<const float4*>(wys[warp]);
 #pragma unroll
-      for (int k = 0; k < W; k++) wy[k] = __shfl_sync(0xffffffffu, wl[1], k);
+        for (int q4 = 0; q4 < (W + 3) / 4; q4++) {
+          const float4 t = v[q4];
+          wy[4 * q4] = t.x;
+          if (4 * q4 + 1 < W) wy[4 * q4 + 1] = t.y;
+          if (4 * q4 + 2 < W) wy[4 * q4 + 2] = t.z;
+          if (4 * q4 + 3 < W) wy[4 * q4 + 3] = t.w;
+        }
+      }
       // y weights in pairs for the packed fma (two points per instruction)
       unsigned long long wy2[W / 2];
 #pragma unroll
