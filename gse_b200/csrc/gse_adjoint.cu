@@ -211,6 +211,15 @@ __global__ void __launch_bounds__(256)
 // whose distance equals the cut-off to rounding, whose weight is e^-9 of the
 // centre's.
 
+// Per-warp slots for the y tables of the reverse-pass scatter, one array for
+// every stencil width a kernel instantiates (a static array in the templated
+// function would be one per width, too much static shared memory for the
+// fused reverse kernel).
+__device__ __forceinline__ float (*adj_ytab())[3][16] {
+  __shared__ __align__(16) float t[kScatterThreads / 32][3][16];
+  return t;
+}
+
 template <int W>
 __device__ __forceinline__ void adj_scatter_brick(
     const float4* __restrict__ sorted, const int* __restrict__ perm, const int* __restrict__ start,
@@ -247,6 +256,7 @@ __device__ __forceinline__ void adj_scatter_brick(
   }
   // per warp: the pairs whose column meets the sphere, packed x | z << 4
   __shared__ unsigned char plist_all[NW][W * W];
+  float (*ytab)[3][16] = adj_ytab();  // e, u, u^2 along y of each warp's atom
   unsigned char* plist = plist_all[warp];
   for (int c0 = 0; c0 < total; c0 += kScatterList) {
     brick_atom_list<NT, kSB * kSB>(rng_a, rng_p, total, c0, kScatterList, alist);
@@ -271,12 +281,36 @@ __device__ __forceinline__ void adj_scatter_brick(
         u2l[d] = u2;
         el[d] = (lane < W) ? expf(mul_rn(-u2, s.inv_2s2)) : 0.f;
       }
+      // the y tables every lane needs, through the warp's shared slots and
+      // 16-byte broadcast loads rather than 39 shuffles (as in the spread)
       float ey[W], eyuy[W], uy2[W];
+      {
+        __syncwarp();  // the warp's previous atom has read its tables
+        if (lane < 16) {
+          ytab[warp][0][lane] = el[1];
+          ytab[warp][1][lane] = ul[1];
+          ytab[warp][2][lane] = u2l[1];
+        }
+        __syncwarp();
+        float uy[W];
+        const float4* v0 = reinterpret_cast<const float4*>(ytab[warp][0]);
+        const float4* v1 = reinterpret_cast<const float4*>(ytab[warp][1]);
+        const float4* v2 = reinterpret_cast<const float4*>(ytab[warp][2]);
 #pragma unroll
-      for (int k = 0; k < W; k++) {
-        ey[k] = __shfl_sync(0xffffffffu, el[1], k);
-        eyuy[k] = ey[k] * __shfl_sync(0xffffffffu, ul[1], k);
-        uy2[k] = __shfl_sync(0xffffffffu, u2l[1], k);
+        for (int q4 = 0; q4 < (W + 3) / 4; q4++) {
+          const float4 a = v0[q4], b = v1[q4], c = v2[q4];
+          const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w},
+                      cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (4 * q4 + j < W) {
+              ey[4 * q4 + j] = av[j];
+              uy[4 * q4 + j] = bv[j];
+              uy2[4 * q4 + j] = cv[j];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < W; k++) eyuy[k] = ey[k] * uy[k];
       }
       // the same weights in pairs of y points for the packed fma
       unsigned long long ey2[W / 2], eyuy2[W / 2], magic2;
