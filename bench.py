@@ -79,8 +79,8 @@ LIMITER = {
     "gather": "latency and instruction issue at low occupancy (ncu: 500 warp instructions "
               "per atom, 64% issue-active, 16 warps per SM); FP32 lanes are the arithmetic "
               "roofline",
-    "spread": "shared-memory integer reductions and instruction issue (ncu: 428 warp "
-              "instructions per atom, 71% issue-active, LSU pipe 74% busy)",
+    "spread": "shared-memory integer reductions and instruction issue (ncu: 424 warp "
+              "instructions per atom, 74% issue-active, LSU pipe 72% busy)",
 }
 
 
